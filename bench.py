@@ -1,0 +1,374 @@
+"""Benchmark of the per-ray hot path on the 500k-Gaussian scattering showcase workload.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--engine warp|megakernel]
+
+Workload (one "step" = one launch batch of 16 samples per pixel over the whole 512x512 image,
+the reference's per-launch granularity, renderer.cpp:32,353-371; 16 steps = the full 256-spp
+render): 500k anisotropic Gaussians in value-noise clusters, procedural 2048x1024 HDR
+environment with alias-table importance sampling, NEE+MIS with two shadow rays, Russian roulette
+from depth 12, max depth 64, isotropic phase.  Metric: Mpaths/s (a path = one (pixel, sample)
+camera path run to termination).  Inputs are resident in HBM when the timed region starts; the
+L2 is flushed (256 MiB write) between timed steps and each step is timed with CUDA events on the
+render stream.  `e2e` times the same metric through the public API from pinned host buffers:
+scene + environment upload and build, the whole render, and the image read-back.
+
+Under torchrun each rank renders its own sample range (weak scaling: per-GPU work fixed) and the
+per-rank images are reduced over NCCL at the end of the timed region.
+`--impl reference` times the reference's path restated on the host cores (oracle port; the
+reference itself needs OptiX and an RT-core GPU) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cuda-volprim_b200"))
+
+METRIC = "Mpaths/s (showcase 500k, NEE+MIS; equal-RMSE vs megakernel = same estimator)"
+UNIT = "Mpaths/s"
+BATCH_SPP = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="warp", choices=["warp", "megakernel"])
+    ap.add_argument("--n", type=int, default=500_000)
+    ap.add_argument("--res", type=int, default=512)
+    ap.add_argument("--spp", type=int, default=256)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-baseline-engine", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    from volprim_b200 import scenes
+    return scenes.showcase_500k(seed=0, n=args.n, res=args.res, spp=args.spp)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class CpuBaseline:
+    """The reference's path restated on the host (oracle port, reference RNG order) on a bounded
+    sample of the workload: image rows spread evenly over the image, 2 spp, all host threads."""
+
+    def __init__(self, w):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        self.O, self.w = O, w
+        t0 = time.time()
+        self.osc = O.OracleScene.from_gaussians(w.gaussians, sigma_multiplier=w.sigma_multiplier, use_bvh=True)
+        self.env = O.OracleEnv(w.env) if w.env is not None else O.OracleEnv.constant()
+        self.build_s = time.time() - t0
+        cfg = w.config
+        self.c16 = O.camera16(w.camera, cfg.image_width, cfg.image_height)
+        self.threads = O.max_threads()
+        H = cfg.image_height
+        self.stride = max(1, H // 64)
+        self.rows = list(range(self.stride // 2, H, self.stride))
+        self.next = 0
+
+    def sample(self, seconds_target=15.0) -> dict:
+        cfg = self.w.config
+        spent, paths, nrows = 0.0, 0, 0
+        while spent < seconds_target and nrows < len(self.rows):
+            y = self.rows[self.next % len(self.rows)]
+            self.next += 1
+            _, secs = self.O.render(self.osc, self.env, self.c16, cfg, y0=y, y1=y + 1, s0=0, s1=2,
+                                    rng_mode="sequential", threads=self.threads)
+            spent += secs
+            paths += cfg.image_width * 2
+            nrows += 1
+        return {"value": paths / spent / 1e6, "unit": UNIT, "cores": self.threads, "kind": "port",
+                "sample": f"{nrows} image rows from an even spread (every {self.stride}th of "
+                          f"{cfg.image_height}) x {cfg.image_width} px x 2 spp, reference RNG order, CPU BVH; "
+                          f"{paths} paths in {spent:.1f} s (scene + BVH build {self.build_s:.1f} s untimed)"}
+
+
+def cpu_baseline(w, seconds_target=15.0):
+    return CpuBaseline(w).sample(seconds_target)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(args)
+    cb = CpuBaseline(w)
+    res = []
+    for i in range(args.warmup + args.steps):
+        r = cb.sample(seconds_target=6.0 if i >= args.warmup else 1.0)
+        if i >= args.warmup:
+            res.append(r)
+    vals = [r["value"] for r in res]
+    v = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": f"showcase_{args.n // 1000}k", "gaussians": args.n, "width": args.res,
+                       "height": args.res, "spp": args.spp, "nee": "mis", "max_depth": 64, "rr_depth": 12,
+                       "env": "procedural 2048x1024", "l2": "n/a (host)"},
+            "cpu_baseline": {**res[-1], "value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import volprim_b200 as vp
+    from volprim_b200 import _capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    w = workload(args)
+    cfg = w.config
+    cfg.engine = args.engine
+    cfg.batch_spp = BATCH_SPP
+    # weak scaling: every rank renders its own `spp` samples of a world*spp-sample image
+    cfg.num_samples_per_pixel = args.spp * world
+    W, H = cfg.image_width, cfg.image_height
+    ctx = vp.Context(local)
+    scene = vp.Scene(ctx, w.gaussians, w.sigma_multiplier)
+    env = vp.Environment(ctx, rgb=w.env)
+    img = vp.ProgressiveImage(ctx, W, H)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    base = rank * args.spp
+
+    def step(i):  # one launch batch of BATCH_SPP samples
+        off = base + (i * BATCH_SPP) % args.spp
+        return img.accumulate(scene, env, w.camera, cfg, off, BATCH_SPP)
+
+    # warm-up (also the first steps of the image)
+    for i in range(args.warmup):
+        step(i)
+    # measured counters of one batch (untimed): crossings, node visits, Gaussian tests
+    mcfg = vp.Config(**{**cfg.__dict__, "measure_caps": True})
+    img_m = vp.ProgressiveImage(ctx, W, H)
+    mstats = img_m.accumulate(scene, env, w.camera, mcfg, base, BATCH_SPP)
+    img_m.close()
+    img.clear()
+
+    clocks = ClockSampler(local)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))  # L2 flush, outside the step's events
+            starts[i].record(stream)
+        step(i)
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    reduce_ms = 0.0
+    if dist:  # the job's one exchange: mean of the per-rank images (equal sample counts)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        acc = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+        ev0.record(stream)
+        _capi.check(_capi.lib.vp_image_read(img.handle, acc.data_ptr(), _capi.VP_MEMORY_DEVICE))
+        with torch.cuda.stream(stream):
+            dist.all_reduce(acc)
+            acc /= world
+            ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist:
+        reduce_ms = ev0.elapsed_time(ev1)
+    total_ms = sum(step_ms) + reduce_ms
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    paths_per_rank = W * H * BATCH_SPP * args.steps
+    value = paths_per_rank * world / (total_ms / 1e3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # roofline of the dominant kernel (k_render_warp): algorithmic bytes per launch (one batch) =
+    # Gaussian boxes tested x 32 B + Gaussian records loaded x 64 B + inner-node visits x node
+    # bytes (BVH32: 32 child boxes = 1 KiB; binary LBVH: 64 B)
+    node_bytes = 1024 if args.engine == "warp" else 64
+    alg_bytes = mstats["prim_tests"] * 32 + mstats["geo_loads"] * 64 + mstats["nodes_visited"] * node_bytes
+    launch_ms = statistics.mean(step_ms)
+    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": peak_kind,
+            "note": "achieved = (Gaussian boxes tested x 32 B + records loaded x 64 B + BVH32 inner nodes x 1 KiB) per launch / mean "
+                    "launch time; the scene is L2-resident, so most of these bytes are L2 hits",
+            "per_launch": {"prim_tests": mstats["prim_tests"], "geo_loads": mstats["geo_loads"], "crossings": mstats["crossings"],
+                           "inner_nodes": mstats["nodes_visited"], "leaves": mstats["leaves_visited"],
+                           "bounces": mstats["bounces"], "shadow_rays": mstats["shadow_rays"],
+                           "max_point_overlap": mstats["max_point_overlap"], "max_hits_per_ray": mstats["max_hits_per_ray"]}}
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        try:
+            tr = json.loads(traffic_file.read_text()).get(args.engine)
+            if tr:
+                roof["traffic"] = tr["bytes_per_launch"]
+        except Exception:
+            pass
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": f"showcase_{args.n // 1000}k", "gaussians": args.n, "width": W, "height": H,
+                       "spp_per_rank": args.spp, "step": f"{BATCH_SPP} spp over the full image", "nee": "mis",
+                       "max_depth": cfg.max_bounces, "rr_depth": cfg.rr_depth, "env": "procedural 2048x1024",
+                       "engine": args.engine, "precision": "fast (FP32)",
+                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"samples x{world}"},
+            "clocks": clk, "gpu_launches": args.steps, "roofline": roof,
+            "scene": scene.info(), "env_build_ms": env.build_ms, "wall_s": wall}
+    if rank == 0 and not args.no_baseline_engine and args.engine == "warp" and world == 1:
+        # the plain per-pixel megakernel of the same method on the same batches (for the ratio)
+        mcfg2 = vp.Config(**{**cfg.__dict__, "engine": "megakernel"})
+        im2 = vp.ProgressiveImage(ctx, W, H)
+        im2.accumulate(scene, env, w.camera, mcfg2, 0, BATCH_SPP)
+        torch.cuda.synchronize()
+        ms = []
+        for i in range(2):
+            st = im2.accumulate(scene, env, w.camera, mcfg2, BATCH_SPP * (i + 1), BATCH_SPP)
+            ms.append(st["ms_kernels"])
+        im2.close()
+        line["megakernel_baseline"] = {"value": W * H * BATCH_SPP / (statistics.mean(ms) / 1e3) / 1e6, "unit": UNIT,
+                                       "ms_per_step": statistics.mean(ms)}
+    if not args.no_e2e and world == 1:
+        line["e2e"] = e2e_run(args, w, local)
+    if rank == 0 and not args.no_cpu and world == 1:
+        line["cpu_baseline"] = cpu_baseline(w)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    img.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e_run(args, w, device):
+    """Public API end to end from pinned host memory: scene + env upload and device builds, the full
+    render, read-back of the image; Mpaths/s over the whole job."""
+    import numpy as np
+    import torch
+    import volprim_b200 as vp
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()
+        return t.numpy()
+
+    g = w.gaussians
+    gp = vp.Gaussians(pinned(g.mean), pinned(g.scale), pinned(g.quat_wxyz), pinned(g.density), pinned(g.albedo))
+    envp = pinned(w.env)
+    cfg = vp.Config(**{**w.config.__dict__, "num_samples_per_pixel": args.spp, "batch_spp": BATCH_SPP,
+                       "engine": args.engine})
+    ctx = vp.Context(device)
+    times = []
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = vp.Renderer(cfg, gp, w.camera, env=envp, sigma_multiplier=w.sigma_multiplier, ctx=ctx)
+        out = r.render()
+        times.append(time.perf_counter() - t0)
+        r.scene.close()
+        r.env.close()
+    paths = cfg.image_width * cfg.image_height * cfg.num_samples_per_pixel
+    h2d = sum(a.nbytes for a in (gp.mean, gp.scale, gp.quat_wxyz, gp.density, gp.albedo)) + envp.nbytes
+    return {"value": paths / min(times) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(out.nbytes), "seconds": min(times),
+            "note": "one step here = the whole job (upload, BVH + env builds, 256 spp, read-back)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,648 @@
+// Scene build on the device: per-Gaussian precompute, 3-sigma ellipsoid bounds, 63-bit Morton
+// codes, radix sort, Karras binary radix tree, bottom-up refit, collapse to a 32-wide BVH.
+//
+// Replaces the reference's host Morton sort + OptiX unit-sphere GAS / instance IAS build
+// (src/thesis/host/app/renderer.cpp:85-173, include/thesis/host/utils/math.h:103-131,
+// include/thesis/host/optix/acceleration_structure.h:23-87) and the Primitive precompute
+// (include/thesis/device/params/primitive.h:70-87) plus PLY-load validation
+// (src/thesis/host/utils/io/ply.cpp:124-172).
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "vp_internal.h"
+
+namespace vp {
+namespace {
+
+constexpr uint32_t kLeafMax = 32;  // Gaussians per BVH32 leaf = one per lane
+
+struct ErrorWords {
+  int bad_scale, bad_density, bad_center;  // lowest failing index (INT_MAX = none)
+  unsigned int any_albedo;                 // 1 if some albedo component > 0
+};
+
+__device__ __forceinline__ float clamp_albedo(float v) {
+  if (!isfinite(v)) return 0.0f;
+  if (v < 0.0f) return 0.0f;
+  if (v > 1.0f) return 1.0f;
+  return v;
+}
+
+// One thread per Gaussian: the reference's Primitive constructor arithmetic in FP32 (host
+// order; IEEE division/sqrt), the whitening matrix W = diag(1/s) R(q)^T and the 3-sigma
+// ellipsoid's axis-aligned bound (from renderer.cpp:142-157's local-to-world TRS with 3x scale).
+__global__ void k_precompute(uint32_t n, const float* __restrict__ mean,
+                             const float* __restrict__ scale, const float* __restrict__ quat,
+                             const float* __restrict__ density, const float* __restrict__ albedo,
+                             int scale_is_log, float sigma_multiplier, float4* __restrict__ rec,
+                             float4* __restrict__ lo, float4* __restrict__ hi,
+                             ErrorWords* __restrict__ err) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float cx = mean[3 * i], cy = mean[3 * i + 1], cz = mean[3 * i + 2];
+  float sx = scale[3 * i], sy = scale[3 * i + 1], sz = scale[3 * i + 2];
+  if (scale_is_log) {
+    sx = expf(sx);
+    sy = expf(sy);
+    sz = expf(sz);
+  }
+  const float qw = quat[4 * i], qx = quat[4 * i + 1], qy = quat[4 * i + 2], qz = quat[4 * i + 3];
+  // UnitQuaternion::from: rlength(float4(w,x,y,z)) = 1 / sqrt(fma(w,w,fma(x,x,fma(y,y,z*z))))
+  const float qr = __fdiv_rn(1.0f, __fsqrt_rn(fmaf(qw, qw, fmaf(qx, qx, fmaf(qy, qy, __fmul_rn(qz, qz))))));
+  const float w = __fmul_rn(qw, qr), x = __fmul_rn(qx, qr), y = __fmul_rn(qy, qr), z = __fmul_rn(qz, qr);
+  const float M = __fmul_rn(density[i], sigma_multiplier);  // ply.cpp:116
+  float ar = 0.f, ag = 0.f, ab = 0.f;
+  if (albedo) {
+    ar = clamp_albedo(albedo[3 * i]);
+    ag = clamp_albedo(albedo[3 * i + 1]);
+    ab = clamp_albedo(albedo[3 * i + 2]);
+  }
+  if (ar > 0.f || ag > 0.f || ab > 0.f) atomicOr(&err->any_albedo, 1u);
+  const bool scale_ok = sx > 0.f && sy > 0.f && sz > 0.f && isfinite(sx) && isfinite(sy) && isfinite(sz);
+  if (!scale_ok) atomicMin(&err->bad_scale, (int)i);
+  if (!(M > 0.f) || !isfinite(M)) atomicMin(&err->bad_density, (int)i);
+  if (!isfinite(cx) || !isfinite(cy) || !isfinite(cz) || !isfinite(w) || !isfinite(x) ||
+      !isfinite(y) || !isfinite(z))
+    atomicMin(&err->bad_center, (int)i);
+  // Primitive ctor (primitive.h:80-87): rcp_scale, density_norm_factor, inv_cdf_factor.
+  const float rx = __fdiv_rn(1.0f, sx), ry = __fdiv_rn(1.0f, sy), rz = __fdiv_rn(1.0f, sz);
+  const float dnf = __fmul_rn(0.0634936359f, __fmul_rn(__fmul_rn(rx, ry), rz));
+  const float icf = __fmul_rn(__fmul_rn(M, dnf), 1.2533141373f);
+  // Forward rotation matrix R(q) (include/thesis/host/utils/math.h:52-97 without scale).
+  const double dw = w, dx = x, dy = y, dz = z;
+  double R[3][3];
+  R[0][0] = 1.0 - 2.0 * (dy * dy + dz * dz);
+  R[0][1] = 2.0 * (dx * dy - dw * dz);
+  R[0][2] = 2.0 * (dx * dz + dw * dy);
+  R[1][0] = 2.0 * (dx * dy + dw * dz);
+  R[1][1] = 1.0 - 2.0 * (dx * dx + dz * dz);
+  R[1][2] = 2.0 * (dy * dz - dw * dx);
+  R[2][0] = 2.0 * (dx * dz - dw * dy);
+  R[2][1] = 2.0 * (dy * dz + dw * dx);
+  R[2][2] = 1.0 - 2.0 * (dx * dx + dy * dy);
+  const double rs[3] = {rx, ry, rz};
+  const double ss[3] = {sx, sy, sz};
+  float W[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) W[r][c] = (float)(rs[r] * R[c][r]);
+  rec[4 * i + 0] = make_float4(cx, cy, cz, W[0][0]);
+  rec[4 * i + 1] = make_float4(W[0][1], W[0][2], W[1][0], W[1][1]);
+  rec[4 * i + 2] = make_float4(W[1][2], W[2][0], W[2][1], W[2][2]);
+  rec[4 * i + 3] = make_float4(icf, ar, ag, ab);
+  double e[3];
+  for (int k = 0; k < 3; ++k) {
+    const double a0 = R[k][0] * ss[0], a1 = R[k][1] * ss[1], a2 = R[k][2] * ss[2];
+    // 3-sigma half extent along world axis k, padded so FP32 chord tests never escape it.
+    e[k] = 3.0 * sqrt(a0 * a0 + a1 * a1 + a2 * a2) * (1.0 + 1e-5) + 1e-7 * (1.0 + fabs((double)mean[3 * i + k]));
+  }
+  lo[i] = make_float4((float)((double)cx - e[0]), (float)((double)cy - e[1]), (float)((double)cz - e[2]), 0.f);
+  hi[i] = make_float4((float)((double)cx + e[0]), (float)((double)cy + e[1]), (float)((double)cz + e[2]), 0.f);
+}
+
+__device__ __forceinline__ unsigned int f2ord(float f) {
+  const unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned int u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Bounds of the Gaussian centres (Morton frame, as computeBounds in math.h:135-160) and of
+// the 3-sigma boxes (scene bounds).
+__global__ void k_bounds(uint32_t n, const float* __restrict__ mean, const float4* __restrict__ lo,
+                         const float4* __restrict__ hi, unsigned int* __restrict__ out12) {
+  float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  float bmn[3] = {INFINITY, INFINITY, INFINITY}, bmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int k = 0; k < 3; ++k) {
+      const float c = mean[3 * i + k];
+      cmn[k] = fminf(cmn[k], c);
+      cmx[k] = fmaxf(cmx[k], c);
+    }
+    const float4 l = lo[i], h = hi[i];
+    bmn[0] = fminf(bmn[0], l.x); bmn[1] = fminf(bmn[1], l.y); bmn[2] = fminf(bmn[2], l.z);
+    bmx[0] = fmaxf(bmx[0], h.x); bmx[1] = fmaxf(bmx[1], h.y); bmx[2] = fmaxf(bmx[2], h.z);
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xFFFFFFFFu, cmn[k], o));
+      cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xFFFFFFFFu, cmx[k], o));
+      bmn[k] = fminf(bmn[k], __shfl_xor_sync(0xFFFFFFFFu, bmn[k], o));
+      bmx[k] = fmaxf(bmx[k], __shfl_xor_sync(0xFFFFFFFFu, bmx[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(&out12[k], f2ord(cmn[k]));
+      atomicMax(&out12[3 + k], f2ord(cmx[k]));
+      atomicMin(&out12[6 + k], f2ord(bmn[k]));
+      atomicMax(&out12[9 + k], f2ord(bmx[k]));
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t expand21(uint64_t v) {  // 21 bits -> every third of 63
+  v &= 0x1FFFFFull;
+  v = (v | (v << 32)) & 0x1F00000000FFFFull;
+  v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+  v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+  v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+// 63-bit Morton code of each centre (21 bits per axis; the reference uses 10 bits per axis on
+// the host, math.h:117-131 -- more bits keep 2M-Gaussian scenes from collapsing into shared
+// codes).
+__global__ void k_morton(uint32_t n, const float* __restrict__ mean, const unsigned int* __restrict__ b,
+                         uint64_t* __restrict__ codes, uint32_t* __restrict__ idx) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t code = 0;
+  for (int k = 0; k < 3; ++k) {
+    const float mn = ord2f(b[k]), mx = ord2f(b[3 + k]);
+    const float inv = 1.0f / fmaxf(mx - mn, 1e-30f);
+    const float t = fminf(fmaxf((mean[3 * i + k] - mn) * inv, 0.0f), 1.0f);
+    const uint64_t q = (uint64_t)(t * 2097151.0f);
+    code |= expand21(q) << k;  // x lowest bit, then y, then z (math.h:128)
+  }
+  codes[i] = code;
+  idx[i] = i;
+}
+
+__global__ void k_gather(uint32_t n, const uint32_t* __restrict__ order, const float4* __restrict__ rec_in,
+                         const float4* __restrict__ lo_in, const float4* __restrict__ hi_in,
+                         float4* __restrict__ rec_out, float4* __restrict__ lo_out,
+                         float4* __restrict__ hi_out, float4* __restrict__ pbox) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = order[i];
+  for (int k = 0; k < 4; ++k) rec_out[4 * i + k] = rec_in[4 * s + k];
+  lo_out[i] = lo_in[s];
+  hi_out[i] = hi_in[s];
+  pbox[2 * i] = lo_in[s];
+  pbox[2 * i + 1] = hi_in[s];
+}
+
+__device__ __forceinline__ int karras_delta(const uint64_t* __restrict__ codes, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const uint64_t a = codes[i], b = codes[j];
+  if (a == b) return 64 + __clz(i ^ j);
+  return __clzll(a ^ b);
+}
+
+// Karras 2012 ("Maximizing parallelism in the construction of BVHs, octrees, and k-d trees"):
+// one thread per internal node of the binary radix tree over the sorted codes.
+__global__ void k_karras(int n, const uint64_t* __restrict__ codes, uint32_t* __restrict__ left,
+                         uint32_t* __restrict__ right, uint32_t* __restrict__ first,
+                         uint32_t* __restrict__ last, uint32_t* __restrict__ parent_int,
+                         uint32_t* __restrict__ parent_leaf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = (karras_delta(codes, n, i, i + 1) - karras_delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = karras_delta(codes, n, i, i - d);
+  int lmax = 2;
+  while (karras_delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (karras_delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = karras_delta(codes, n, i, j);
+  int s = 0, t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (karras_delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  const int gamma = i + s * d + min(d, 0);
+  const int lo_i = min(i, j), hi_i = max(i, j);
+  uint32_t lref, rref;
+  if (lo_i == gamma) {
+    lref = kLeafBit | (uint32_t)gamma;
+    parent_leaf[gamma] = i;
+  } else {
+    lref = (uint32_t)gamma;
+    parent_int[gamma] = i;
+  }
+  if (hi_i == gamma + 1) {
+    rref = kLeafBit | (uint32_t)(gamma + 1);
+    parent_leaf[gamma + 1] = i;
+  } else {
+    rref = (uint32_t)(gamma + 1);
+    parent_int[gamma + 1] = i;
+  }
+  left[i] = lref;
+  right[i] = rref;
+  first[i] = lo_i;
+  last[i] = hi_i;
+}
+
+__device__ __forceinline__ void child_box(uint32_t ref, const float4* plo, const float4* phi,
+                                          const float4* nlo, const float4* nhi, float4& l, float4& h) {
+  if (ref_is_leaf(ref)) {
+    const uint32_t p = ref & ~kLeafBit;
+    l = plo[p];
+    h = phi[p];
+  } else {
+    l = __ldcg(nlo + ref);
+    h = __ldcg(nhi + ref);
+  }
+}
+
+// Bottom-up refit: the second thread to reach an internal node unions its children.
+__global__ void k_refit(int n, const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                        const uint32_t* __restrict__ parent_int, const uint32_t* __restrict__ parent_leaf,
+                        const float4* __restrict__ plo, const float4* __restrict__ phi,
+                        float4* nlo, float4* nhi, unsigned int* flags) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n || n < 2) return;
+  uint32_t node = parent_leaf[k];
+  while (true) {
+    __threadfence();
+    if (atomicAdd(&flags[node], 1u) == 0u) return;
+    __threadfence();
+    float4 al, ah, bl, bh;
+    child_box(left[node], plo, phi, nlo, nhi, al, ah);
+    child_box(right[node], plo, phi, nlo, nhi, bl, bh);
+    __stcg(nlo + node, make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f));
+    __stcg(nhi + node, make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f));
+    if (node == 0u) return;
+    node = parent_int[node];
+  }
+}
+
+// Binary-LBVH node records for the thread-per-ray megakernel: (l_lo, l_hi, r_lo, r_hi), child
+// refs in l_lo.w / r_lo.w (leaf bit | Morton-order Gaussian index).
+__global__ void k_binary_nodes(int n, const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                               const float4* __restrict__ plo, const float4* __restrict__ phi,
+                               const float4* __restrict__ nlo, const float4* __restrict__ nhi,
+                               float4* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  float4 al, ah, bl, bh;
+  child_box(left[i], plo, phi, nlo, nhi, al, ah);
+  child_box(right[i], plo, phi, nlo, nhi, bl, bh);
+  al.w = __uint_as_float(left[i]);
+  bl.w = __uint_as_float(right[i]);
+  out[4 * i + 0] = al;
+  out[4 * i + 1] = ah;
+  out[4 * i + 2] = bl;
+  out[4 * i + 3] = bh;
+}
+
+struct CollapseItem {
+  uint32_t bin;   // binary internal node to expand
+  uint32_t slot;  // BVH32 node slot it becomes
+};
+
+__device__ __forceinline__ float box_area(float4 l, float4 h) {
+  const float dx = fmaxf(h.x - l.x, 0.f), dy = fmaxf(h.y - l.y, 0.f), dz = fmaxf(h.z - l.z, 0.f);
+  return 2.f * (dx * dy + dy * dz + dz * dx);
+}
+
+// Greedy collapse of the binary tree into 32-wide nodes: starting from a binary node's two
+// children, repeatedly replace the largest-area child holding more than 32 Gaussians by its
+// two children until 32 slots are used.  Children with <= 32 Gaussians become leaves (one
+// contiguous Morton range, one lane per Gaussian); larger ones become the next level's nodes.
+__global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in,
+                           CollapseItem* __restrict__ out, unsigned int* __restrict__ out_count,
+                           unsigned int* __restrict__ slot_counter, const uint32_t* __restrict__ left,
+                           const uint32_t* __restrict__ right, const uint32_t* __restrict__ first,
+                           const uint32_t* __restrict__ last, const float4* __restrict__ plo,
+                           const float4* __restrict__ phi, const float4* __restrict__ nlo,
+                           const float4* __restrict__ nhi, float4* __restrict__ wide) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_items) return;
+  const CollapseItem it = in[t];
+  uint32_t refs[32];
+  int cnt = 2;
+  refs[0] = left[it.bin];
+  refs[1] = right[it.bin];
+  while (cnt < 32) {
+    int best = -1;
+    float best_a = -1.f;
+    for (int c = 0; c < cnt; ++c) {
+      const uint32_t r = refs[c];
+      if (ref_is_leaf(r)) continue;
+      if (last[r] - first[r] + 1u <= kLeafMax) continue;
+      const float a = box_area(nlo[r], nhi[r]);
+      if (a > best_a) {
+        best_a = a;
+        best = c;
+      }
+    }
+    if (best < 0) break;
+    const uint32_t r = refs[best];
+    refs[best] = left[r];
+    refs[cnt++] = right[r];
+  }
+  float4* node = wide + (size_t)it.slot * 64u;
+  for (int c = 0; c < 32; ++c) {
+    float4 l, h;
+    uint32_t wref;
+    if (c >= cnt) {
+      l = make_float4(INFINITY, INFINITY, INFINITY, __uint_as_float(kEmptyRef));
+      h = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+      node[c] = l;
+      node[32 + c] = h;
+      continue;
+    }
+    const uint32_t r = refs[c];
+    if (ref_is_leaf(r)) {
+      const uint32_t p = r & ~kLeafBit;
+      l = plo[p];
+      h = phi[p];
+      wref = wide_leaf_ref(p, 1u);
+    } else {
+      l = nlo[r];
+      h = nhi[r];
+      const uint32_t count = last[r] - first[r] + 1u;
+      if (count <= kLeafMax) {
+        wref = wide_leaf_ref(first[r], count);
+      } else {
+        const uint32_t slot = atomicAdd(slot_counter, 1u);
+        const uint32_t pos = atomicAdd(out_count, 1u);
+        out[pos] = CollapseItem{r, slot};
+        wref = slot;
+      }
+    }
+    l.w = __uint_as_float(wref);
+    h.w = 0.f;
+    node[c] = l;
+    node[32 + c] = h;
+  }
+}
+
+// Root of a scene with <= 32 Gaussians: one node holding one leaf.
+__global__ void k_single_leaf_root(uint32_t n, const float4* __restrict__ plo,
+                                   const float4* __restrict__ phi, float4* __restrict__ wide) {
+  const int c = threadIdx.x;
+  if (c >= 32) return;
+  if (c == 0) {
+    float4 l = make_float4(INFINITY, INFINITY, INFINITY, 0.f), h = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+    for (uint32_t i = 0; i < n; ++i) {
+      const float4 a = plo[i], b = phi[i];
+      l.x = fminf(l.x, a.x); l.y = fminf(l.y, a.y); l.z = fminf(l.z, a.z);
+      h.x = fmaxf(h.x, b.x); h.y = fmaxf(h.y, b.y); h.z = fmaxf(h.z, b.z);
+    }
+    l.w = __uint_as_float(wide_leaf_ref(0u, n));
+    wide[0] = l;
+    wide[32] = h;
+  } else {
+    wide[c] = make_float4(INFINITY, INFINITY, INFINITY, __uint_as_float(kEmptyRef));
+    wide[32 + c] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+  }
+}
+
+// One-Gaussian binary "tree": a root whose left child is the Gaussian and right is empty.
+__global__ void k_single_binary_root(const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                     float4* __restrict__ out) {
+  float4 l = plo[0];
+  l.w = __uint_as_float(kLeafBit | 0u);
+  out[0] = l;
+  out[1] = phi[0];
+  out[2] = make_float4(INFINITY, INFINITY, INFINITY, __uint_as_float(kEmptyRef));
+  out[3] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+}
+
+template <class T>
+struct Scratch {  // stream-ordered temporary, freed on scope exit
+  T* p = nullptr;
+  cudaStream_t s;
+  explicit Scratch(cudaStream_t st) : s(st) {}
+  ~Scratch() { dev_free(p, s); }
+};
+
+}  // namespace
+
+vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene* sc) {
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = g->count;
+  if (n == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "scene has no Gaussians");
+  if (n >= (1u << 26)) return fail(VP_ERROR_LIMIT, "scene exceeds 2^26 Gaussians");
+  if (!g->mean || !g->scale || !g->quat_wxyz || !g->density)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_gaussians: mean, scale, quat_wxyz and density are required");
+  if (!(sigma_multiplier > 0.f) || !std::isfinite(sigma_multiplier))
+    return fail(VP_ERROR_INVALID_ARGUMENT, "sigma_multiplier must be positive and finite");
+
+  VP_CUDA(cudaEventRecord(ctx->ev0, st));
+  // Inputs on the device.
+  Scratch<float> d_mean(st), d_scale(st), d_quat(st), d_dens(st), d_alb(st);
+  const float *mean = g->mean, *scale = g->scale, *quat = g->quat_wxyz, *dens = g->density,
+              *alb = g->albedo;
+  if (g->memory == VP_MEMORY_HOST) {
+    vp_status s;
+    if ((s = dev_alloc(&d_mean.p, 3ull * n, st))) return s;
+    if ((s = dev_alloc(&d_scale.p, 3ull * n, st))) return s;
+    if ((s = dev_alloc(&d_quat.p, 4ull * n, st))) return s;
+    if ((s = dev_alloc(&d_dens.p, 1ull * n, st))) return s;
+    VP_CUDA(cudaMemcpyAsync(d_mean.p, mean, 12ull * n, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(d_scale.p, scale, 12ull * n, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(d_quat.p, quat, 16ull * n, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(d_dens.p, dens, 4ull * n, cudaMemcpyHostToDevice, st));
+    mean = d_mean.p;
+    scale = d_scale.p;
+    quat = d_quat.p;
+    dens = d_dens.p;
+    if (alb) {
+      if ((s = dev_alloc(&d_alb.p, 3ull * n, st))) return s;
+      VP_CUDA(cudaMemcpyAsync(d_alb.p, alb, 12ull * n, cudaMemcpyHostToDevice, st));
+      alb = d_alb.p;
+    }
+  } else if (g->memory != VP_MEMORY_DEVICE) {
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_gaussians.memory must be VP_MEMORY_HOST or VP_MEMORY_DEVICE");
+  }
+
+  vp_status s;
+  Scratch<float4> rec0(st), lo0(st), hi0(st), plo(st), phi(st);
+  Scratch<ErrorWords> errw(st);
+  Scratch<unsigned int> bounds(st);
+  if ((s = dev_alloc(&rec0.p, 4ull * n, st))) return s;
+  if ((s = dev_alloc(&lo0.p, n, st))) return s;
+  if ((s = dev_alloc(&hi0.p, n, st))) return s;
+  if ((s = dev_alloc(&errw.p, 1, st))) return s;
+  if ((s = dev_alloc(&bounds.p, 12, st))) return s;
+  {
+    ErrorWords e0{0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, 0u};
+    VP_CUDA(cudaMemcpyAsync(errw.p, &e0, sizeof(e0), cudaMemcpyHostToDevice, st));
+    unsigned int b0[12];
+    for (int k = 0; k < 3; ++k) {
+      b0[k] = 0xFFFFFFFFu;
+      b0[3 + k] = 0u;
+      b0[6 + k] = 0xFFFFFFFFu;
+      b0[9 + k] = 0u;
+    }
+    VP_CUDA(cudaMemcpyAsync(bounds.p, b0, sizeof(b0), cudaMemcpyHostToDevice, st));
+  }
+  const int TB = 256;
+  const unsigned nb = (n + TB - 1) / TB;
+  k_precompute<<<nb, TB, 0, st>>>(n, mean, scale, quat, dens, alb, g->scale_is_log, sigma_multiplier,
+                                  rec0.p, lo0.p, hi0.p, errw.p);
+  VP_CUDA(cudaGetLastError());
+  k_bounds<<<std::min(nb, 1184u), TB, 0, st>>>(n, mean, lo0.p, hi0.p, bounds.p);
+  VP_CUDA(cudaGetLastError());
+  ErrorWords eh{};
+  unsigned int bh[12];
+  VP_CUDA(cudaMemcpyAsync(&eh, errw.p, sizeof(eh), cudaMemcpyDeviceToHost, st));
+  VP_CUDA(cudaMemcpyAsync(bh, bounds.p, sizeof(bh), cudaMemcpyDeviceToHost, st));
+  VP_CUDA(cudaStreamSynchronize(st));
+  if (eh.bad_scale != 0x7FFFFFFF)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "Gaussian " + std::to_string(eh.bad_scale) +
+                                               ": invalid scale - all components must be finite and > 0");
+  if (eh.bad_density != 0x7FFFFFFF)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "Gaussian " + std::to_string(eh.bad_density) +
+                                               ": invalid density - must be finite and > 0");
+  if (eh.bad_center != 0x7FFFFFFF)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "Gaussian " + std::to_string(eh.bad_center) +
+                                               ": NaN/Inf in centre or rotation");
+
+  // Morton codes + radix sort (stable: ties keep the caller's order).
+  Scratch<uint64_t> codes(st), codes_sorted(st);
+  Scratch<uint32_t> idx(st);
+  Scratch<unsigned char> cub_tmp(st);
+  uint32_t* perm = nullptr;
+  if ((s = dev_alloc(&codes.p, n, st))) return s;
+  if ((s = dev_alloc(&codes_sorted.p, n, st))) return s;
+  if ((s = dev_alloc(&idx.p, n, st))) return s;
+  if ((s = dev_alloc(&perm, n, st))) return s;
+  sc->perm = perm;
+  k_morton<<<nb, TB, 0, st>>>(n, mean, bounds.p, codes.p, idx.p);
+  VP_CUDA(cudaGetLastError());
+  size_t tmp_bytes = 0;
+  VP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, codes.p, codes_sorted.p, idx.p, perm,
+                                          (int)n, 0, 63, st));
+  if ((s = dev_alloc(&cub_tmp.p, tmp_bytes, st))) return s;
+  VP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp_bytes, codes.p, codes_sorted.p, idx.p, perm,
+                                          (int)n, 0, 63, st));
+  float4* prims = nullptr;
+  if ((s = dev_alloc(&prims, 4ull * n, st))) return s;
+  sc->prims = prims;
+  if ((s = dev_alloc(&plo.p, n, st))) return s;
+  if ((s = dev_alloc(&phi.p, n, st))) return s;
+  float4* pbox = nullptr;
+  if ((s = dev_alloc(&pbox, 2ull * n, st))) return s;
+  sc->pbox = pbox;
+  k_gather<<<nb, TB, 0, st>>>(n, perm, rec0.p, lo0.p, hi0.p, prims, plo.p, phi.p, pbox);
+  VP_CUDA(cudaGetLastError());
+
+  // Binary radix tree + refit.
+  const uint32_t ni = n > 1 ? n - 1 : 1;
+  Scratch<uint32_t> left(st), right(st), first(st), last(st), par_i(st), par_l(st);
+  Scratch<float4> nlo(st), nhi(st);
+  Scratch<unsigned int> flags(st);
+  if ((s = dev_alloc(&left.p, ni, st))) return s;
+  if ((s = dev_alloc(&right.p, ni, st))) return s;
+  if ((s = dev_alloc(&first.p, ni, st))) return s;
+  if ((s = dev_alloc(&last.p, ni, st))) return s;
+  if ((s = dev_alloc(&par_i.p, ni, st))) return s;
+  if ((s = dev_alloc(&par_l.p, n, st))) return s;
+  if ((s = dev_alloc(&nlo.p, ni, st))) return s;
+  if ((s = dev_alloc(&nhi.p, ni, st))) return s;
+  if ((s = dev_alloc(&flags.p, ni, st))) return s;
+  float4* bin = nullptr;
+  if ((s = dev_alloc(&bin, 4ull * ni, st))) return s;
+  sc->bin = bin;
+  if (n > 1) {
+    VP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned int) * ni, st));
+    k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted.p, left.p, right.p, first.p, last.p,
+                                                par_i.p, par_l.p);
+    VP_CUDA(cudaGetLastError());
+    k_refit<<<nb, TB, 0, st>>>((int)n, left.p, right.p, par_i.p, par_l.p, plo.p, phi.p, nlo.p, nhi.p, flags.p);
+    VP_CUDA(cudaGetLastError());
+    k_binary_nodes<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, left.p, right.p, plo.p, phi.p, nlo.p, nhi.p, bin);
+    VP_CUDA(cudaGetLastError());
+  } else {
+    k_single_binary_root<<<1, 1, 0, st>>>(plo.p, phi.p, bin);
+    VP_CUDA(cudaGetLastError());
+  }
+
+  // Collapse to BVH32.
+  // Upper bound on BVH32 nodes: childless nodes hold > 32 disjoint Gaussians (<= n/33), nodes
+  // with one node child hold 31 leaves of their own (<= n/31), branching nodes are fewer than
+  // childless ones (<= n/33).
+  const uint32_t max_wide = n / 31u + 2u * (n / 33u) + 4u;
+  float4* wide = nullptr;
+  if ((s = dev_alloc(&wide, 64ull * max_wide, st))) return s;
+  sc->wide = wide;
+  uint32_t depth = 1, wide_nodes = 1;
+  if (n <= kLeafMax) {
+    k_single_leaf_root<<<1, 32, 0, st>>>(n, plo.p, phi.p, wide);
+    VP_CUDA(cudaGetLastError());
+  } else {
+    Scratch<CollapseItem> qa(st), qb(st);
+    Scratch<unsigned int> ctr(st);
+    if ((s = dev_alloc(&qa.p, max_wide, st))) return s;
+    if ((s = dev_alloc(&qb.p, max_wide, st))) return s;
+    if ((s = dev_alloc(&ctr.p, 2, st))) return s;
+    CollapseItem root{0u, 0u};
+    VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    unsigned int c0[2] = {1u, 0u};  // [0] = next free slot, [1] = next-level queue length
+    VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
+    uint32_t n_items = 1;
+    depth = 0;
+    while (n_items > 0) {
+      ++depth;
+      VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
+      k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, left.p, right.p,
+                                                        first.p, last.p, plo.p, phi.p, nlo.p, nhi.p, wide);
+      VP_CUDA(cudaGetLastError());
+      unsigned int ch[2];
+      VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
+      VP_CUDA(cudaStreamSynchronize(st));
+      n_items = ch[1];
+      wide_nodes = ch[0];
+      std::swap(qa.p, qb.p);
+      if (wide_nodes > max_wide) return fail(VP_ERROR_INTERNAL, "BVH32 node budget exceeded");
+    }
+  }
+  if (wide_nodes < max_wide) {  // keep only the nodes in use
+    float4* tight = nullptr;
+    if ((s = dev_alloc(&tight, 64ull * wide_nodes, st))) return s;
+    VP_CUDA(cudaMemcpyAsync(tight, wide, 1024ull * wide_nodes, cudaMemcpyDeviceToDevice, st));
+    dev_free(wide, st);
+    wide = tight;
+    sc->wide = wide;
+  }
+  VP_CUDA(cudaEventRecord(ctx->ev1, st));
+  VP_CUDA(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  VP_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+
+  sc->ctx = ctx;
+  SceneView& v = sc->view;
+  v.prims = prims;
+  v.perm = perm;
+  v.wide = wide;
+  v.bin = bin;
+  v.pbox = pbox;
+  v.count = n;
+  v.wide_root = 0u;
+  v.bin_root = 0u;
+  v.stack_cap = 31u * depth + 2u;
+  v.albedo_all_zero = eh.any_albedo ? 0 : 1;
+  vp_scene_info& info = sc->info;
+  info.count = n;
+  info.wide_nodes = wide_nodes;
+  info.wide_depth = depth;
+  info.binary_nodes = n > 1 ? n - 1 : 1;
+  info.leaves = 0;
+  info.albedo_all_zero = v.albedo_all_zero;
+  info.build_ms = ms;
+  for (int k = 0; k < 3; ++k) {
+    auto o2f = [](unsigned int u) {
+      unsigned int b = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+      float f;
+      std::memcpy(&f, &b, 4);
+      return f;
+    };
+    info.bounds_min[k] = o2f(bh[6 + k]);
+    info.bounds_max[k] = o2f(bh[9 + k]);
+  }
+  info.device_bytes = 64ull * n + 4ull * n + 1024ull * wide_nodes + 64ull * ni;
+  return VP_OK;
+}
+
+}  // namespace vp

@@ -1,0 +1,97 @@
+// Host-side objects behind the opaque handles of include/volprim_b200.h, and the error
+// plumbing shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/volprim_b200.h"
+#include "vp_device.cuh"
+
+namespace vp {
+
+// Thread-local last error (vp_last_error_string).
+void set_error(const std::string& msg);
+vp_status fail(vp_status code, const std::string& msg);
+vp_status cuda_fail(cudaError_t e, const char* what);
+
+#define VP_CUDA(call)                                       \
+  do {                                                      \
+    cudaError_t _e = (call);                                \
+    if (_e != cudaSuccess) return ::vp::cuda_fail(_e, #call); \
+  } while (0)
+
+template <class T>
+vp_status dev_alloc(T** p, size_t count, cudaStream_t s) {
+  *p = nullptr;
+  if (count == 0) return VP_OK;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), count * sizeof(T), s);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    return fail(VP_ERROR_OUT_OF_MEMORY, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+  return VP_OK;
+}
+template <class T>
+void dev_free(T*& p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+  p = nullptr;
+}
+
+}  // namespace vp
+
+struct vp_context {
+  int32_t device = 0;
+  int32_t sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  vp::Counters* counters = nullptr;   // device, one block of statistics per render call
+  unsigned int* work_counter = nullptr;  // device, persistent-kernel work queue head
+};
+
+struct vp_scene {
+  vp_context* ctx = nullptr;
+  vp::SceneView view{};
+  float4* prims = nullptr;
+  uint32_t* perm = nullptr;
+  float4* wide = nullptr;
+  float4* bin = nullptr;
+  float4* pbox = nullptr;
+  vp_scene_info info{};
+};
+
+struct vp_env {
+  vp_context* ctx = nullptr;
+  vp::EnvView view{};
+  float4* texels = nullptr;
+  float2* cond = nullptr;
+  float2* marg = nullptr;
+  float* joint = nullptr;
+  double build_ms = 0.0;
+};
+
+struct vp_image {
+  vp_context* ctx = nullptr;
+  uint32_t width = 0, height = 0;
+  float4* mean = nullptr;
+  uint32_t* count = nullptr;
+};
+
+namespace vp {
+vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene* s);
+vp_status build_env(vp_context* ctx, const float* rgb, uint32_t w, uint32_t h, uint32_t channels,
+                    int32_t memory, vp_env* env);
+// Host restatement of host::params::Camera::build (camera.h:106-177).
+void build_camera(const vp_camera& cam, uint32_t width, uint32_t height, CameraView& out);
+ParamsView make_params(const vp_render_params& p, const vp_scene* s);
+vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const ParamsView& P,
+                        int32_t engine, vp_image* img, uint32_t spp_offset, uint32_t spp_count);
+vp_status launch_transmittance(vp_scene* s, const float* o, const float* d, uint32_t n,
+                               bool accurate, int32_t engine, float* out);
+vp_status launch_albedo(vp_scene* s, const float* pts, uint32_t n, bool accurate, int32_t engine, float* rgb,
+                        uint32_t* cnt);
+vp_status launch_normalize(const float4* in, float4* out, size_t n, float scale, cudaStream_t st);
+}  // namespace vp

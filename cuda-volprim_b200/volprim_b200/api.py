@@ -1,0 +1,367 @@
+"""Host-side mirror of the reference renderer's operator interface, over the C ABI.
+
+Reference interface (kfernandez31/cuda-volprim):
+  app::Config                        include/thesis/host/app/config.h:14-50
+  app::Renderer(config, primitives, camera) + render()
+                                     include/thesis/host/app/renderer.h:77-81,
+                                     src/thesis/host/app/renderer.cpp:34-439
+  host::params::Camera::createPerspective / createOrthographic / getDefaultCamera
+                                     include/thesis/host/params/camera.h:182-216
+  io::loadPrimitives (PLY semantics: log-scales, (w,x,y,z) quaternions, mass x sigma-multiplier)
+                                     src/thesis/host/utils/io/ply.cpp:21-175
+Differences: the image is returned in memory (H x W x 4 float32, alpha = 1) instead of written
+to an EXR file, errors raise VpError instead of exiting the process, and the scene has no
+65,535-Gaussian cap.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, lib
+
+
+def _is_cuda_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+def _host_f32(x, n: int, what: str) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).reshape(-1)
+    if a.size != n:
+        raise ValueError(f"{what}: expected {n} floats, got {a.size}")
+    return a
+
+
+class Context:
+    """One CUDA device + stream (vp_context_create)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.vp_context_create(int(device), C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib.vp_context_stream(self.handle, C.byref(s)))
+        return s.value or 0
+
+    @property
+    def sm_count(self) -> int:
+        n = C.c_int32()
+        check(lib.vp_context_sm_count(self.handle, C.byref(n)))
+        return n.value
+
+    def synchronize(self) -> None:
+        check(lib.vp_context_synchronize(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.vp_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Gaussians:
+    """Gaussian primitive buffers in the reference's PLY semantics (ply.cpp:99-118)."""
+
+    mean: object            # (N, 3)
+    scale: object           # (N, 3) linear (or log when scale_is_log)
+    quat_wxyz: object       # (N, 4) forward rotation, normalised by the library
+    density: object         # (N,) total mass M per Gaussian (multiplied by sigma_multiplier)
+    albedo: object = None   # (N, 3) or None
+    scale_is_log: bool = False
+
+    @property
+    def count(self) -> int:
+        return int(self.density.shape[0]) if hasattr(self.density, "shape") else len(self.density)
+
+
+class Scene:
+    """Gaussians + acceleration structure on the device (vp_scene_create)."""
+
+    def __init__(self, ctx: Context, g: Gaussians, sigma_multiplier: float = 1.0):
+        n = g.count
+        self.ctx = ctx
+        self._keep = []
+        s = _capi.vp_gaussians()
+        s.count = n
+        s.scale_is_log = 1 if g.scale_is_log else 0
+        if _is_cuda_tensor(g.density):
+            import torch
+
+            def dptr(t, k):
+                t = t.detach().to(torch.float32).contiguous().reshape(-1)
+                if t.numel() != k:
+                    raise ValueError("bad tensor size")
+                self._keep.append(t)
+                return t.data_ptr()
+
+            s.memory = _capi.VP_MEMORY_DEVICE
+            s.mean, s.scale = dptr(g.mean, 3 * n), dptr(g.scale, 3 * n)
+            s.quat_wxyz, s.density = dptr(g.quat_wxyz, 4 * n), dptr(g.density, n)
+            s.albedo = dptr(g.albedo, 3 * n) if g.albedo is not None else None
+        else:
+            arrs = [_host_f32(g.mean, 3 * n, "mean"), _host_f32(g.scale, 3 * n, "scale"),
+                    _host_f32(g.quat_wxyz, 4 * n, "quat_wxyz"), _host_f32(g.density, n, "density")]
+            alb = _host_f32(g.albedo, 3 * n, "albedo") if g.albedo is not None else None
+            self._keep = arrs + ([alb] if alb is not None else [])
+            s.memory = _capi.VP_MEMORY_HOST
+            s.mean, s.scale, s.quat_wxyz, s.density = (a.ctypes.data for a in arrs)
+            s.albedo = alb.ctypes.data if alb is not None else None
+        h = C.c_void_p()
+        check(lib.vp_scene_create(ctx.handle, C.byref(s), C.c_float(sigma_multiplier), C.byref(h)))
+        self.handle = h
+        self._keep = []
+
+    def info(self) -> dict:
+        i = _capi.vp_scene_info()
+        check(lib.vp_scene_info_get(self.handle, C.byref(i)))
+        return {
+            "count": i.count, "wide_nodes": i.wide_nodes, "wide_depth": i.wide_depth,
+            "binary_nodes": i.binary_nodes, "albedo_all_zero": bool(i.albedo_all_zero),
+            "build_ms": i.build_ms, "bounds_min": list(i.bounds_min), "bounds_max": list(i.bounds_max),
+            "device_bytes": i.device_bytes,
+        }
+
+    def transmittance(self, origins, dirs, precision: int = _capi.VP_PRECISION_AUTO,
+                      engine: int = _capi.VP_ENGINE_WARP):
+        """exp(-tau) along rays over [0, inf) (vp_transmittance)."""
+        if _is_cuda_tensor(origins):
+            import torch
+            o = origins.detach().to(torch.float32).contiguous()
+            d = dirs.detach().to(torch.float32).contiguous()
+            n = o.numel() // 3
+            out = torch.empty(n, dtype=torch.float32, device=o.device)
+            check(lib.vp_transmittance(self.handle, o.data_ptr(), d.data_ptr(), n, precision, engine,
+                                       out.data_ptr(), _capi.VP_MEMORY_DEVICE))
+            return out
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1)
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1)
+        n = o.size // 3
+        out = np.empty(n, dtype=np.float32)
+        check(lib.vp_transmittance(self.handle, o.ctypes.data, d.ctypes.data, n, precision, engine,
+                                   out.ctypes.data, _capi.VP_MEMORY_HOST))
+        return out
+
+    def albedo_at(self, points, precision: int = _capi.VP_PRECISION_AUTO, engine: int = _capi.VP_ENGINE_WARP):
+        """(albedo rgb (n, 3), overlap count (n,)) at points (vp_albedo_at)."""
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1)
+        n = p.size // 3
+        rgb = np.empty((n, 3), dtype=np.float32)
+        cnt = np.empty(n, dtype=np.uint32)
+        check(lib.vp_albedo_at(self.handle, p.ctypes.data, n, precision, engine, rgb.ctypes.data, cnt.ctypes.data,
+                               _capi.VP_MEMORY_HOST))
+        return rgb, cnt
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.vp_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Environment:
+    """Lat-long HDR environment + importance-sampling tables (vp_env_create)."""
+
+    def __init__(self, ctx: Context, rgb=None, constant=None):
+        h = C.c_void_p()
+        self.ctx = ctx
+        if constant is not None:
+            r, g, b = (float(v) for v in constant)
+            check(lib.vp_env_create_constant(ctx.handle, r, g, b, C.byref(h)))
+        else:
+            if _is_cuda_tensor(rgb):
+                import torch
+                t = rgb.detach().to(torch.float32).contiguous()
+                hgt, wid, ch = t.shape
+                check(lib.vp_env_create(ctx.handle, t.data_ptr(), wid, hgt, ch, _capi.VP_MEMORY_DEVICE,
+                                        C.byref(h)))
+            else:
+                a = np.ascontiguousarray(rgb, dtype=np.float32)
+                hgt, wid, ch = a.shape
+                check(lib.vp_env_create(ctx.handle, a.ctypes.data, wid, hgt, ch, _capi.VP_MEMORY_HOST,
+                                        C.byref(h)))
+        self.handle = h
+
+    @property
+    def build_ms(self) -> float:
+        v = C.c_double()
+        check(lib.vp_env_build_ms(self.handle, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.vp_env_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Camera:
+    """host::params::Camera (camera.h:84-228)."""
+
+    eye: tuple = (0.0, 0.0, -1.0)
+    lookat: tuple = (0.0, 0.0, 0.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    vfov_deg: float = 90.0
+    ortho_height: float = 2.0
+    orthographic: bool = False
+
+    @staticmethod
+    def perspective(origin, target, up, vertical_fov_deg: float) -> "Camera":
+        return Camera(tuple(origin), tuple(target), tuple(up), float(vertical_fov_deg), 2.0, False)
+
+    @staticmethod
+    def orthographic_camera(origin, target, up, ortho_height: float) -> "Camera":
+        return Camera(tuple(origin), tuple(target), tuple(up), 90.0, float(ortho_height), True)
+
+    @staticmethod
+    def default() -> "Camera":  # getDefaultCamera (camera.h:183-188)
+        return Camera()
+
+    def to_c(self) -> _capi.vp_camera:
+        c = _capi.vp_camera()
+        c.eye[:] = [float(v) for v in self.eye]
+        c.lookat[:] = [float(v) for v in self.lookat]
+        c.up[:] = [float(v) for v in self.up]
+        c.vfov_deg = self.vfov_deg
+        c.ortho_height = self.ortho_height
+        c.orthographic = 1 if self.orthographic else 0
+        return c
+
+
+@dataclass
+class Config:
+    """Render controls of app::Config (config.h:14-50) plus this library's engine choices."""
+
+    num_samples_per_pixel: int = 1
+    image_width: int = 1000
+    image_height: int = 750
+    seed: int = 42
+    max_bounces: int = 128
+    rr_depth: int = 12
+    rr_max_survival: float = 0.99
+    firefly_clamp_luminance: float = 0.0
+    pixel_filter_stddev: float = 0.0
+    hg_g: float = 0.85
+    use_ris: bool = False
+    ris_num_candidates: int = 6
+    measure_caps: bool = False
+    nee: str = "mis"            # "mis" | "phase" | "ris" | "none"  (use_ris=True selects "ris")
+    engine: str = "warp"        # "warp" | "megakernel"
+    precision: str = "auto"     # "auto" | "fast" | "accurate"
+    batch_spp: int = 16         # BATCH_SIZE (renderer.cpp:32)
+
+    def to_c(self) -> _capi.vp_render_params:
+        p = _capi.vp_render_params()
+        check(lib.vp_render_params_default(C.byref(p)))
+        p.width, p.height = self.image_width, self.image_height
+        p.spp, p.seed = self.num_samples_per_pixel, self.seed
+        p.max_bounces, p.rr_depth = self.max_bounces, self.rr_depth
+        p.rr_max_survival, p.hg_g = self.rr_max_survival, self.hg_g
+        p.firefly_clamp, p.pixel_filter_stddev = self.firefly_clamp_luminance, self.pixel_filter_stddev
+        nee = "ris" if self.use_ris else self.nee
+        p.nee_mode = {"mis": 0, "phase": 1, "ris": 2, "none": 3}[nee]
+        p.ris_candidates = self.ris_num_candidates
+        p.batch_spp = self.batch_spp
+        p.engine = {"warp": 0, "megakernel": 1}[self.engine]
+        p.precision = {"auto": 0, "fast": 1, "accurate": 2}[self.precision]
+        p.measure = 1 if self.measure_caps else 0
+        return p
+
+
+class Renderer:
+    """app::Renderer(config, primitives, camera) + render() over the C ABI.
+
+    `primitives` is a Gaussians record or an already-built Scene; `env` is an Environment, an
+    (H, W, C) array, or None for the constant white environment.
+    """
+
+    def __init__(self, config: Config, primitives, camera: Optional[Camera] = None, env=None,
+                 sigma_multiplier: float = 1.0, ctx: Optional[Context] = None):
+        self.config = config
+        self.ctx = ctx or (primitives.ctx if isinstance(primitives, Scene) else Context(0))
+        self.scene = primitives if isinstance(primitives, Scene) else Scene(self.ctx, primitives, sigma_multiplier)
+        if isinstance(env, Environment):
+            self.env = env
+        elif env is None:
+            self.env = Environment(self.ctx, constant=(1.0, 1.0, 1.0))
+        else:
+            self.env = Environment(self.ctx, rgb=env)
+        self.camera = camera or Camera.default()
+        self.last_stats: dict = {}
+
+    def render(self, out=None):
+        """Whole render; returns an (H, W, 4) float32 array (or fills the torch CUDA tensor `out`)."""
+        p = self.config.to_c()
+        cam = self.camera.to_c()
+        st = _capi.vp_render_stats()
+        if out is not None and _is_cuda_tensor(out):
+            check(lib.vp_render(self.scene.handle, self.env.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                _capi.VP_MEMORY_DEVICE, C.byref(st)))
+            self.last_stats = st.as_dict()
+            return out
+        img = np.empty((p.height, p.width, 4), dtype=np.float32)
+        check(lib.vp_render(self.scene.handle, self.env.handle, C.byref(cam), C.byref(p), img.ctypes.data,
+                            _capi.VP_MEMORY_HOST, C.byref(st)))
+        self.last_stats = st.as_dict()
+        return img
+
+
+class ProgressiveImage:
+    """Welford accumulation image (vp_image_*), for rendering sample ranges incrementally."""
+
+    def __init__(self, ctx: Context, width: int, height: int):
+        h = C.c_void_p()
+        check(lib.vp_image_create(ctx.handle, width, height, C.byref(h)))
+        self.handle, self.ctx, self.width, self.height = h, ctx, width, height
+
+    def clear(self):
+        check(lib.vp_image_clear(self.handle))
+
+    def accumulate(self, scene: Scene, env: Environment, camera: Camera, config: Config,
+                   spp_offset: int, spp_count: int) -> dict:
+        p = config.to_c()
+        cam = camera.to_c()
+        st = _capi.vp_render_stats()
+        check(lib.vp_render_accumulate(scene.handle, env.handle, C.byref(cam), C.byref(p), self.handle,
+                                       spp_offset, spp_count, C.byref(st)))
+        return st.as_dict()
+
+    def read(self) -> np.ndarray:
+        img = np.empty((self.height, self.width, 4), dtype=np.float32)
+        check(lib.vp_image_read(self.handle, img.ctypes.data, _capi.VP_MEMORY_HOST))
+        return img
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.vp_image_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,276 @@
+/*
+ * volprim_b200 — C ABI of the B200-native per-ray hot path of a volumetric path tracer for
+ * Gaussian kernel-mixture volumes (analog decomposition tracking + NEE/MIS + env importance
+ * sampling), with no OptiX.
+ *
+ * The reference renderer (kfernandez31/cuda-volprim) exposes this path only as a C++ facade:
+ *   app::Renderer(const Config&, std::vector<Primitive>&&, std::optional<Camera>) + render()
+ *   (include/thesis/host/app/renderer.h:77-81, src/thesis/host/app/renderer.cpp:34-439),
+ * plus one plain C-ABI kernel, launch_normalize_accumulator_kernel
+ *   (device/kernels/normalize_accumulator.h:11-13).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns vp_status: 0 = OK, negative = error.  The library never exits the
+ *    process (the reference's CUDA_CHECK/try_unwrap_or_exit call std::exit, check.h:16-72,
+ *    result.h:89-97); vp_last_error_string() returns the message of the calling thread's last
+ *    failure.
+ *  - Handles are opaque.  Host arrays passed in are copied; the caller keeps ownership.
+ *  - A context owns one CUDA stream; calls on one context are serialised by the caller.
+ *  - Pointers tagged with a vp_memory argument are host pointers (VP_MEMORY_HOST) or device
+ *    pointers on the context's device (VP_MEMORY_DEVICE).
+ */
+#ifndef VOLPRIM_B200_H
+#define VOLPRIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VP_VERSION_MAJOR 0
+#define VP_VERSION_MINOR 1
+
+typedef int32_t vp_status;
+enum {
+  VP_OK = 0,
+  VP_ERROR_INVALID_ARGUMENT = -1, /* bad pointer, size or parameter */
+  VP_ERROR_CUDA = -2,             /* a CUDA runtime call failed */
+  VP_ERROR_OUT_OF_MEMORY = -3,    /* device allocation failed */
+  VP_ERROR_UNSUPPORTED = -4,      /* option not supported by this build */
+  VP_ERROR_LIMIT = -5,            /* a size exceeds a documented limit */
+  VP_ERROR_DEVICE_STATUS = -6,    /* a kernel reported an error word (e.g. stack bound) */
+  VP_ERROR_INTERNAL = -7
+};
+
+typedef enum vp_memory { VP_MEMORY_HOST = 0, VP_MEMORY_DEVICE = 1 } vp_memory;
+
+/* Next-event estimator at a scatter vertex.  Replaces the compile-time ENABLE_NEE / ENABLE_MIS
+ * switches and the runtime --ris flag (device/core/constants.cuh:419,429; launch_params.h:43;
+ * device/entry/path_stages.cuh:394-472). */
+typedef enum vp_nee_mode {
+  VP_NEE_MIS = 0,   /* balance-heuristic MIS of phase-IS and env-IS, 2 shadow rays (default) */
+  VP_NEE_PHASE = 1, /* phase importance sampling only, 1 shadow ray */
+  VP_NEE_RIS = 2,   /* product RIS over ris_candidates env-IS candidates, 1 shadow ray */
+  VP_NEE_NONE = 3   /* pure analog: env gathered on escape only */
+} vp_nee_mode;
+
+/* Which GPU engine runs the path loop. */
+typedef enum vp_engine {
+  VP_ENGINE_WARP = 0,      /* persistent kernel, one path per warp, warp-cooperative BVH32 traversal */
+  VP_ENGINE_MEGAKERNEL = 1 /* plain per-pixel megakernel, thread-per-ray binary-LBVH traversal */
+} vp_engine;
+
+/* Precision of the per-(ray, Gaussian) chord set-up (whitening transform, closest approach,
+ * 3-sigma chord).  The erf/erfinv/exp evaluations are FP32 in both. */
+typedef enum vp_precision {
+  VP_PRECISION_AUTO = 0,    /* ACCURATE for absorption-only scenes (albedo == 0), else FAST */
+  VP_PRECISION_FAST = 1,    /* FP32 throughout */
+  VP_PRECISION_ACCURATE = 2 /* FP64 chord set-up; meets 1e-5 relative transmittance */
+} vp_precision;
+
+typedef struct vp_context vp_context;
+typedef struct vp_scene vp_scene;
+typedef struct vp_env vp_env;
+typedef struct vp_image vp_image;
+
+/* ---------------------------------------------------------------------------------------- */
+/* errors / version                                                                         */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Message of the calling thread's most recent failed call ("" if none).  Replaces the
+ * reference's Error/make_error (include/thesis/host/utils/result.h:86-101). */
+const char* vp_last_error_string(void);
+vp_status vp_version(int32_t* major, int32_t* minor);
+
+/* ---------------------------------------------------------------------------------------- */
+/* context                                                                                  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Binds a CUDA device and creates the context's stream.  Replaces cuda::Context + StreamDAG
+ * construction in Renderer::Renderer (src/thesis/host/app/renderer.cpp:34-51). */
+vp_status vp_context_create(int32_t device, vp_context** out);
+vp_status vp_context_destroy(vp_context* ctx);
+/* The context's cudaStream_t (as void*), for callers that order their own work after it. */
+vp_status vp_context_stream(vp_context* ctx, void** out_stream);
+vp_status vp_context_synchronize(vp_context* ctx);
+/* Number of streaming multiprocessors of the context's device. */
+vp_status vp_context_sm_count(vp_context* ctx, int32_t* out);
+
+/* ---------------------------------------------------------------------------------------- */
+/* scene: Gaussian primitives + acceleration structure                                       */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Gaussian primitive buffers in the reference's PLY semantics (src/thesis/host/utils/io/ply.cpp:
+ * 21-27,99-118): centre, per-axis scale (linear, or log when scale_is_log != 0, as the PLY
+ * stores it), forward rotation quaternion (w, x, y, z; normalised by the library), density =
+ * the primitive's total integrated mass M (multiplied by sigma_multiplier), RGB albedo
+ * (clamped to [0, 1], non-finite -> 0, as ply.cpp:124-145).  albedo may be NULL (= 0). */
+typedef struct vp_gaussians {
+  uint32_t count;
+  const float* mean;      /* [3 * count] */
+  const float* scale;     /* [3 * count] */
+  const float* quat_wxyz; /* [4 * count] */
+  const float* density;   /* [count] */
+  const float* albedo;    /* [3 * count] or NULL */
+  int32_t scale_is_log;
+  int32_t memory; /* vp_memory of all five arrays */
+} vp_gaussians;
+
+typedef struct vp_scene_info {
+  uint32_t count;           /* primitives */
+  uint32_t wide_nodes;      /* BVH32 nodes */
+  uint32_t wide_depth;      /* BVH32 depth (root = 1) */
+  uint32_t binary_nodes;    /* binary LBVH internal nodes */
+  uint32_t leaves;          /* BVH32 leaf ranges */
+  int32_t albedo_all_zero;  /* 1 when every albedo is 0 (absorption-only scene) */
+  double build_ms;          /* device time of the whole build (precompute, Morton, sort,
+                               hierarchy, refit, collapse), CUDA events */
+  double bounds_min[3];
+  double bounds_max[3];
+  uint64_t device_bytes;    /* device memory held by the scene */
+} vp_scene_info;
+
+/* Validates the primitives (positive finite scales, positive finite density, finite centres;
+ * ply.cpp:146-172), precomputes the per-primitive whitening record (primitive.h:70-87), builds
+ * the LBVH over 3-sigma ellipsoid bounds on the device (Morton codes, radix sort, Karras
+ * hierarchy, bottom-up refit, collapse to a 32-wide BVH).  Replaces Renderer::initPrimsAndGAS
+ * (renderer.cpp:85-173: host Morton sort + OptiX GAS/IAS build).  No primitive-count cap below
+ * 2^26 (the reference caps at 65,535, renderer.cpp:54-59). */
+vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* prims, float sigma_multiplier,
+                          vp_scene** out);
+vp_status vp_scene_info_get(vp_scene* scene, vp_scene_info* out);
+vp_status vp_scene_destroy(vp_scene* scene);
+
+/* ---------------------------------------------------------------------------------------- */
+/* environment map (lat-long, bilinear, wrap-U / clamp-V) + importance sampling              */
+/* ---------------------------------------------------------------------------------------- */
+
+/* rgb: width*height*channels floats, row-major, channels = 3 or 4.  Builds the luminance x
+ * sin(theta) sampling distribution in FP64 on the device as per-row alias tables plus a
+ * marginal alias table over rows.  Replaces host::params::EnvironmentMap (texture upload +
+ * FP32 host buildCdf, include/thesis/host/params/environment_map.h:45-151). */
+vp_status vp_env_create(vp_context* ctx, const float* rgb, uint32_t width, uint32_t height,
+                        uint32_t channels, int32_t memory, vp_env** out);
+/* Constant radiance (r, g, b) on a 2x1 map (the "white_constant" environment when r=g=b=1). */
+vp_status vp_env_create_constant(vp_context* ctx, float r, float g, float b, vp_env** out);
+/* Device time of the last env build in milliseconds. */
+vp_status vp_env_build_ms(vp_env* env, double* out_ms);
+vp_status vp_env_destroy(vp_env* env);
+
+/* ---------------------------------------------------------------------------------------- */
+/* camera + render parameters                                                               */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Mirrors host::params::Camera::createPerspective / createOrthographic
+ * (include/thesis/host/params/camera.h:106-216). */
+typedef struct vp_camera {
+  float eye[3];
+  float lookat[3];
+  float up[3];
+  float vfov_deg;      /* perspective vertical field of view */
+  float ortho_height;  /* orthographic viewport height */
+  int32_t orthographic;
+} vp_camera;
+
+/* Mirrors app::Config's render controls (include/thesis/host/app/config.h:14-50) and
+ * RenderParams (include/thesis/common/params/launch_params.h:37-59). */
+typedef struct vp_render_params {
+  uint32_t width;
+  uint32_t height;
+  uint32_t spp;            /* --spp */
+  uint32_t seed;           /* --seed (launch seed of every PCG32 stream) */
+  uint32_t max_bounces;    /* --max-depth (default 128) */
+  uint32_t rr_depth;       /* --rr-depth (default 12) */
+  float rr_max_survival;   /* --rr-max-survival (default 0.99) */
+  float hg_g;              /* --phase-g (default 0.85; |g| < 1e-3 is isotropic) */
+  float firefly_clamp;     /* --firefly-clamp (0 = off) */
+  float pixel_filter_stddev; /* --filter-width (0 = box) */
+  int32_t nee_mode;        /* vp_nee_mode */
+  uint32_t ris_candidates; /* --ris-candidates (default 6) */
+  uint32_t batch_spp;      /* samples per launch (reference BATCH_SIZE = 16) */
+  int32_t engine;          /* vp_engine */
+  int32_t precision;       /* vp_precision */
+  int32_t measure;         /* 1: count crossings/bounces/shadow rays and maxima (costs atomics) */
+} vp_render_params;
+
+/* Fills the reference's defaults (config.h:119-136, launch_params.h:38-58). */
+vp_status vp_render_params_default(vp_render_params* out);
+
+typedef struct vp_render_stats {
+  double ms_kernels;           /* device time of the render launches (CUDA events) */
+  uint64_t paths;              /* width * height * spp */
+  uint64_t bounces;            /* scatter-or-escape events        (measure != 0) */
+  uint64_t scatters;           /* events that scattered           (measure != 0) */
+  uint64_t crossings;          /* closed-form (ray, Gaussian) evaluations (measure != 0) */
+  uint64_t shadow_rays;        /* transmittance queries           (measure != 0) */
+  uint64_t nodes_visited;      /* inner BVH node visits           (measure != 0) */
+  uint64_t leaves_visited;     /* BVH32 leaf visits (warp engine) (measure != 0) */
+  uint64_t prim_tests;         /* Gaussian 3-sigma boxes tested at BVH32 leaves (measure != 0) */
+  uint64_t geo_loads;          /* Gaussian whitening records loaded for a chord or point test
+                                  (box hits)                      (measure != 0) */
+  uint32_t max_hits_per_ray;   /* largest candidate count of one query (measure != 0) */
+  uint32_t max_point_overlap;  /* largest Gaussian overlap at a path vertex (measure != 0) */
+  uint32_t device_status;      /* 0 = fine; else an error word raised by a kernel */
+  uint32_t reserved;
+} vp_render_stats;
+
+/* ---------------------------------------------------------------------------------------- */
+/* rendering                                                                                */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Progressive Welford image (float4 mean + uint32 count per pixel).  Replaces
+ * host::params::Image (include/thesis/host/params/image.h) and device::params::Image
+ * (include/thesis/device/params/image.h:15-38). */
+vp_status vp_image_create(vp_context* ctx, uint32_t width, uint32_t height, vp_image** out);
+vp_status vp_image_clear(vp_image* image);
+vp_status vp_image_destroy(vp_image* image);
+/* Copies the mean (RGBA float32, alpha = 1) to out (host or device memory). */
+vp_status vp_image_read(vp_image* image, float* out_rgba, int32_t memory);
+/* Raw device pointers (float4 mean[W*H], uint32 count[W*H]). */
+vp_status vp_image_device_buffers(vp_image* image, void** mean, void** count);
+
+/* Renders samples [spp_offset, spp_offset + spp_count) of a params->spp-sample render into
+ * image (Welford update).  Replaces one Renderer::render batch iteration
+ * (renderer.cpp:353-376 -> optixLaunch of __raygen__rg, device/entry/raygen.cuh:21-243). */
+vp_status vp_render_accumulate(vp_scene* scene, vp_env* env, const vp_camera* camera,
+                               const vp_render_params* params, vp_image* image,
+                               uint32_t spp_offset, uint32_t spp_count, vp_render_stats* stats);
+
+/* Whole render: all params->spp samples in batches of params->batch_spp, then the mean is
+ * written to out_rgba (width*height*4 floats, host or device).  Replaces Renderer::render
+ * (renderer.cpp:341-439) minus the EXR write.  stats may be NULL. */
+vp_status vp_render(vp_scene* scene, vp_env* env, const vp_camera* camera,
+                    const vp_render_params* params, float* out_rgba, int32_t memory,
+                    vp_render_stats* stats);
+
+/* Transmittance exp(-tau) along n rays (origin, unit direction) over [0, inf), each summing
+ * the 3-sigma-truncated closed-form optical depth of every Gaussian the ray overlaps.
+ * Replaces compute_transmittance_to_env (device/core/sampling.cuh:548-583) with its any-hit
+ * TRANSMITTANCE fusion (device/entry/anyhit.cuh:53-66).  Arrays: origins[3n], dirs[3n],
+ * out_transmittance[n]; precision as vp_precision; engine as vp_engine. */
+vp_status vp_transmittance(vp_scene* scene, const float* origins, const float* dirs, uint32_t n,
+                           int32_t precision, int32_t engine, float* out_transmittance,
+                           int32_t memory);
+
+/* Albedo at n points: the sigma_t * pdf-weighted mean albedo of the Gaussians whose 3-sigma
+ * ellipsoid contains each point, and how many contain it.  Replaces evaluate_albedo over the
+ * active set (device/core/sampling.cuh:257-283, 422-458) and point_inside_bvh_bound
+ * (include/thesis/common/geometry/intersection.h:56-61).  points[3n], out_rgb[3n] (0 where no
+ * Gaussian contains the point), out_overlap[n]. */
+vp_status vp_albedo_at(vp_scene* scene, const float* points, uint32_t n, int32_t precision,
+                       int32_t engine, float* out_rgb, uint32_t* out_overlap, int32_t memory);
+
+/* Grid-stride copy out[i] = accumulator[i] * normalization_factor over n float4 pixels on the
+ * context's stream (or `stream` when non-NULL).  Same contract as the reference's
+ * launch_normalize_accumulator_kernel (device/kernels/normalize_accumulator.cu:27-35). */
+vp_status vp_normalize_accumulator(vp_context* ctx, float* out_pixels, const float* accumulator,
+                                   size_t n_pixels, float normalization_factor, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOLPRIM_B200_H */

@@ -1,0 +1,79 @@
+// ORACLE pin (test infrastructure only): a C-ABI shim over the reference's OWN host-compilable
+// headers, compiled from /root/reference/include by oracle/Makefile into _ref/libref_pin.so.
+// It exposes the reference's Primitive constructor and whitening transforms
+// (include/thesis/device/params/primitive.h:70-122), the 3-sigma containment test
+// (include/thesis/common/geometry/intersection.h:56-61), the host camera build
+// (include/thesis/host/params/camera.h:106-216) and the Morton code
+// (include/thesis/host/utils/math.h:103-131), so the oracle's restatement of them can be checked
+// against the reference's code itself.  The device-only parts of the path (OptiX programs,
+// sampling.cuh) need the OptiX SDK and are not built here.
+// <cstdint> first: the reference's own build provides it through its precompiled header.
+#include <cstdint>
+
+#include "thesis/device/params/primitive.h"
+#include "thesis/common/geometry/intersection.h"
+#include "thesis/host/params/camera.h"
+#include "thesis/host/utils/math.h"
+
+#include <cstring>
+
+using thesis::common::geometry::UnitQuaternion;
+using thesis::device::params::Primitive;
+
+extern "C" {
+
+// out20: center[3], rot_quat(s, u[3]) (stored conjugate), rcp_scale[3], density_norm_factor,
+// inv_cdf_factor, albedo[3], optical_thickness, scale[3], 0
+void ref_primitive(const float* mean3, const float* scale3, const float* quat_wxyz, const float* albedo3,
+                   float optical_thickness, float* out20) {
+  const Primitive p = Primitive::from_forward_quat(
+      make_float3(mean3[0], mean3[1], mean3[2]),
+      UnitQuaternion::from(quat_wxyz[0], quat_wxyz[1], quat_wxyz[2], quat_wxyz[3]),
+      make_float3(scale3[0], scale3[1], scale3[2]), make_float3(albedo3[0], albedo3[1], albedo3[2]),
+      optical_thickness);
+  const float v[20] = {p.center_.x, p.center_.y, p.center_.z, p.rot_quat_.s_, p.rot_quat_.u_.x,
+                       p.rot_quat_.u_.y, p.rot_quat_.u_.z, p.rcp_scale_.x, p.rcp_scale_.y, p.rcp_scale_.z,
+                       p.density_norm_factor_, p.inv_cdf_factor_, p.albedo_.x, p.albedo_.y, p.albedo_.z,
+                       p.optical_thickness_, p.scale_.x, p.scale_.y, p.scale_.z, 0.0f};
+  std::memcpy(out20, v, sizeof(v));
+}
+
+// Whitened position and direction + point_inside_bvh_bound for one Gaussian.
+// out7: pos_local[3], dir_local[3], inside (0/1)
+void ref_transform(const float* mean3, const float* scale3, const float* quat_wxyz, float optical_thickness,
+                   const float* pos3, const float* dir3, float* out7) {
+  const Primitive p = Primitive::from_forward_quat(
+      make_float3(mean3[0], mean3[1], mean3[2]),
+      UnitQuaternion::from(quat_wxyz[0], quat_wxyz[1], quat_wxyz[2], quat_wxyz[3]),
+      make_float3(scale3[0], scale3[1], scale3[2]), make_float3(0.f, 0.f, 0.f), optical_thickness);
+  const float3 a = p.transform_pos_local(make_float3(pos3[0], pos3[1], pos3[2]));
+  const float3 b = p.transform_dir_local(make_float3(dir3[0], dir3[1], dir3[2]));
+  const bool in = thesis::common::geometry::point_inside_bvh_bound(make_float3(pos3[0], pos3[1], pos3[2]), p);
+  const float v[7] = {a.x, a.y, a.z, b.x, b.y, b.z, in ? 1.0f : 0.0f};
+  std::memcpy(out7, v, sizeof(v));
+}
+
+// out16: eye[3], pixel00_relative[3], pixel_du[3], pixel_dv[3], view_direction[3], ortho
+void ref_camera(const float* eye3, const float* lookat3, const float* up3, float vfov_deg, float ortho_height,
+                int orthographic, unsigned width, unsigned height, float* out16) {
+  const auto o = make_float3(eye3[0], eye3[1], eye3[2]);
+  const auto t = make_float3(lookat3[0], lookat3[1], lookat3[2]);
+  const auto u = make_float3(up3[0], up3[1], up3[2]);
+  const auto cam = orthographic
+                       ? thesis::host::params::Camera::createOrthographic(width, height, o, t, u, ortho_height)
+                       : thesis::host::params::Camera::createPerspective(width, height, o, t, u, vfov_deg);
+  const auto& d = cam.device_camera();
+  const float v[16] = {d.eye_.x, d.eye_.y, d.eye_.z, d.pixel00_relative_.x, d.pixel00_relative_.y,
+                       d.pixel00_relative_.z, d.pixel_du_.x, d.pixel_du_.y, d.pixel_du_.z, d.pixel_dv_.x,
+                       d.pixel_dv_.y, d.pixel_dv_.z, d.view_direction_.x, d.view_direction_.y,
+                       d.view_direction_.z, d.is_orthographic_ ? 1.0f : 0.0f};
+  std::memcpy(out16, v, sizeof(v));
+}
+
+unsigned ref_morton3d(const float* pos3, const float* scene_min3, const float* inv_extent3) {
+  return thesis::host::utils::math::morton3D(make_float3(pos3[0], pos3[1], pos3[2]),
+                                             make_float3(scene_min3[0], scene_min3[1], scene_min3[2]),
+                                             make_float3(inv_extent3[0], inv_extent3[1], inv_extent3[2]));
+}
+
+}  // extern "C"

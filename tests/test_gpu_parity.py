@@ -1,0 +1,307 @@
+"""GPU parity of the CUDA path (through the C ABI) against the oracle.
+
+Tolerances:
+  * transmittance / absorption images vs the FP64 closed form (ACCURATE set-up):
+      |T - T64| <= 1e-5 * T64 where T64 >= 1e-4, else |T - T64| <= 1e-9   (the stated gate)
+  * FAST (FP32 set-up) transmittance: |T - T64| <= 2e-4 * T64 + 1e-8
+  * scattering vs the oracle with the same keyed free-flight draws: per-pixel relative difference
+    below 1e-3 on >= 97% of pixels and mean relative difference below 2e-4
+  * scattering vs the oracle with the reference's sequential draws: seed-stack z-scores with
+    |mean z| < 0.15, 0.75 < std z < 1.3, and relative mean-image difference < 1%
+  * white furnace (albedo 1, unit environment): |bias| < max(5 SEM, 2e-3) and 33x33-blurred
+    structure below 3e-3 (experiments/mitsuba-reference/furnace_check.py:33-40)
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import volprim_b200 as vp
+from volprim_b200 import scenes
+from volprim_b200._capi import (VP_ENGINE_MEGAKERNEL, VP_ENGINE_WARP, VP_PRECISION_ACCURATE,
+                                VP_PRECISION_FAST)
+
+pytestmark = pytest.mark.gpu
+
+
+def gate_T(T, T64, rel=1e-5, floor=1e-4, abs_below=1e-9):
+    T = np.asarray(T, np.float64)
+    err = np.abs(T - T64)
+    ok = np.where(T64 >= floor, err <= rel * T64, err <= abs_below)
+    return ok, err
+
+
+def random_rays(rng, n, radius=3.5, inside_frac=0.0):
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    # origins on a sphere, aimed roughly at the cloud, plus some inside the cloud
+    o = rng.normal(size=(n, 3))
+    o = radius * o / np.linalg.norm(o, axis=1, keepdims=True)
+    aim = rng.uniform(-0.8, 0.8, (n, 3)) - o
+    aim /= np.linalg.norm(aim, axis=1, keepdims=True)
+    k = int(inside_frac * n)
+    o[:k] = rng.uniform(-1, 1, (k, 3))
+    aim[:k] = d[:k]
+    return o.astype(np.float32), (aim / np.linalg.norm(aim, axis=1, keepdims=True)).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def scene256(vp_ctx):
+    g = scenes.absorption_gaussians(256, 0)
+    return vp.Scene(vp_ctx, g), O.OracleScene.from_gaussians(g), g
+
+
+@pytest.mark.parametrize("engine", [VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL])
+def test_transmittance_accurate_vs_fp64(scene256, engine):
+    sc, osc, _ = scene256
+    o, d = random_rays(np.random.default_rng(1), 20000)
+    T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=engine)
+    T64, _ = osc.transmittance_fp64(o, d)
+    ok, err = gate_T(T, T64)
+    assert (T64 < 0.999).sum() > 2000, "rays must actually cross Gaussians"
+    assert ok.all(), f"{(~ok).sum()} rays fail; worst rel {np.max(err / np.maximum(T64, 1e-30)):.3e}"
+
+
+@pytest.mark.parametrize("engine", [VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL])
+def test_transmittance_inside_origins(scene256, engine):
+    sc, osc, _ = scene256
+    o, d = random_rays(np.random.default_rng(2), 20000, inside_frac=1.0)
+    T64, _ = osc.transmittance_fp64(o, d)
+    for prec, tol in ((VP_PRECISION_ACCURATE, 2e-5), (VP_PRECISION_FAST, 2e-4)):
+        T = sc.transmittance(o, d, precision=prec, engine=engine).astype(np.float64)
+        err = np.abs(T - T64)
+        assert np.all(err <= tol * T64 + 1e-8), (prec, np.max(err / np.maximum(T64, 1e-30)))
+
+
+def test_fast_transmittance_vs_fp64(scene256):
+    sc, osc, _ = scene256
+    o, d = random_rays(np.random.default_rng(3), 20000)
+    T = sc.transmittance(o, d, precision=VP_PRECISION_FAST).astype(np.float64)
+    T64, _ = osc.transmittance_fp64(o, d)
+    assert np.all(np.abs(T - T64) <= 2e-4 * T64 + 1e-8)
+
+
+def test_single_gaussian_closed_form(vp_ctx):
+    """single_gaussian_validation: unit isotropic Gaussian of mass M, rays along +z at
+    perpendicular distance d -> tau(d) = M/(2 pi) exp(-d^2/2) erf(sqrt((9 - d^2)/2))
+    (3-sigma-truncated form of experiments/mitsuba-reference/single_gaussian_analytic.py:78-80)."""
+    M = 7.5
+    g = vp.Gaussians(np.zeros((1, 3)), np.ones((1, 3)), np.array([[1.0, 0, 0, 0]]), np.array([M]))
+    sc = vp.Scene(vp_ctx, g)
+    dd = np.linspace(0.0, 2.95, 60).astype(np.float32)
+    o = np.stack([dd, np.zeros_like(dd), np.full_like(dd, -5.0)], 1)
+    dirs = np.tile(np.array([0, 0, 1.0], np.float32), (60, 1))
+    dd64 = dd.astype(np.float64)
+    tau = M / (2 * math.pi) * np.exp(-dd64 ** 2 / 2) * np.array([math.erf(math.sqrt((9 - x * x) / 2)) for x in dd64])
+    for prec in (VP_PRECISION_ACCURATE, VP_PRECISION_FAST):
+        for eng in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+            T = sc.transmittance(o, dirs, precision=prec, engine=eng).astype(np.float64)
+            np.testing.assert_allclose(-np.log(T), tau, rtol=2e-6, atol=2e-7)
+
+
+@pytest.mark.parametrize("engine", ["warp", "megakernel"])
+def test_absorption_image_matches_fp64(vp_ctx, engine):
+    """128x128x16 absorption render of the 256-Gaussian workload vs the FP64 oracle, replaying
+    the reference's PCG32 jitter stream per (pixel, sample)."""
+    w = scenes.absorption_256()
+    w.config.engine = engine
+    r = vp.Renderer(w.config, w.gaussians, w.camera, env=None, ctx=vp_ctx)
+    img = r.render()[..., :3].astype(np.float64)
+    osc = O.OracleScene.from_gaussians(w.gaussians, use_bvh=True)
+    env = O.OracleEnv.constant()
+    c16 = O.camera16(w.camera, 128, 128)
+    ref = O.render_absorption_fp64(osc, env, c16, 128, 128, 16, w.config.seed)
+    ok, err = gate_T(img, ref)
+    assert ref.min() < 1e-3 and ref.max() > 0.999, "image must span opaque and clear pixels"
+    assert ok.all(), f"{(~ok).sum()} pixel channels fail; worst rel {np.max(err / np.maximum(ref, 1e-30)):.3e}"
+    assert r.last_stats["device_status"] == 0
+
+
+def small_scatter_workload(seed=3, n=400, res=32, spp=64, env=True, albedo=0.9, nee="mis", hg=0.0):
+    rng = np.random.default_rng(seed)
+    mean = rng.uniform(-0.6, 0.6, (n, 3)).astype(np.float32)
+    scale = np.exp(rng.normal(math.log(0.12), 0.3, (n, 3))).astype(np.float32)
+    quat = scenes.uniform_quaternions(rng, n)
+    dens = np.exp(rng.normal(0.0, 0.5, n)).astype(np.float32)
+    alb = np.clip(albedo * rng.uniform(0.7, 1.0, (n, 3)), 0, 1).astype(np.float32)
+    g = vp.Gaussians(mean, scale, quat, dens, alb)
+    cfg = vp.Config(num_samples_per_pixel=spp, image_width=res, image_height=res, seed=seed, hg_g=hg,
+                    max_bounces=64, rr_depth=12, nee=nee)
+    envimg = scenes.procedural_env(64, 32, sun_radiance=50.0, sun_radius_deg=8.0) if env else None
+    return g, cfg, envimg
+
+
+def _render_both(vp_ctx, g, cfg, envimg, sigma=2.0, rng_mode="keyed", engine="warp"):
+    cfg.engine = engine
+    cam = scenes.negz_camera(3.0, 40.0)
+    r = vp.Renderer(cfg, g, cam, env=envimg, sigma_multiplier=sigma, ctx=vp_ctx)
+    img = r.render()[..., :3]
+    osc = O.OracleScene.from_gaussians(g, sigma_multiplier=sigma)
+    oenv = O.OracleEnv(envimg) if envimg is not None else O.OracleEnv.constant()
+    ref, _ = O.render(osc, oenv, O.camera16(cam, cfg.image_width, cfg.image_height), cfg, rng_mode=rng_mode)
+    return img, ref, r.last_stats
+
+
+@pytest.mark.parametrize("nee", ["mis", "phase", "ris", "none"])
+def test_scatter_matches_keyed_oracle(vp_ctx, nee):
+    g, cfg, env = small_scatter_workload(nee=nee, hg=0.3 if nee == "phase" else 0.0)
+    img, ref, st = _render_both(vp_ctx, g, cfg, env)
+    assert st["device_status"] == 0
+    scale = max(float(ref.mean()), 1e-6)
+    rel = np.abs(img - ref) / np.maximum(np.abs(ref), 0.05 * scale)
+    assert ref.mean() > 0.01
+    assert np.mean(rel < 1e-3) >= 0.97, f"only {np.mean(rel < 1e-3):.3f} of pixels within 1e-3"
+    assert np.abs(img - ref).mean() / scale < 2e-4
+
+
+def test_engines_agree(vp_ctx):
+    g, cfg, env = small_scatter_workload(seed=5, spp=32)
+    cam = scenes.negz_camera(3.0, 40.0)
+    imgs = []
+    for eng in ("warp", "megakernel"):
+        cfg.engine = eng
+        imgs.append(vp.Renderer(cfg, g, cam, env=env, sigma_multiplier=2.0, ctx=vp_ctx).render()[..., :3])
+    scale = float(imgs[0].mean())
+    assert np.abs(imgs[0] - imgs[1]).mean() / scale < 1e-4
+
+
+def test_scatter_statistical_vs_reference_order(vp_ctx):
+    """Seed stack: GPU (keyed draws, alias-table env sampling) vs the oracle with the reference's
+    sequential free-flight draws and CDF env sampling."""
+    seeds = range(6)
+    ga, gb = [], []
+    for s in seeds:
+        g, cfg, env = small_scatter_workload(seed=11, res=24, spp=32)
+        cfg.seed = 100 + s
+        img, ref, _ = _render_both(vp_ctx, g, cfg, env, rng_mode="sequential")
+        ga.append(img)
+        gb.append(ref)
+    A, B = np.stack(ga), np.stack(gb)
+    ma, mb = A.mean(0), B.mean(0)
+    se = np.sqrt(A.var(0, ddof=1) / len(seeds) + B.var(0, ddof=1) / len(seeds))
+    z = ((ma - mb) / np.maximum(se, 1e-12))[se > 1e-6]
+    assert abs(z.mean()) < 0.15, z.mean()
+    assert 0.75 < z.std() < 1.3, z.std()
+    assert abs(ma.mean() - mb.mean()) / mb.mean() < 0.01
+
+
+def _furnace(vp_ctx, g, sigma, cam, nee="mis", hg=0.0, engine="warp", spp=256):
+    cfg = vp.Config(num_samples_per_pixel=spp, image_width=64, image_height=64, seed=1, hg_g=hg,
+                    max_bounces=1024, nee=nee, engine=engine)
+    img = vp.Renderer(cfg, g, cam, env=None, sigma_multiplier=sigma, ctx=vp_ctx).render()[..., :3].astype(np.float64)
+    d = img - 1.0
+    mean = img.mean()
+    sem = img.std() / math.sqrt(img.size)
+    from scipy.ndimage import uniform_filter
+    worst = np.abs(uniform_filter(d.mean(-1), size=33)).max()
+    assert abs(mean - 1.0) < max(5 * sem, 2e-3), (mean, sem)
+    assert worst < 3e-3, worst
+
+
+@pytest.mark.parametrize("nee,hg,engine", [("mis", 0.0, "warp"), ("mis", 0.6, "warp"), ("phase", 0.0, "warp"),
+                                           ("ris", 0.0, "warp"), ("none", 0.0, "warp"), ("mis", 0.0, "megakernel")])
+def test_white_furnace_cluster(vp_ctx, nee, hg, engine):
+    """Albedo 1 everywhere in a unit constant environment: every pixel must be 1
+    (Russian roulette from depth 12 keeps it unbiased)."""
+    rng = np.random.default_rng(7)
+    n = 200
+    g = vp.Gaussians(rng.uniform(-0.5, 0.5, (n, 3)), np.exp(rng.normal(math.log(0.2), 0.3, (n, 3))),
+                     scenes.uniform_quaternions(rng, n), np.exp(rng.normal(0, 0.5, n)), np.ones((n, 3)))
+    _furnace(vp_ctx, g, 0.02, scenes.negz_camera(3.0, 40.0), nee=nee, hg=hg, engine=engine)
+
+
+def test_white_furnace_single_gaussian(vp_ctx):
+    """The reference's furnace scene: one unit isotropic Gaussian, M = 7.5, albedo 1, orthographic
+    view of [-3, 3]^2 (test/scenes/single_gaussian.cpp:95-176 with SG_ALBEDO=1)."""
+    g = vp.Gaussians(np.zeros((1, 3)), np.ones((1, 3)), np.array([[1.0, 0, 0, 0]]), np.array([7.5]), np.ones((1, 3)))
+    cam = vp.Camera.orthographic_camera((0, 0, -5), (0, 0, 0), (0, 1, 0), 6.0)
+    _furnace(vp_ctx, g, 1.0, cam)
+
+
+@pytest.fixture(scope="module")
+def showcase(vp_ctx):
+    g = scenes.showcase_gaussians(500_000, 0)
+    return g, vp.Scene(vp_ctx, g, 7.5), O.OracleScene.from_gaussians(g, sigma_multiplier=7.5, use_bvh=True)
+
+
+@pytest.mark.parametrize("engine", [VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL])
+def test_showcase_point_queries(showcase, engine):
+    """BVH point queries at 500k scale: ellipsoid overlap counts and albedo at Gaussian centres and
+    random points equal the oracle's (brute containment over CPU-BVH candidates)."""
+    g, sc, osc = showcase
+    rng = np.random.default_rng(5)
+    pts = np.concatenate([g.mean[rng.choice(len(g.density), 3000, replace=False)],
+                          rng.uniform([-1, -0.5, -0.5], [1, 0.5, 0.5], (3000, 3))]).astype(np.float32)
+    rgb, cnt = sc.albedo_at(pts, engine=engine)
+    orgb, ocnt = osc.albedo_at(pts)
+    assert ocnt.max() > 300
+    diff = np.abs(cnt.astype(np.int64) - ocnt.astype(np.int64))
+    assert diff.max() <= 1 and np.mean(diff > 0) < 1e-3, (diff.max(), np.mean(diff > 0))
+    np.testing.assert_allclose(rgb, orgb, atol=1e-5)
+
+
+def test_showcase_transmittance(showcase):
+    g, sc, osc = showcase
+    rng = np.random.default_rng(6)
+    o, d = random_rays(rng, 3000, radius=3.0, inside_frac=0.3)
+    k = int(0.3 * 3000)
+    o[:k] = g.mean[rng.choice(len(g.density), k, replace=False)]
+    T64, tau64 = osc.transmittance_fp64(o, d)
+    for eng in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+        T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=eng).astype(np.float64)
+        Tf = sc.transmittance(o, d, precision=VP_PRECISION_FAST, engine=eng).astype(np.float64)
+        sel = tau64 < 80  # beyond, the GPU stops at tau >= 88 and reports 0
+        assert np.all(np.abs(T - T64)[sel] <= 2e-5 * T64[sel] + 1e-9), eng
+        assert np.all(np.abs(Tf - T64)[sel] <= 1e-3 * T64[sel] + 1e-7), eng
+        assert np.all(T[tau64 > 90] == 0.0)
+
+
+def test_dense_overlap_no_caps(vp_ctx):
+    """A collinear stack of 300 unit Gaussians (the reference's cluster 'stress' layout with K
+    beyond its 128 hit-buffer / active-set caps): transmittance along the axis must still equal
+    the FP64 sum over all of them."""
+    K = 300
+    z = np.linspace(-1.5, 1.5, K).astype(np.float32)
+    mean = np.stack([np.zeros(K), np.zeros(K), z], 1).astype(np.float32)
+    g = vp.Gaussians(mean, np.ones((K, 3), np.float32), np.tile([1.0, 0, 0, 0], (K, 1)),
+                     np.full(K, 10.0 / K, np.float32))
+    sc = vp.Scene(vp_ctx, g)
+    osc = O.OracleScene.from_gaussians(g)
+    o, d = random_rays(np.random.default_rng(4), 4000, radius=5.0)
+    o[:100] = [0.0, 0.0, -6.0]
+    d[:100] = [0.0, 0.0, 1.0]
+    T64, _ = osc.transmittance_fp64(o, d)
+    for eng in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+        T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=eng)
+        ok, err = gate_T(T, T64)
+        assert ok.all(), np.max(err / np.maximum(T64, 1e-30))
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 1000, 1025])
+def test_leaf_boundaries(vp_ctx, n):
+    rng = np.random.default_rng(n)
+    g = vp.Gaussians(rng.uniform(-1, 1, (n, 3)), np.exp(rng.normal(math.log(0.2), 0.4, (n, 3))),
+                     scenes.uniform_quaternions(rng, n), np.exp(rng.normal(0.5, 0.5, n)))
+    sc = vp.Scene(vp_ctx, g)
+    osc = O.OracleScene.from_gaussians(g)
+    o, d = random_rays(np.random.default_rng(9), 5000, inside_frac=0.3)
+    T64, _ = osc.transmittance_fp64(o, d)
+    for eng in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+        T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=eng).astype(np.float64)
+        assert np.all(np.abs(T - T64) <= 2e-5 * T64 + 1e-9), (eng, np.max(np.abs(T - T64)))
+    info = sc.info()
+    assert info["count"] == n and info["wide_depth"] >= 1
+
+
+def test_invalid_inputs_raise(vp_ctx):
+    g = vp.Gaussians(np.zeros((3, 3)), np.array([[1, 1, 1], [1, -1, 1], [1, 1, 1]]), np.tile([1.0, 0, 0, 0], (3, 1)),
+                     np.ones(3))
+    with pytest.raises(vp.VpError, match="Gaussian 1: invalid scale"):
+        vp.Scene(vp_ctx, g)
+    g2 = vp.Gaussians(np.zeros((2, 3)), np.ones((2, 3)), np.tile([1.0, 0, 0, 0], (2, 1)), np.array([1.0, 0.0]))
+    with pytest.raises(vp.VpError, match="Gaussian 1: invalid density"):
+        vp.Scene(vp_ctx, g2)
+    g3 = vp.Gaussians(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 4)), np.zeros(0))
+    with pytest.raises(vp.VpError, match="no Gaussians"):
+        vp.Scene(vp_ctx, g3)
