@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--engine", default="warp", choices=["warp", "megakernel"])
+    ap.add_argument("--engine", default="wavefront", choices=["warp", "wavefront", "megakernel"])
     ap.add_argument("--n", type=int, default=500_000)
     ap.add_argument("--res", type=int, default=512)
     ap.add_argument("--spp", type=int, default=256)
@@ -272,7 +272,7 @@ def run_ours(args):
     # roofline of the dominant kernel (k_render_warp): algorithmic bytes per launch (one batch) =
     # Gaussian boxes tested x 32 B + Gaussian records loaded x 64 B + inner-node visits x node
     # bytes (BVH32: 32 child boxes = 1 KiB; binary LBVH: 64 B)
-    node_bytes = 1024 if args.engine == "warp" else 64
+    node_bytes = 64 if args.engine == "megakernel" else 1024
     alg_bytes = mstats["prim_tests"] * 32 + mstats["geo_loads"] * 64 + mstats["nodes_visited"] * node_bytes
     launch_ms = statistics.mean(step_ms)
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
@@ -284,7 +284,9 @@ def run_ours(args):
             "per_launch": {"prim_tests": mstats["prim_tests"], "geo_loads": mstats["geo_loads"], "crossings": mstats["crossings"],
                            "inner_nodes": mstats["nodes_visited"], "leaves": mstats["leaves_visited"],
                            "bounces": mstats["bounces"], "shadow_rays": mstats["shadow_rays"],
-                           "max_point_overlap": mstats["max_point_overlap"], "max_hits_per_ray": mstats["max_hits_per_ray"]}}
+                           "max_point_overlap": mstats["max_point_overlap"], "max_hits_per_ray": mstats["max_hits_per_ray"],
+                           "query_nodes[argmin,tau,albedo]": mstats["query_nodes"],
+                           "query_leaves[argmin,tau,albedo]": mstats["query_leaves"]}}
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         try:
@@ -304,7 +306,7 @@ def run_ours(args):
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"samples x{world}"},
             "clocks": clk, "gpu_launches": args.steps, "roofline": roof,
             "scene": scene.info(), "env_build_ms": env.build_ms, "wall_s": wall}
-    if rank == 0 and not args.no_baseline_engine and args.engine == "warp" and world == 1:
+    if rank == 0 and not args.no_baseline_engine and args.engine != "megakernel" and world == 1:
         # the plain per-pixel megakernel of the same method on the same batches (for the ratio)
         mcfg2 = vp.Config(**{**cfg.__dict__, "engine": "megakernel"})
         im2 = vp.ProgressiveImage(ctx, W, H)

@@ -55,7 +55,11 @@ def _compile(nvcc: str, src: Path, extra: list[str]) -> tuple[Path, str]:
 
 
 def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
+    """extra_flags (or the space-separated VP_NVCC_FLAGS environment variable) are appended to
+    every nvcc compile, e.g. -DVP_WARP_MIN_BLOCKS=3; changing them needs force=True."""
     nvcc = _nvcc()
+    if extra_flags is None:
+        extra_flags = os.environ.get("VP_NVCC_FLAGS", "").split()
     OBJ.mkdir(parents=True, exist_ok=True)
     LIBDIR.mkdir(parents=True, exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))

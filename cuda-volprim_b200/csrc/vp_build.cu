@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -18,7 +19,16 @@
 namespace vp {
 namespace {
 
-constexpr uint32_t kLeafMax = 32;  // Gaussians per BVH32 leaf = one per lane
+// Gaussians per BVH32 leaf (at most one per lane).  Smaller leaves have tighter bounds; the warp
+// traversal tests several small leaves in one step.  VP_LEAF_MAX in the environment overrides it.
+constexpr uint32_t kLeafMaxDefault = 32;
+
+uint32_t leaf_max_setting() {
+  const char* e = std::getenv("VP_LEAF_MAX");
+  if (!e) return kLeafMaxDefault;
+  const long v = std::strtol(e, nullptr, 10);
+  return (v >= 1 && v <= 32) ? static_cast<uint32_t>(v) : kLeafMaxDefault;
+}
 
 struct ErrorWords {
   int bad_scale, bad_density, bad_center;  // lowest failing index (INT_MAX = none)
@@ -313,7 +323,7 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
                            const uint32_t* __restrict__ right, const uint32_t* __restrict__ first,
                            const uint32_t* __restrict__ last, const float4* __restrict__ plo,
                            const float4* __restrict__ phi, const float4* __restrict__ nlo,
-                           const float4* __restrict__ nhi, float4* __restrict__ wide) {
+                           const float4* __restrict__ nhi, float4* __restrict__ wide, uint32_t kLeafMax) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_items) return;
   const CollapseItem it = in[t];
@@ -560,10 +570,11 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   }
 
   // Collapse to BVH32.
-  // Upper bound on BVH32 nodes: childless nodes hold > 32 disjoint Gaussians (<= n/33), nodes
+  // Upper bound on BVH32 nodes: childless nodes hold > L disjoint Gaussians (<= n/(L+1)), nodes
   // with one node child hold 31 leaves of their own (<= n/31), branching nodes are fewer than
-  // childless ones (<= n/33).
-  const uint32_t max_wide = n / 31u + 2u * (n / 33u) + 4u;
+  // childless ones (<= n/(L+1)).
+  const uint32_t kLeafMax = leaf_max_setting();
+  const uint32_t max_wide = n / 31u + 2u * (n / (kLeafMax + 1u)) + 4u;
   float4* wide = nullptr;
   if ((s = dev_alloc(&wide, 64ull * max_wide, st))) return s;
   sc->wide = wide;
@@ -587,7 +598,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
       ++depth;
       VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
       k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, left.p, right.p,
-                                                        first.p, last.p, plo.p, phi.p, nlo.p, nhi.p, wide);
+                                                        first.p, last.p, plo.p, phi.p, nlo.p, nhi.p, wide, kLeafMax);
       VP_CUDA(cudaGetLastError());
       unsigned int ch[2];
       VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));

@@ -138,7 +138,7 @@ vp_status check_params(const vp_render_params* p) {
   if (p->nee_mode < VP_NEE_MIS || p->nee_mode > VP_NEE_NONE) return fail(VP_ERROR_INVALID_ARGUMENT, "unknown nee_mode");
   if (p->nee_mode == VP_NEE_RIS && p->ris_candidates == 0)
     return fail(VP_ERROR_INVALID_ARGUMENT, "ris_candidates must be positive");
-  if (p->engine != VP_ENGINE_WARP && p->engine != VP_ENGINE_MEGAKERNEL)
+  if (p->engine != VP_ENGINE_WARP && p->engine != VP_ENGINE_MEGAKERNEL && p->engine != VP_ENGINE_WAVEFRONT)
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown engine");
   if (p->precision < VP_PRECISION_AUTO || p->precision > VP_PRECISION_ACCURATE)
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown precision");
@@ -200,6 +200,8 @@ vp_status vp_context_destroy(vp_context* c) {
   if (c->work_counter) cudaFree(c->work_counter);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  free_wavefront(c);
+  if (c->wf.host_count) cudaFreeHost(c->wf.host_count);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return VP_OK;
@@ -318,7 +320,7 @@ vp_status vp_render_params_default(vp_render_params* p) {
   p->nee_mode = VP_NEE_MIS;
   p->ris_candidates = 6;
   p->batch_spp = 16;  // BATCH_SIZE (renderer.cpp:32)
-  p->engine = VP_ENGINE_WARP;
+  p->engine = VP_ENGINE_WAVEFRONT;
   p->precision = VP_PRECISION_AUTO;
   p->measure = 0;
   return VP_OK;
@@ -414,7 +416,11 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
   const uint32_t batch = p->batch_spp ? p->batch_spp : spp_count;
   for (uint32_t off = 0; off < spp_count; off += batch) {
     const uint32_t cnt = std::min(batch, spp_count - off);
-    if ((st = launch_render(s, e, cv, P, p->engine, im, spp_offset + off, cnt))) return st;
+    if (p->engine == VP_ENGINE_WAVEFRONT) {
+      if ((st = launch_wavefront(s, e, cv, P, im, spp_offset + off, cnt))) return st;
+    } else if ((st = launch_render(s, e, cv, P, p->engine, im, spp_offset + off, cnt))) {
+      return st;
+    }
   }
   VP_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   VP_CUDA(cudaEventSynchronize(ctx->ev1));
@@ -434,6 +440,10 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
     stats->leaves_visited = c.leaves;
     stats->prim_tests = c.prim_tests;
     stats->geo_loads = c.geo_loads;
+    for (int k = 0; k < 3; ++k) {
+      stats->query_nodes[k] = c.kind_nodes[k];
+      stats->query_leaves[k] = c.kind_leaves[k];
+    }
     stats->max_hits_per_ray = c.max_hits;
     stats->max_point_overlap = c.max_overlap;
     stats->device_status = c.status;

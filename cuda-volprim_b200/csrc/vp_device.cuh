@@ -100,6 +100,7 @@ struct ParamsView {
 
 struct Counters {  // device-side statistics (only touched when ParamsView::measure)
   unsigned long long bounces, scatters, crossings, shadow_rays, nodes, leaves, prim_tests, geo_loads;
+  unsigned long long kind_nodes[3], kind_leaves[3];  // per query kind: argmin, transmittance, albedo
   unsigned int max_hits, max_overlap, status;
 };
 

@@ -43,6 +43,27 @@ void dev_free(T*& p, cudaStream_t s) {
 
 }  // namespace vp
 
+namespace vp {
+// Wavefront path state (structure of arrays, one entry per path of a launch batch) and queues.
+struct WfBuffers {
+  float4 *o4, *d4, *thr4, *rad4;  // ray origin / direction / throughput / radiance (.w unused)
+  uint4* rng4;                    // PCG32 state (lo, hi) and increment (lo, hi)
+  uint2* key2;                    // free-flight key of the next bounce
+  uint32_t* meta;                 // bounce | shadow count << 16 | alive << 18
+  float4* alb4;                   // albedo at the scatter point, scatter distance
+  float4 *so4, *sd4, *sw4;        // 3 transmittance queries per path: origin (+T in .w), dir, weight
+  float4* L4;                     // finished sample radiance
+  uint32_t *qa, *qb, *qs;         // path queues (current / next) and shadow-query queue
+  uint32_t* ctr;                  // [0] paths now, [1] paths next, [2] shadow queries, [3..4] work heads
+};
+struct WfWorkspace {
+  size_t cap = 0;  // paths
+  WfBuffers b{};
+  void* base = nullptr;
+  uint32_t* host_count = nullptr;  // pinned, for polling the active-path count
+};
+}  // namespace vp
+
 struct vp_context {
   int32_t device = 0;
   int32_t sm_count = 0;
@@ -50,6 +71,7 @@ struct vp_context {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   vp::Counters* counters = nullptr;   // device, one block of statistics per render call
   unsigned int* work_counter = nullptr;  // device, persistent-kernel work queue head
+  vp::WfWorkspace wf;                 // wavefront engine buffers (grow-only)
 };
 
 struct vp_scene {
@@ -91,6 +113,9 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
                         int32_t engine, vp_image* img, uint32_t spp_offset, uint32_t spp_count);
 vp_status launch_transmittance(vp_scene* s, const float* o, const float* d, uint32_t n,
                                bool accurate, int32_t engine, float* out);
+vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const ParamsView& P, vp_image* img,
+                           uint32_t spp_offset, uint32_t spp_count);
+void free_wavefront(vp_context* ctx);
 vp_status launch_albedo(vp_scene* s, const float* pts, uint32_t n, bool accurate, int32_t engine, float* rgb,
                         uint32_t* cnt);
 vp_status launch_normalize(const float4* in, float4* out, size_t n, float scale, cudaStream_t st);

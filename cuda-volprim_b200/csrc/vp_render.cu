@@ -23,406 +23,54 @@
 #include <algorithm>
 
 #include "vp_internal.h"
+#include "vp_path.cuh"
+#include "vp_traverse.cuh"
 
 namespace vp {
 namespace {
-
-constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kHitCap = 64;    // hit-buffer entries per warp (a leaf adds <= 32 to < 32)
-constexpr int kBinStack = 128; // thread-private stack of the binary traversal
-
-__device__ __forceinline__ float3 safe_inv(float3 d) {
-  auto inv1 = [](float x) { return 1.0f / (fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x); };
-  return f3(inv1(d.x), inv1(d.y), inv1(d.z));
-}
-
-__device__ __forceinline__ bool slab(float3 o, float3 inv, float4 lo, float4 hi, float t_lo,
-                                     float t_hi, float& tnear) {
-  const float tx0 = (lo.x - o.x) * inv.x, tx1 = (hi.x - o.x) * inv.x;
-  const float ty0 = (lo.y - o.y) * inv.y, ty1 = (hi.y - o.y) * inv.y;
-  const float tz0 = (lo.z - o.z) * inv.z, tz1 = (hi.z - o.z) * inv.z;
-  const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), t_lo));
-  const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), t_hi));
-  tnear = tn;
-  return tn <= tf;
-}
-
-__device__ __forceinline__ bool box_contains(float4 lo, float4 hi, float3 p) {
-  return p.x >= lo.x && p.x <= hi.x && p.y >= lo.y && p.y <= hi.y && p.z >= lo.z && p.z <= hi.z;
-}
-
-// ------------------------------------------------------------------------------------------
-// warp engine
-// ------------------------------------------------------------------------------------------
-struct WarpSmem {
-  uint32_t* st_ref;
-  float* st_t;
-  uint32_t* hb_idx;
-  float *hb_tc, *hb_rw, *hb_d2, *hb_h, *hb_u0, *hb_tin, *hb_tout, *hb_icf;
-};
-
-__device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap) {
-  return (size_t)stack_cap * 8u + (size_t)kHitCap * 9u * 4u;
-}
-
-__device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_cap) {
-  WarpSmem w;
-  w.st_ref = reinterpret_cast<uint32_t*>(base);
-  w.st_t = reinterpret_cast<float*>(base + 4u * stack_cap);
-  float* hb = reinterpret_cast<float*>(base + 8u * stack_cap);
-  w.hb_idx = reinterpret_cast<uint32_t*>(hb);
-  w.hb_tc = hb + 1 * kHitCap;
-  w.hb_rw = hb + 2 * kHitCap;
-  w.hb_d2 = hb + 3 * kHitCap;
-  w.hb_h = hb + 4 * kHitCap;
-  w.hb_u0 = hb + 5 * kHitCap;
-  w.hb_tin = hb + 6 * kHitCap;
-  w.hb_tout = hb + 7 * kHitCap;
-  w.hb_icf = hb + 8 * kHitCap;
-  return w;
-}
-
-enum QueryKind { kArgmin = 0, kTau = 1 };
-
-struct WarpStats {
-  unsigned long long crossings = 0, nodes = 0, leaves = 0, prim_tests = 0, geo_loads = 0;
-  unsigned int max_hits = 0;
-};
-
-// One ray query of the warp: kArgmin returns the smallest accepted free-flight distance over
-// every Gaussian whose chord overlaps [0, t) (kInf = escape); kTau returns the optical depth
-// over [0, inf), stopping once it reaches MAX_OPTICAL_DEPTH.
-template <bool kAcc, int kKind>
-__device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o, float3 d,
-                                uint64_t key, uint32_t& status, WarpStats& ws, bool measure) {
-  const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const float3 inv = safe_inv(d);
-  float t_hi = kInf;
-  float acc = 0.0f;
-  int sp = 1, hb = 0;
-  unsigned int hits_seen = 0;
-  if (lane == 0) {
-    W.st_ref[0] = S.wide_root;
-    W.st_t[0] = 0.0f;
-  }
-  __syncwarp();
-
-  auto process = [&](int base, int cnt) {
-    float v = (kKind == kArgmin) ? kInf : 0.0f;
-    if (lane < cnt) {
-      const int e = base + lane;
-      const float tc = W.hb_tc[e], rw = W.hb_rw[e], d2 = W.hb_d2[e], h = W.hb_h[e], u0 = W.hb_u0[e];
-      const float tin = W.hb_tin[e], tout = W.hb_tout[e], icf = W.hb_icf[e];
-      if (kKind == kArgmin) {
-        const uint32_t orig = __ldg(S.perm + W.hb_idx[e]);
-        v = chord_free_flight(tc, rw, d2, h, u0, tin, tout, icf, free_flight_tau(key, orig));
-      } else {
-        v = chord_tau(tc, rw, d2, h, u0, fmaxf(tin, 0.0f), tout, icf);
-      }
-    }
-    if (kKind == kArgmin) t_hi = fminf(t_hi, warp_min(v));
-    else acc += warp_sum(v);
-    if (measure) ws.crossings += (unsigned)cnt;
-  };
-
-  while (sp > 0) {
-    --sp;
-    const uint32_t ref = W.st_ref[sp];
-    const float tn = W.st_t[sp];
-    __syncwarp();
-    if (tn > t_hi) continue;
-    if (ref_is_leaf(ref)) {
-      const uint32_t first = wide_leaf_first(ref), count = wide_leaf_count(ref);
-      if (measure) {
-        ws.leaves++;
-        ws.prim_tests += count;
-      }
-      bool hit = false;
-      Chord ch;
-      float icf = 0.f;
-      const uint32_t pi = first + (uint32_t)lane;
-      bool boxed = false;
-      if ((uint32_t)lane < count) {  // the Gaussian's own 3-sigma box first (32 B), then its record
-        float tb;
-        boxed = slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, t_hi, tb);
-      }
-      if (boxed) {
-        const PrimGeo g = load_geo(S.prims, pi);
-        if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f && ch.t_in <= t_hi) {
-          hit = true;
-          icf = g.icf;
-        }
-      }
-      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
-      const unsigned m = __ballot_sync(kFull, hit);
-      if (hit) {
-        const int pos = hb + __popc(m & lt_mask);
-        W.hb_idx[pos] = pi;
-        W.hb_tc[pos] = ch.tc;
-        W.hb_rw[pos] = ch.rw;
-        W.hb_d2[pos] = ch.d2;
-        W.hb_h[pos] = ch.h;
-        W.hb_u0[pos] = chord_u0(ch, 0.0f);
-        W.hb_tin[pos] = ch.t_in;
-        W.hb_tout[pos] = ch.t_out;
-        W.hb_icf[pos] = icf;
-      }
-      hb += __popc(m);
-      hits_seen += __popc(m);
-      __syncwarp();
-      // Evaluate the buffered chords after every leaf that produced any: the argmin bound t_hi
-      // and the shadow ray's optical depth must be current for pruning and early exit.
-      if (hb > 0) {
-        const int cnt = min(hb, 32);
-        process(hb - cnt, cnt);
-        hb -= cnt;
-        __syncwarp();
-        if (kKind == kTau && acc >= kMaxOpticalDepth) break;
-      }
-    } else {
-      if (measure) ws.nodes++;
-      const float4* node = S.wide + (size_t)ref * 64u;
-      const float4 lo = __ldg(node + lane);
-      const float4 hi = __ldg(node + 32 + lane);
-      const uint32_t cref = __float_as_uint(lo.w);
-      float tnear = 0.f;
-      const bool hit = (cref != kEmptyRef) && slab(o, inv, lo, hi, 0.0f, t_hi, tnear);
-      const unsigned m = __ballot_sync(kFull, hit);
-      const int nh = __popc(m);
-      if (nh > 0) {
-        if ((uint32_t)(sp + nh) > S.stack_cap) {  // cannot happen for a BVH of the recorded depth
-          status |= kStatusStackOverflow;
-          break;
-        }
-        int rank = 0;  // farther children sit deeper in the stack
-        for (unsigned mm = m; mm; mm &= mm - 1u) {
-          const int j = __ffs(mm) - 1;
-          const float tj = __shfl_sync(kFull, tnear, j);
-          rank += (tj > tnear || (tj == tnear && j < lane)) ? 1 : 0;
-        }
-        if (hit) {
-          W.st_ref[sp + rank] = cref;
-          W.st_t[sp + rank] = tnear;
-        }
-        sp += nh;
-      }
-      __syncwarp();
-    }
-  }
-  if (!(kKind == kTau && acc >= kMaxOpticalDepth) && hb > 0) process(0, hb);
-  __syncwarp();
-  if (measure) ws.max_hits = max(ws.max_hits, hits_seen);
-  return (kKind == kArgmin) ? t_hi : acc;
-}
-
-// Albedo at a point: sigma_t * pdf weighted mean over the ellipsoids containing it
-// (evaluate_albedo, sampling.cuh:257-283, over the active set of rebuild_active_set_at_scatter,
-// :422-458).  Also returns the overlap count.
-template <bool kAcc>
-__device__ float3 warp_albedo(const SceneView& S, const WarpSmem& W, float3 x, uint32_t& overlap,
-                              uint32_t& status, WarpStats& ws, bool measure) {
-  const int lane = threadIdx.x & 31;
-  float aw = 0.f, ar = 0.f, ag = 0.f, ab = 0.f;
-  unsigned int cnt = 0;
-  int sp = 1;
-  if (lane == 0) W.st_ref[0] = S.wide_root;
-  __syncwarp();
-  while (sp > 0) {
-    --sp;
-    const uint32_t ref = W.st_ref[sp];
-    __syncwarp();
-    if (ref_is_leaf(ref)) {
-      const uint32_t first = wide_leaf_first(ref), count = wide_leaf_count(ref);
-      if (measure) {
-        ws.leaves++;
-        ws.prim_tests += count;
-      }
-      const uint32_t pi = first + lane;
-      const bool boxed = (uint32_t)lane < count &&
-                         box_contains(__ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), x);
-      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
-      if (boxed) {
-        const PrimGeo g = load_geo(S.prims, pi);
-        float r2;
-        if constexpr (kAcc) {
-          const double Dx = (double)x.x - g.a.x, Dy = (double)x.y - g.a.y, Dz = (double)x.z - g.a.z;
-          const double yx = g.a.w * Dx + g.b.x * Dy + g.b.y * Dz;
-          const double yy = g.b.z * Dx + g.b.w * Dy + g.c.x * Dz;
-          const double yz = g.c.y * Dx + g.c.z * Dy + g.c.w * Dz;
-          r2 = (float)(yx * yx + yy * yy + yz * yz);
-        } else {
-          const float3 y = whiten(g, sub(x, f3(g.a.x, g.a.y, g.a.z)));
-          r2 = dot3(y, y);
-        }
-        if (r2 <= kExtent2) {  // point_inside_bvh_bound (intersection.h:56-61)
-          const float wgt = g.icf * expf(-0.5f * r2);
-          const float3 al = load_albedo(S.prims, pi);
-          aw += wgt;
-          ar += wgt * al.x;
-          ag += wgt * al.y;
-          ab += wgt * al.z;
-          ++cnt;
-        }
-      }
-    } else {
-      if (measure) ws.nodes++;
-      const float4* node = S.wide + (size_t)ref * 64u;
-      const float4 lo = __ldg(node + lane);
-      const float4 hi = __ldg(node + 32 + lane);
-      const uint32_t cref = __float_as_uint(lo.w);
-      const bool hit = (cref != kEmptyRef) && box_contains(lo, hi, x);
-      const unsigned m = __ballot_sync(kFull, hit);
-      const int nh = __popc(m);
-      if ((uint32_t)(sp + nh) > S.stack_cap) {
-        status |= kStatusStackOverflow;
-        break;
-      }
-      if (hit) W.st_ref[sp + __popc(m & ((1u << lane) - 1u))] = cref;
-      sp += nh;
-      __syncwarp();
-    }
-  }
-  __syncwarp();
-  aw = warp_sum(aw);
-  ar = warp_sum(ar);
-  ag = warp_sum(ag);
-  ab = warp_sum(ab);
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
-  overlap = cnt;
-  if (!(aw > 0.f)) return f3(0.f, 0.f, 0.f);
-  const float r = __frcp_rn(aw);
-  return f3(ar * r, ag * r, ab * r);
-}
 
 struct PathStats {
   unsigned long long bounces = 0, scatters = 0, shadow = 0;
   unsigned int max_overlap = 0;
 };
 
-// ---- the path loop, shared by both engines through a query policy ------------------------
+// ---- the path loop, shared by the warp engine and the megakernel through a query policy -----
 template <class Q>
 __device__ float3 trace_path(const SceneView& S, const EnvView& E, const CameraView& C,
                              const ParamsView& P, Q& q, uint32_t px, uint32_t py,
                              uint64_t sample_index, PathStats& ps) {
-  const uint64_t pix = (uint64_t)py * P.width + px;
-  Pcg32 rng = pcg_init(P.seed, seq_hash(pix * (uint64_t)P.spp_total + sample_index));
-  float3 o, d;
-  camera_ray(C, P, px, py, rng, o, d);
-  float3 thr = f3(1.f, 1.f, 1.f), rad = f3(0.f, 0.f, 0.f);
-  for (uint32_t bounce = 0; bounce < P.max_bounces; ++bounce) {
-    const uint32_t khi = rng.next();
-    const uint32_t klo = rng.next();
-    const uint64_t key = ((uint64_t)khi << 32) | klo;
-    // Stage 1-3 of sample_scattering_event: ADT argmin over every overlapped Gaussian.  In a
-    // scene whose albedo is 0 everywhere a scatter ends the path with zero contribution, so
-    // the camera-ray argmin is skipped there (the bounce-0 direct term below is the image).
+  PathState s = start_path(C, P, px, py, sample_index);
+  bool alive = P.max_bounces > 0;
+  while (alive) {
+    const uint64_t key = draw_bounce_key(s.rng);
+    // Stages 1-3 of sample_scattering_event (sampling.cuh:474-540): ADT argmin over every
+    // overlapped Gaussian, with the albedo of the rebuilt active set.  In a scene whose albedo
+    // is 0 everywhere a scatter ends the path with zero contribution, so the camera-ray argmin
+    // is skipped there (the bounce-0 direct term is the whole image).
     float tstar = kInf;
-    if (!(bounce == 0 && S.albedo_all_zero)) tstar = q.argmin(o, d, key);
+    ScatterAlbedo sa;
+    sa.valid = false;
+    if (!(s.bounce == 0 && S.albedo_all_zero)) tstar = q.argmin(s.o, s.d, key, &sa);
     const bool scattered = tstar < kInf;
+    float3 albedo = f3(0.f, 0.f, 0.f);
+    if (scattered) {
+      uint32_t overlap = sa.overlap;
+      albedo = sa.valid ? sa.albedo : q.albedo(fma3(tstar, s.d, s.o), overlap);
+      if (P.measure) ps.max_overlap = max(ps.max_overlap, overlap);
+    }
     if (P.measure) {
       ps.bounces++;
       if (scattered) ps.scatters++;
     }
-    float3 pos = o, dir_next = d;
-    if (scattered) {
-      pos = fma3(tstar, d, o);  // ray.at(t) = o + t d
-      float pdf;
-      dir_next = hg_sample(P, d, rng, pdf);
-    }
-    // Transmittance queries of this bounce (the bounce-0 camera ray and the NEE shadow rays)
-    // are collected first and traced in one loop below: they draw no random numbers, so the
-    // PCG32 stream is the reference's, and the query code exists once in the kernel.
-    float3 sh_o[3], sh_d[3], sh_w[3];
-    int ns = 0;
-    if (bounce == 0) {  // Rao-Blackwellised direct term (raygen.cuh:148-160)
-      sh_o[0] = o;
-      sh_d[0] = d;
-      sh_w[0] = mul(thr, env_lookup(E, d));
-      ns = 1;
-    }
-    float3 albedo = f3(0.f, 0.f, 0.f);
-    if (!scattered) {  // accumulate_escape_radiance (path_stages.cuh:368-386)
-      if (P.nee_mode == VP_NEE_NONE && bounce > 0) rad = add(rad, mul(thr, env_lookup(E, d)));
-    } else {
-      uint32_t overlap = 0;
-      albedo = q.albedo(pos, overlap);
-      if (P.measure) ps.max_overlap = max(ps.max_overlap, overlap);
-      const float3 base = mul(thr, albedo);
-      if (P.nee_mode != VP_NEE_NONE && (base.x != 0.f || base.y != 0.f || base.z != 0.f)) {
-        // accumulate_nee_direct (path_stages.cuh:394-472); shadow rays start at the scatter point.
-        if (P.nee_mode == VP_NEE_MIS) {
-          float pdf_a;
-          const float3 wa = hg_sample(P, d, rng, pdf_a);
-          const float w_a = mis_balance(pdf_a, env_pdf(E, wa));
-          const float3 c_a = mul(mul(base, env_lookup(E, wa)), w_a);
-          float pdf_b;
-          const float3 wb = env_sample(E, rng, pdf_b);
-          const float ph_b = hg_eval(P, d, wb);
-          const float w_b = mis_balance(pdf_b, ph_b);
-          const float3 c_b = mul(mul(base, env_lookup(E, wb)), w_b * ph_b * __frcp_rn(pdf_b));
-          sh_o[ns] = pos, sh_d[ns] = wa, sh_w[ns] = c_a;
-          ++ns;
-          sh_o[ns] = pos, sh_d[ns] = wb, sh_w[ns] = c_b;
-          ++ns;
-        } else if (P.nee_mode == VP_NEE_PHASE) {
-          float pdf;
-          const float3 ws_ = hg_sample(P, d, rng, pdf);
-          sh_o[ns] = pos, sh_d[ns] = ws_, sh_w[ns] = mul(base, env_lookup(E, ws_));
-          ++ns;
-        } else {  // VP_NEE_RIS: product RIS over ris_k env-IS candidates, 1 shadow ray
-          const float3 luma = f3(0.2126f, 0.7152f, 0.0722f);
-          float wsum = 0.f;
-          float3 y_dir = f3(0.f, 0.f, 0.f), y_env = f3(0.f, 0.f, 0.f);
-          for (uint32_t k = 0; k < P.ris_k; ++k) {
-            float cpdf;
-            const float3 cw = env_sample(E, rng, cpdf);
-            if (cpdf <= 0.f) continue;
-            const float3 env_c = env_lookup(E, cw);
-            const float lum_c = dot3(env_c, luma);
-            const float w = hg_eval(P, d, cw) * lum_c * __frcp_rn(cpdf);
-            if (!(w > 0.f)) continue;
-            wsum += w;
-            if (rng.uniform() * wsum < w) {
-              y_dir = cw;
-              y_env = env_c;
-            }
-          }
-          if (wsum > 0.f) {
-            const float lum_y = dot3(y_env, luma);
-            if (lum_y > 0.f) {
-              const float W_ris = wsum * __frcp_rn((float)P.ris_k);
-              sh_o[ns] = pos, sh_d[ns] = y_dir, sh_w[ns] = mul(mul(base, mul(y_env, __frcp_rn(lum_y))), W_ris);
-              ++ns;
-            }
-          }
-        }
-      }
-    }
+    ShadowSet sh;
+    alive = shade_bounce(E, P, s, scattered, tstar, albedo, sh);
 #pragma unroll 1
-    for (int k = 0; k < ns; ++k) {  // compute_transmittance_to_env (sampling.cuh:548-583)
-      rad = add(rad, mul(sh_w[k], q.transmittance(sh_o[k], sh_d[k])));
+    for (int k = 0; k < sh.n; ++k) {  // compute_transmittance_to_env (sampling.cuh:548-583)
+      s.rad = add(s.rad, mul(sh.w[k], q.transmittance(sh.o[k], sh.d[k])));
       if (P.measure) ps.shadow++;
     }
-    if (!scattered) break;
-    thr = mul(thr, albedo);
-    if (bounce >= P.rr_depth) {  // russian_roulette (path_stages.cuh:25-37)
-      const float p_survive = fminf(P.rr_max_survival, fmax3(thr));
-      if (rng.uniform() > p_survive || p_survive <= 0.f) break;
-      thr = mul(thr, __frcp_rn(p_survive));
-    }
-    if (fmax3(thr) < kMinThroughput) break;
-    if (!isfinite(sum3(thr))) break;
-    o = pos;
-    d = dir_next;
   }
-  // finalize_sample (path_stages.cuh:52-62)
-  if (P.firefly_clamp > 0.f) {
-    const float lum = dot3(rad, f3(0.2126f, 0.7152f, 0.0722f));
-    if (lum > P.firefly_clamp) rad = mul(rad, P.firefly_clamp * __frcp_rn(lum));
-  }
-  if (!isfinite(sum3(rad))) rad = f3(0.f, 0.f, 0.f);
-  return rad;
+  return finalize_sample(P, s.rad);
 }
 
 template <bool kAcc>
@@ -432,8 +80,8 @@ struct WarpQueries {
   uint32_t& status;
   WarpStats& ws;
   bool measure;
-  __device__ float argmin(float3 o, float3 d, uint64_t key) {
-    return warp_ray_query<kAcc, kArgmin>(S, W, o, d, key, status, ws, measure);
+  __device__ float argmin(float3 o, float3 d, uint64_t key, ScatterAlbedo* sa) {
+    return warp_ray_query<kAcc, kArgmin>(S, W, o, d, key, status, ws, measure, sa);
   }
   __device__ float transmittance(float3 o, float3 d) {
     const float tau = warp_ray_query<kAcc, kTau>(S, W, o, d, 0ull, status, ws, measure);
@@ -456,6 +104,10 @@ __device__ __forceinline__ void flush_stats(Counters* c, const PathStats& ps, co
   atomicAdd(&c->leaves, ws.leaves);
   atomicAdd(&c->prim_tests, ws.prim_tests);
   atomicAdd(&c->geo_loads, ws.geo_loads);
+  for (int k = 0; k < 3; ++k) {
+    atomicAdd(&c->kind_nodes[k], ws.kind_nodes[k]);
+    atomicAdd(&c->kind_leaves[k], ws.kind_leaves[k]);
+  }
   atomicMax(&c->max_hits, ws.max_hits);
   atomicMax(&c->max_overlap, ps.max_overlap);
 }
@@ -463,7 +115,7 @@ __device__ __forceinline__ void flush_stats(Counters* c, const PathStats& ps, co
 // Persistent warp-per-path kernel: warps pull pixels from a global counter; each pixel runs
 // samples [spp_offset, spp_offset + spp_count) in order and Welford-updates mean/count.
 template <bool kAcc>
-__global__ void __launch_bounds__(256) k_render_warp(SceneView S, EnvView E, CameraView C,
+__global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneView S, EnvView E, CameraView C,
                                                      ParamsView P, float4* __restrict__ mean,
                                                      uint32_t* __restrict__ count,
                                                      uint32_t spp_offset, uint32_t spp_count,
@@ -503,146 +155,6 @@ __global__ void __launch_bounds__(256) k_render_warp(SceneView S, EnvView E, Cam
 // ------------------------------------------------------------------------------------------
 // megakernel (thread per pixel, binary LBVH)
 // ------------------------------------------------------------------------------------------
-template <bool kAcc>
-struct ThreadQueries {
-  const SceneView& S;
-  uint32_t& status;
-  WarpStats& ws;
-  bool measure;
-
-  template <int kKind>
-  __device__ float ray(float3 o, float3 d, uint64_t key) {
-    const float3 inv = safe_inv(d);
-    uint32_t stack[kBinStack];
-    int sp = 0;
-    float t_hi = kInf, acc = 0.f;
-    uint32_t node = S.bin_root;
-    unsigned int hits = 0;
-    while (true) {
-      if (measure) ws.nodes++;
-      const float4* nd = S.bin + 4u * node;
-      const float4 ll = __ldg(nd), lh = __ldg(nd + 1), rl = __ldg(nd + 2), rh = __ldg(nd + 3);
-      const uint32_t refs[2] = {__float_as_uint(ll.w), __float_as_uint(rl.w)};
-      float tn[2];
-      bool hit[2];
-      hit[0] = refs[0] != kEmptyRef && slab(o, inv, ll, lh, 0.f, t_hi, tn[0]);
-      hit[1] = refs[1] != kEmptyRef && slab(o, inv, rl, rh, 0.f, t_hi, tn[1]);
-      uint32_t next_inner[2];
-      int n_inner = 0;
-      for (int c = 0; c < 2; ++c) {
-        if (!hit[c]) continue;
-        if (ref_is_leaf(refs[c])) {
-          const uint32_t pi = refs[c] & ~kLeafBit;
-          if (measure) ws.geo_loads++;
-          const PrimGeo g = load_geo(S.prims, pi);
-          Chord ch;
-          if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.f && ch.t_in <= t_hi) {
-            ++hits;
-            if (measure) ws.crossings++;
-            const float u0 = chord_u0(ch, 0.f);
-            if (kKind == kArgmin) {
-              const float ts = chord_free_flight(ch.tc, ch.rw, ch.d2, ch.h, u0, ch.t_in, ch.t_out, g.icf,
-                                                 free_flight_tau(key, __ldg(S.perm + pi)));
-              t_hi = fminf(t_hi, ts);
-            } else {
-              acc += chord_tau(ch.tc, ch.rw, ch.d2, ch.h, u0, fmaxf(ch.t_in, 0.f), ch.t_out, g.icf);
-            }
-          }
-        } else {
-          next_inner[n_inner++] = c;
-        }
-      }
-      if (kKind == kTau && acc >= kMaxOpticalDepth) break;
-      if (n_inner == 2) {  // nearer first
-        const int nearc = tn[0] <= tn[1] ? 0 : 1;
-        if (sp >= kBinStack) {
-          status |= kStatusStackOverflow;
-          break;
-        }
-        stack[sp++] = refs[1 - nearc];
-        node = refs[nearc];
-        continue;
-      }
-      if (n_inner == 1) {
-        node = refs[next_inner[0]];
-        continue;
-      }
-      // pop, skipping nodes that can no longer matter is done on the next visit's slab test
-      if (sp == 0) break;
-      node = stack[--sp];
-    }
-    if (measure) ws.max_hits = max(ws.max_hits, hits);
-    return (kKind == kArgmin) ? t_hi : acc;
-  }
-  __device__ float argmin(float3 o, float3 d, uint64_t key) { return ray<kArgmin>(o, d, key); }
-  __device__ float transmittance(float3 o, float3 d) {
-    const float tau = ray<kTau>(o, d, 0ull);
-    return tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
-  }
-  __device__ float3 albedo(float3 x, uint32_t& overlap) {
-    uint32_t stack[kBinStack];
-    int sp = 0;
-    uint32_t node = S.bin_root;
-    float aw = 0.f;
-    float3 a = f3(0.f, 0.f, 0.f);
-    uint32_t cnt = 0;
-    while (true) {
-      if (measure) ws.nodes++;
-      const float4* nd = S.bin + 4u * node;
-      const float4 bl[2] = {__ldg(nd), __ldg(nd + 2)};
-      const float4 bh[2] = {__ldg(nd + 1), __ldg(nd + 3)};
-      int n_inner = 0;
-      uint32_t inner[2];
-      for (int c = 0; c < 2; ++c) {
-        const uint32_t r = __float_as_uint(bl[c].w);
-        if (r == kEmptyRef || !box_contains(bl[c], bh[c], x)) continue;
-        if (ref_is_leaf(r)) {
-          const uint32_t pi = r & ~kLeafBit;
-          if (measure) ws.geo_loads++;
-          const PrimGeo g = load_geo(S.prims, pi);
-          float r2;
-          if constexpr (kAcc) {
-            const double Dx = (double)x.x - g.a.x, Dy = (double)x.y - g.a.y, Dz = (double)x.z - g.a.z;
-            const double yx = g.a.w * Dx + g.b.x * Dy + g.b.y * Dz;
-            const double yy = g.b.z * Dx + g.b.w * Dy + g.c.x * Dz;
-            const double yz = g.c.y * Dx + g.c.z * Dy + g.c.w * Dz;
-            r2 = (float)(yx * yx + yy * yy + yz * yz);
-          } else {
-            const float3 y = whiten(g, sub(x, f3(g.a.x, g.a.y, g.a.z)));
-            r2 = dot3(y, y);
-          }
-          if (r2 <= kExtent2) {
-            const float wgt = g.icf * expf(-0.5f * r2);
-            aw += wgt;
-            a = add(a, mul(load_albedo(S.prims, pi), wgt));
-            ++cnt;
-          }
-        } else {
-          inner[n_inner++] = r;
-        }
-      }
-      if (n_inner == 2) {
-        if (sp >= kBinStack) {
-          status |= kStatusStackOverflow;
-          break;
-        }
-        stack[sp++] = inner[1];
-        node = inner[0];
-        continue;
-      }
-      if (n_inner == 1) {
-        node = inner[0];
-        continue;
-      }
-      if (sp == 0) break;
-      node = stack[--sp];
-    }
-    overlap = cnt;
-    if (!(aw > 0.f)) return f3(0.f, 0.f, 0.f);
-    return mul(a, __frcp_rn(aw));
-  }
-};
-
 template <bool kAcc>
 __global__ void __launch_bounds__(128) k_render_mega(SceneView S, EnvView E, CameraView C, ParamsView P,
                                                      float4* __restrict__ mean, uint32_t* __restrict__ count,

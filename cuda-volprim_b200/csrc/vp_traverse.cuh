@@ -1,0 +1,522 @@
+// Warp-cooperative BVH32 queries and thread-private binary-LBVH queries over the per-Gaussian
+// math of vp_device.cuh, shared by the persistent warp engine, the plain megakernel and the
+// wavefront engine.
+#pragma once
+
+#include "vp_internal.h"
+
+namespace vp {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+#ifndef VP_HIT_CAP
+#define VP_HIT_CAP 128
+#endif
+constexpr int kHitCap = VP_HIT_CAP;  // hit-buffer entries per warp (retained chords + one step's new ones)
+constexpr int kBinStack = 128; // thread-private stack of the binary traversal
+
+// Resident 256-thread blocks per SM the warp engine's register budget is sized for.
+#ifndef VP_WARP_MIN_BLOCKS
+#define VP_WARP_MIN_BLOCKS 4
+#endif
+
+__device__ __forceinline__ float3 safe_inv(float3 d) {
+  auto inv1 = [](float x) { return 1.0f / (fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x); };
+  return f3(inv1(d.x), inv1(d.y), inv1(d.z));
+}
+
+__device__ __forceinline__ bool slab(float3 o, float3 inv, float4 lo, float4 hi, float t_lo,
+                                     float t_hi, float& tnear) {
+  const float tx0 = (lo.x - o.x) * inv.x, tx1 = (hi.x - o.x) * inv.x;
+  const float ty0 = (lo.y - o.y) * inv.y, ty1 = (hi.y - o.y) * inv.y;
+  const float tz0 = (lo.z - o.z) * inv.z, tz1 = (hi.z - o.z) * inv.z;
+  const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), t_lo));
+  const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), t_hi));
+  tnear = tn;
+  return tn <= tf;
+}
+
+__device__ __forceinline__ bool box_contains(float4 lo, float4 hi, float3 p) {
+  return p.x >= lo.x && p.x <= hi.x && p.y >= lo.y && p.y <= hi.y && p.z >= lo.z && p.z <= hi.z;
+}
+
+// ------------------------------------------------------------------------------------------
+// warp engine
+// ------------------------------------------------------------------------------------------
+struct WarpSmem {
+  uint32_t* st_ref;
+  float* st_t;
+  uint32_t* hb_idx;
+  float *hb_tc, *hb_rw, *hb_d2, *hb_h, *hb_u0, *hb_tin, *hb_tout, *hb_icf;
+};
+
+__device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap) {
+  return (size_t)stack_cap * 8u + (size_t)kHitCap * 9u * 4u;
+}
+
+__device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_cap) {
+  WarpSmem w;
+  w.st_ref = reinterpret_cast<uint32_t*>(base);
+  w.st_t = reinterpret_cast<float*>(base + 4u * stack_cap);
+  float* hb = reinterpret_cast<float*>(base + 8u * stack_cap);
+  w.hb_idx = reinterpret_cast<uint32_t*>(hb);
+  w.hb_tc = hb + 1 * kHitCap;
+  w.hb_rw = hb + 2 * kHitCap;
+  w.hb_d2 = hb + 3 * kHitCap;
+  w.hb_h = hb + 4 * kHitCap;
+  w.hb_u0 = hb + 5 * kHitCap;
+  w.hb_tin = hb + 6 * kHitCap;
+  w.hb_tout = hb + 7 * kHitCap;
+  w.hb_icf = hb + 8 * kHitCap;
+  return w;
+}
+
+enum QueryKind { kArgmin = 0, kTau = 1 };
+
+struct WarpStats {
+  unsigned long long crossings = 0, nodes = 0, leaves = 0, prim_tests = 0, geo_loads = 0;
+  unsigned long long kind_nodes[3] = {0, 0, 0}, kind_leaves[3] = {0, 0, 0};
+  unsigned int max_hits = 0;
+};
+
+// Albedo at the scatter point, when the argmin query could derive it from its own chords.
+struct ScatterAlbedo {
+  float3 albedo;
+  uint32_t overlap;
+  bool valid;
+};
+
+// One ray query of the warp: kArgmin returns the smallest accepted free-flight distance over
+// every Gaussian whose chord overlaps [0, t) (kInf = escape); kTau returns the optical depth
+// over [0, inf), stopping once it reaches MAX_OPTICAL_DEPTH.
+//
+// With `sa` (kArgmin only) the processed chords with t_in <= t stay in the hit buffer, and after
+// the traversal the albedo at the scatter distance t* is the sigma_t * pdf-weighted mean over
+// the chords containing t* -- the reference's rebuilt active set (sampling.cuh:422-458) and
+// evaluate_albedo (:257-283), with the whitened radius from the chord frame,
+// |y|^2 = d2 + ((t* - t_c)|w|)^2.  Every Gaussian containing the scatter point was processed (its
+// chord starts before t* <= t), so the set is complete; if the retained chords outgrow the
+// buffer, sa->valid stays false and the caller runs the point query instead.
+template <bool kAcc, int kKind>
+__device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o, float3 d,
+                                uint64_t key, uint32_t& status, WarpStats& ws, bool measure,
+                                ScatterAlbedo* sa = nullptr) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const float3 inv = safe_inv(d);
+  float t_hi = kInf;
+  float acc = 0.0f;
+  int sp = 1, hb = 0, kept = 0;  // [0, kept) processed and retained, [kept, hb) pending
+  bool keep = (kKind == kArgmin) && sa != nullptr;
+  unsigned int hits_seen = 0;
+  if (lane == 0) {
+    W.st_ref[0] = S.wide_root;
+    W.st_t[0] = 0.0f;
+  }
+  __syncwarp();
+
+  // Drop retained chords that start beyond the current bound (they cannot contain t*).
+  auto compact = [&]() {
+    int w = 0;
+    for (int base = 0; base < kept; base += 32) {
+      const int e = base + lane;
+      const bool keepit = e < kept && W.hb_tin[e] <= t_hi;
+      uint32_t idx = 0;
+      float f[8];
+      if (keepit) {
+        idx = W.hb_idx[e];
+        f[0] = W.hb_tc[e], f[1] = W.hb_rw[e], f[2] = W.hb_d2[e], f[3] = W.hb_h[e];
+        f[4] = W.hb_u0[e], f[5] = W.hb_tin[e], f[6] = W.hb_tout[e], f[7] = W.hb_icf[e];
+      }
+      const unsigned m = __ballot_sync(kFull, keepit);
+      __syncwarp();
+      if (keepit) {
+        const int p = w + __popc(m & lt_mask);
+        W.hb_idx[p] = idx;
+        W.hb_tc[p] = f[0], W.hb_rw[p] = f[1], W.hb_d2[p] = f[2], W.hb_h[p] = f[3];
+        W.hb_u0[p] = f[4], W.hb_tin[p] = f[5], W.hb_tout[p] = f[6], W.hb_icf[p] = f[7];
+      }
+      w += __popc(m);
+      __syncwarp();
+    }
+    kept = hb = w;
+  };
+
+  auto process = [&](int base, int cnt) {
+    float v = (kKind == kArgmin) ? kInf : 0.0f;
+    if (lane < cnt) {
+      const int e = base + lane;
+      const float tc = W.hb_tc[e], rw = W.hb_rw[e], d2 = W.hb_d2[e], h = W.hb_h[e], u0 = W.hb_u0[e];
+      const float tin = W.hb_tin[e], tout = W.hb_tout[e], icf = W.hb_icf[e];
+      if (kKind == kArgmin) {
+        const uint32_t orig = __ldg(S.perm + W.hb_idx[e]);
+        v = chord_free_flight(tc, rw, d2, h, u0, tin, tout, icf, free_flight_tau(key, orig));
+      } else {
+        v = chord_tau(tc, rw, d2, h, u0, fmaxf(tin, 0.0f), tout, icf);
+      }
+    }
+    if (kKind == kArgmin) t_hi = fminf(t_hi, warp_min(v));
+    else acc += warp_sum(v);
+    if (measure) ws.crossings += (unsigned)cnt;
+  };
+
+  while (sp > 0) {
+    --sp;
+    const uint32_t ref = W.st_ref[sp];
+    const float tn = W.st_t[sp];
+    __syncwarp();
+    if (tn > t_hi) continue;
+    if (ref_is_leaf(ref)) {
+      const int total = (int)wide_leaf_count(ref);
+      if (measure) {
+        ws.leaves++;
+        ws.kind_leaves[kKind]++;
+        ws.prim_tests += total;
+      }
+      bool hit = false;
+      Chord ch;
+      float icf = 0.f;
+      const uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
+      bool boxed = false;
+      if (lane < total) {  // the Gaussian's own 3-sigma box first (32 B), then its record
+        float tb;
+        boxed = slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, t_hi, tb);
+      }
+      if (boxed) {
+        const PrimGeo g = load_geo(S.prims, pi);
+        if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f && ch.t_in <= t_hi) {
+          hit = true;
+          icf = g.icf;
+        }
+      }
+      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
+      const unsigned m = __ballot_sync(kFull, hit);
+      if (keep && m != 0u && hb + 32 > kHitCap) {  // make room for up to 32 new chords
+        compact();
+        if (hb + 32 > kHitCap) {  // still full: stop retaining, the caller will query the point
+          keep = false;
+          kept = hb = 0;
+        }
+      }
+      if (hit) {
+        const int pos = hb + __popc(m & lt_mask);
+        W.hb_idx[pos] = pi;
+        W.hb_tc[pos] = ch.tc;
+        W.hb_rw[pos] = ch.rw;
+        W.hb_d2[pos] = ch.d2;
+        W.hb_h[pos] = ch.h;
+        W.hb_u0[pos] = chord_u0(ch, 0.0f);
+        W.hb_tin[pos] = ch.t_in;
+        W.hb_tout[pos] = ch.t_out;
+        W.hb_icf[pos] = icf;
+      }
+      hb += __popc(m);
+      hits_seen += __popc(m);
+      __syncwarp();
+      // Evaluate the new chords after every leaf that produced any: the argmin bound t_hi and
+      // the shadow ray's optical depth must be current for pruning and early exit.
+      if (hb > kept) {
+        process(kept, hb - kept);
+        if (keep) kept = hb;
+        else hb = kept;
+        __syncwarp();
+        if (kKind == kTau && acc >= kMaxOpticalDepth) break;
+      }
+    } else {
+      if (measure) {
+        ws.nodes++;
+        ws.kind_nodes[kKind]++;
+      }
+      const float4* node = S.wide + (size_t)ref * 64u;
+      const float4 lo = __ldg(node + lane);
+      const float4 hi = __ldg(node + 32 + lane);
+      const uint32_t cref = __float_as_uint(lo.w);
+      float tnear = 0.f;
+      const bool hit = (cref != kEmptyRef) && slab(o, inv, lo, hi, 0.0f, t_hi, tnear);
+      const unsigned m = __ballot_sync(kFull, hit);
+      const int nh = __popc(m);
+      if (nh > 0) {
+        if ((uint32_t)(sp + nh) > S.stack_cap) {  // cannot happen for a BVH of the recorded depth
+          status |= kStatusStackOverflow;
+          break;
+        }
+        int rank = 0;  // farther children sit deeper in the stack
+        for (unsigned mm = m; mm; mm &= mm - 1u) {
+          const int j = __ffs(mm) - 1;
+          const float tj = __shfl_sync(kFull, tnear, j);
+          rank += (tj > tnear || (tj == tnear && j < lane)) ? 1 : 0;
+        }
+        if (hit) {
+          W.st_ref[sp + rank] = cref;
+          W.st_t[sp + rank] = tnear;
+        }
+        sp += nh;
+      }
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  if (measure) ws.max_hits = max(ws.max_hits, hits_seen);
+  if constexpr (kKind == kArgmin) {
+    if (sa != nullptr) {
+      sa->valid = false;
+      if (keep && t_hi < kInf) {
+        const float ts = t_hi;
+        float aw = 0.f, ar = 0.f, ag = 0.f, ab = 0.f;
+        unsigned int cnt = 0;
+        for (int base = 0; base < kept; base += 32) {
+          const int e = base + lane;
+          if (e < kept && W.hb_tin[e] <= ts && ts <= W.hb_tout[e]) {
+            const float u = (ts - W.hb_tc[e]) / W.hb_rw[e];
+            const float wgt = W.hb_icf[e] * expf(-0.5f * fmaf(u, u, W.hb_d2[e]));
+            const float3 al = load_albedo(S.prims, W.hb_idx[e]);
+            aw += wgt;
+            ar += wgt * al.x;
+            ag += wgt * al.y;
+            ab += wgt * al.z;
+            ++cnt;
+          }
+        }
+        aw = warp_sum(aw);
+        ar = warp_sum(ar);
+        ag = warp_sum(ag);
+        ab = warp_sum(ab);
+        for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(kFull, cnt, off);
+        const float r = aw > 0.f ? __frcp_rn(aw) : 0.f;
+        sa->albedo = aw > 0.f ? f3(ar * r, ag * r, ab * r) : f3(0.f, 0.f, 0.f);
+        sa->overlap = cnt;
+        sa->valid = true;
+      }
+    }
+  }
+  __syncwarp();
+  return (kKind == kArgmin) ? t_hi : acc;
+}
+
+// Albedo at a point: sigma_t * pdf weighted mean over the ellipsoids containing it
+// (evaluate_albedo, sampling.cuh:257-283, over the active set of rebuild_active_set_at_scatter,
+// :422-458).  Also returns the overlap count.
+template <bool kAcc>
+__device__ float3 warp_albedo(const SceneView& S, const WarpSmem& W, float3 x, uint32_t& overlap,
+                              uint32_t& status, WarpStats& ws, bool measure) {
+  const int lane = threadIdx.x & 31;
+  float aw = 0.f, ar = 0.f, ag = 0.f, ab = 0.f;
+  unsigned int cnt = 0;
+  int sp = 1;
+  if (lane == 0) W.st_ref[0] = S.wide_root;
+  __syncwarp();
+  while (sp > 0) {
+    --sp;
+    const uint32_t ref = W.st_ref[sp];
+    __syncwarp();
+    if (ref_is_leaf(ref)) {
+      const uint32_t first = wide_leaf_first(ref), count = wide_leaf_count(ref);
+      if (measure) {
+        ws.leaves++;
+        ws.kind_leaves[2]++;
+        ws.prim_tests += count;
+      }
+      const uint32_t pi = first + lane;
+      const bool boxed = (uint32_t)lane < count &&
+                         box_contains(__ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), x);
+      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
+      if (boxed) {
+        const PrimGeo g = load_geo(S.prims, pi);
+        float r2;
+        if constexpr (kAcc) {
+          const double Dx = (double)x.x - g.a.x, Dy = (double)x.y - g.a.y, Dz = (double)x.z - g.a.z;
+          const double yx = g.a.w * Dx + g.b.x * Dy + g.b.y * Dz;
+          const double yy = g.b.z * Dx + g.b.w * Dy + g.c.x * Dz;
+          const double yz = g.c.y * Dx + g.c.z * Dy + g.c.w * Dz;
+          r2 = (float)(yx * yx + yy * yy + yz * yz);
+        } else {
+          const float3 y = whiten(g, sub(x, f3(g.a.x, g.a.y, g.a.z)));
+          r2 = dot3(y, y);
+        }
+        if (r2 <= kExtent2) {  // point_inside_bvh_bound (intersection.h:56-61)
+          const float wgt = g.icf * expf(-0.5f * r2);
+          const float3 al = load_albedo(S.prims, pi);
+          aw += wgt;
+          ar += wgt * al.x;
+          ag += wgt * al.y;
+          ab += wgt * al.z;
+          ++cnt;
+        }
+      }
+    } else {
+      if (measure) {
+        ws.nodes++;
+        ws.kind_nodes[2]++;
+      }
+      const float4* node = S.wide + (size_t)ref * 64u;
+      const float4 lo = __ldg(node + lane);
+      const float4 hi = __ldg(node + 32 + lane);
+      const uint32_t cref = __float_as_uint(lo.w);
+      const bool hit = (cref != kEmptyRef) && box_contains(lo, hi, x);
+      const unsigned m = __ballot_sync(kFull, hit);
+      const int nh = __popc(m);
+      if ((uint32_t)(sp + nh) > S.stack_cap) {
+        status |= kStatusStackOverflow;
+        break;
+      }
+      if (hit) W.st_ref[sp + __popc(m & ((1u << lane) - 1u))] = cref;
+      sp += nh;
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  aw = warp_sum(aw);
+  ar = warp_sum(ar);
+  ag = warp_sum(ag);
+  ab = warp_sum(ab);
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+  overlap = cnt;
+  if (!(aw > 0.f)) return f3(0.f, 0.f, 0.f);
+  const float r = __frcp_rn(aw);
+  return f3(ar * r, ag * r, ab * r);
+}
+
+
+template <bool kAcc>
+struct ThreadQueries {
+  const SceneView& S;
+  uint32_t& status;
+  WarpStats& ws;
+  bool measure;
+
+  template <int kKind>
+  __device__ float ray(float3 o, float3 d, uint64_t key) {
+    const float3 inv = safe_inv(d);
+    uint32_t stack[kBinStack];
+    int sp = 0;
+    float t_hi = kInf, acc = 0.f;
+    uint32_t node = S.bin_root;
+    unsigned int hits = 0;
+    while (true) {
+      if (measure) ws.nodes++;
+      const float4* nd = S.bin + 4u * node;
+      const float4 ll = __ldg(nd), lh = __ldg(nd + 1), rl = __ldg(nd + 2), rh = __ldg(nd + 3);
+      const uint32_t refs[2] = {__float_as_uint(ll.w), __float_as_uint(rl.w)};
+      float tn[2];
+      bool hit[2];
+      hit[0] = refs[0] != kEmptyRef && slab(o, inv, ll, lh, 0.f, t_hi, tn[0]);
+      hit[1] = refs[1] != kEmptyRef && slab(o, inv, rl, rh, 0.f, t_hi, tn[1]);
+      uint32_t next_inner[2];
+      int n_inner = 0;
+      for (int c = 0; c < 2; ++c) {
+        if (!hit[c]) continue;
+        if (ref_is_leaf(refs[c])) {
+          const uint32_t pi = refs[c] & ~kLeafBit;
+          if (measure) ws.geo_loads++;
+          const PrimGeo g = load_geo(S.prims, pi);
+          Chord ch;
+          if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.f && ch.t_in <= t_hi) {
+            ++hits;
+            if (measure) ws.crossings++;
+            const float u0 = chord_u0(ch, 0.f);
+            if (kKind == kArgmin) {
+              const float ts = chord_free_flight(ch.tc, ch.rw, ch.d2, ch.h, u0, ch.t_in, ch.t_out, g.icf,
+                                                 free_flight_tau(key, __ldg(S.perm + pi)));
+              t_hi = fminf(t_hi, ts);
+            } else {
+              acc += chord_tau(ch.tc, ch.rw, ch.d2, ch.h, u0, fmaxf(ch.t_in, 0.f), ch.t_out, g.icf);
+            }
+          }
+        } else {
+          next_inner[n_inner++] = c;
+        }
+      }
+      if (kKind == kTau && acc >= kMaxOpticalDepth) break;
+      if (n_inner == 2) {  // nearer first
+        const int nearc = tn[0] <= tn[1] ? 0 : 1;
+        if (sp >= kBinStack) {
+          status |= kStatusStackOverflow;
+          break;
+        }
+        stack[sp++] = refs[1 - nearc];
+        node = refs[nearc];
+        continue;
+      }
+      if (n_inner == 1) {
+        node = refs[next_inner[0]];
+        continue;
+      }
+      // pop, skipping nodes that can no longer matter is done on the next visit's slab test
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+    if (measure) ws.max_hits = max(ws.max_hits, hits);
+    return (kKind == kArgmin) ? t_hi : acc;
+  }
+  __device__ float argmin(float3 o, float3 d, uint64_t key, ScatterAlbedo* sa) {
+    sa->valid = false;  // the plain megakernel evaluates the albedo with its own point query
+    return ray<kArgmin>(o, d, key);
+  }
+  __device__ float transmittance(float3 o, float3 d) {
+    const float tau = ray<kTau>(o, d, 0ull);
+    return tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
+  }
+  __device__ float3 albedo(float3 x, uint32_t& overlap) {
+    uint32_t stack[kBinStack];
+    int sp = 0;
+    uint32_t node = S.bin_root;
+    float aw = 0.f;
+    float3 a = f3(0.f, 0.f, 0.f);
+    uint32_t cnt = 0;
+    while (true) {
+      if (measure) ws.nodes++;
+      const float4* nd = S.bin + 4u * node;
+      const float4 bl[2] = {__ldg(nd), __ldg(nd + 2)};
+      const float4 bh[2] = {__ldg(nd + 1), __ldg(nd + 3)};
+      int n_inner = 0;
+      uint32_t inner[2];
+      for (int c = 0; c < 2; ++c) {
+        const uint32_t r = __float_as_uint(bl[c].w);
+        if (r == kEmptyRef || !box_contains(bl[c], bh[c], x)) continue;
+        if (ref_is_leaf(r)) {
+          const uint32_t pi = r & ~kLeafBit;
+          if (measure) ws.geo_loads++;
+          const PrimGeo g = load_geo(S.prims, pi);
+          float r2;
+          if constexpr (kAcc) {
+            const double Dx = (double)x.x - g.a.x, Dy = (double)x.y - g.a.y, Dz = (double)x.z - g.a.z;
+            const double yx = g.a.w * Dx + g.b.x * Dy + g.b.y * Dz;
+            const double yy = g.b.z * Dx + g.b.w * Dy + g.c.x * Dz;
+            const double yz = g.c.y * Dx + g.c.z * Dy + g.c.w * Dz;
+            r2 = (float)(yx * yx + yy * yy + yz * yz);
+          } else {
+            const float3 y = whiten(g, sub(x, f3(g.a.x, g.a.y, g.a.z)));
+            r2 = dot3(y, y);
+          }
+          if (r2 <= kExtent2) {
+            const float wgt = g.icf * expf(-0.5f * r2);
+            aw += wgt;
+            a = add(a, mul(load_albedo(S.prims, pi), wgt));
+            ++cnt;
+          }
+        } else {
+          inner[n_inner++] = r;
+        }
+      }
+      if (n_inner == 2) {
+        if (sp >= kBinStack) {
+          status |= kStatusStackOverflow;
+          break;
+        }
+        stack[sp++] = inner[1];
+        node = inner[0];
+        continue;
+      }
+      if (n_inner == 1) {
+        node = inner[0];
+        continue;
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+    overlap = cnt;
+    if (!(aw > 0.f)) return f3(0.f, 0.f, 0.f);
+    return mul(a, __frcp_rn(aw));
+  }
+};
+
+}  // namespace vp

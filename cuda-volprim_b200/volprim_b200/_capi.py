@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libvolprim_b200.so"
 VP_OK = 0
 VP_MEMORY_HOST, VP_MEMORY_DEVICE = 0, 1
 VP_NEE_MIS, VP_NEE_PHASE, VP_NEE_RIS, VP_NEE_NONE = 0, 1, 2, 3
-VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL = 0, 1
+VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL, VP_ENGINE_WAVEFRONT = 0, 1, 2
 VP_PRECISION_AUTO, VP_PRECISION_FAST, VP_PRECISION_ACCURATE = 0, 1, 2
 
 ERROR_NAMES = {
@@ -103,6 +103,8 @@ class vp_render_stats(C.Structure):
         ("leaves_visited", C.c_uint64),
         ("prim_tests", C.c_uint64),
         ("geo_loads", C.c_uint64),
+        ("query_nodes", C.c_uint64 * 3),
+        ("query_leaves", C.c_uint64 * 3),
         ("max_hits_per_ray", C.c_uint32),
         ("max_point_overlap", C.c_uint32),
         ("device_status", C.c_uint32),
@@ -110,7 +112,13 @@ class vp_render_stats(C.Structure):
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        out = {}
+        for name, _ in self._fields_:
+            if name == "reserved":
+                continue
+            v = getattr(self, name)
+            out[name] = list(v) if isinstance(v, C.Array) else v
+        return out
 
 
 P = C.c_void_p

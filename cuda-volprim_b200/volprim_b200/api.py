@@ -270,7 +270,7 @@ class Config:
     ris_num_candidates: int = 6
     measure_caps: bool = False
     nee: str = "mis"            # "mis" | "phase" | "ris" | "none"  (use_ris=True selects "ris")
-    engine: str = "warp"        # "warp" | "megakernel"
+    engine: str = "wavefront"   # "wavefront" | "warp" | "megakernel"
     precision: str = "auto"     # "auto" | "fast" | "accurate"
     batch_spp: int = 16         # BATCH_SIZE (renderer.cpp:32)
 
@@ -286,7 +286,7 @@ class Config:
         p.nee_mode = {"mis": 0, "phase": 1, "ris": 2, "none": 3}[nee]
         p.ris_candidates = self.ris_num_candidates
         p.batch_spp = self.batch_spp
-        p.engine = {"warp": 0, "megakernel": 1}[self.engine]
+        p.engine = {"warp": 0, "megakernel": 1, "wavefront": 2}[self.engine]
         p.precision = {"auto": 0, "fast": 1, "accurate": 2}[self.precision]
         p.measure = 1 if self.measure_caps else 0
         return p

@@ -59,8 +59,10 @@ typedef enum vp_nee_mode {
 
 /* Which GPU engine runs the path loop. */
 typedef enum vp_engine {
-  VP_ENGINE_WARP = 0,      /* persistent kernel, one path per warp, warp-cooperative BVH32 traversal */
-  VP_ENGINE_MEGAKERNEL = 1 /* plain per-pixel megakernel, thread-per-ray binary-LBVH traversal */
+  VP_ENGINE_WARP = 0,       /* persistent kernel, one path per warp, warp-cooperative BVH32 traversal */
+  VP_ENGINE_MEGAKERNEL = 1, /* plain per-pixel megakernel, thread-per-ray binary-LBVH traversal */
+  VP_ENGINE_WAVEFRONT = 2   /* wavefront of persistent stage kernels over compacted path queues,
+                               warp-cooperative BVH32 traversal; same results as VP_ENGINE_WARP */
 } vp_engine;
 
 /* Precision of the per-(ray, Gaussian) chord set-up (whitening transform, closest approach,
@@ -211,6 +213,9 @@ typedef struct vp_render_stats {
   uint64_t prim_tests;         /* Gaussian 3-sigma boxes tested at BVH32 leaves (measure != 0) */
   uint64_t geo_loads;          /* Gaussian whitening records loaded for a chord or point test
                                   (box hits)                      (measure != 0) */
+  uint64_t query_nodes[3];     /* inner-node visits per query kind: [0] free-flight argmin,
+                                  [1] transmittance, [2] albedo point query (measure != 0) */
+  uint64_t query_leaves[3];    /* BVH32 leaf visits per query kind (measure != 0) */
   uint32_t max_hits_per_ray;   /* largest candidate count of one query (measure != 0) */
   uint32_t max_point_overlap;  /* largest Gaussian overlap at a path vertex (measure != 0) */
   uint32_t device_status;      /* 0 = fine; else an error word raised by a kernel */

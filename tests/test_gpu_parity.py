@@ -100,7 +100,7 @@ def test_single_gaussian_closed_form(vp_ctx):
             np.testing.assert_allclose(-np.log(T), tau, rtol=2e-6, atol=2e-7)
 
 
-@pytest.mark.parametrize("engine", ["warp", "megakernel"])
+@pytest.mark.parametrize("engine", ["warp", "megakernel", "wavefront"])
 def test_absorption_image_matches_fp64(vp_ctx, engine):
     """128x128x16 absorption render of the 256-Gaussian workload vs the FP64 oracle, replaying
     the reference's PCG32 jitter stream per (pixel, sample)."""
@@ -143,10 +143,11 @@ def _render_both(vp_ctx, g, cfg, envimg, sigma=2.0, rng_mode="keyed", engine="wa
     return img, ref, r.last_stats
 
 
+@pytest.mark.parametrize("engine", ["warp", "wavefront"])
 @pytest.mark.parametrize("nee", ["mis", "phase", "ris", "none"])
-def test_scatter_matches_keyed_oracle(vp_ctx, nee):
+def test_scatter_matches_keyed_oracle(vp_ctx, nee, engine):
     g, cfg, env = small_scatter_workload(nee=nee, hg=0.3 if nee == "phase" else 0.0)
-    img, ref, st = _render_both(vp_ctx, g, cfg, env)
+    img, ref, st = _render_both(vp_ctx, g, cfg, env, engine=engine)
     assert st["device_status"] == 0
     scale = max(float(ref.mean()), 1e-6)
     rel = np.abs(img - ref) / np.maximum(np.abs(ref), 0.05 * scale)
@@ -156,14 +157,17 @@ def test_scatter_matches_keyed_oracle(vp_ctx, nee):
 
 
 def test_engines_agree(vp_ctx):
+    """The wavefront engine runs the warp engine's shading code and queries in the same order:
+    identical images.  The megakernel's binary-BVH sums differ only in FP32 summation order."""
     g, cfg, env = small_scatter_workload(seed=5, spp=32)
     cam = scenes.negz_camera(3.0, 40.0)
-    imgs = []
-    for eng in ("warp", "megakernel"):
+    imgs = {}
+    for eng in ("warp", "megakernel", "wavefront"):
         cfg.engine = eng
-        imgs.append(vp.Renderer(cfg, g, cam, env=env, sigma_multiplier=2.0, ctx=vp_ctx).render()[..., :3])
-    scale = float(imgs[0].mean())
-    assert np.abs(imgs[0] - imgs[1]).mean() / scale < 1e-4
+        imgs[eng] = vp.Renderer(cfg, g, cam, env=env, sigma_multiplier=2.0, ctx=vp_ctx).render()[..., :3]
+    scale = float(imgs["warp"].mean())
+    assert np.array_equal(imgs["warp"], imgs["wavefront"])
+    assert np.abs(imgs["warp"] - imgs["megakernel"]).mean() / scale < 1e-4
 
 
 def test_scatter_statistical_vs_reference_order(vp_ctx):
@@ -186,7 +190,7 @@ def test_scatter_statistical_vs_reference_order(vp_ctx):
     assert abs(ma.mean() - mb.mean()) / mb.mean() < 0.01
 
 
-def _furnace(vp_ctx, g, sigma, cam, nee="mis", hg=0.0, engine="warp", spp=256):
+def _furnace(vp_ctx, g, sigma, cam, nee="mis", hg=0.0, engine="warp", spp=2048):
     cfg = vp.Config(num_samples_per_pixel=spp, image_width=64, image_height=64, seed=1, hg_g=hg,
                     max_bounces=1024, nee=nee, engine=engine)
     img = vp.Renderer(cfg, g, cam, env=None, sigma_multiplier=sigma, ctx=vp_ctx).render()[..., :3].astype(np.float64)
@@ -200,7 +204,8 @@ def _furnace(vp_ctx, g, sigma, cam, nee="mis", hg=0.0, engine="warp", spp=256):
 
 
 @pytest.mark.parametrize("nee,hg,engine", [("mis", 0.0, "warp"), ("mis", 0.6, "warp"), ("phase", 0.0, "warp"),
-                                           ("ris", 0.0, "warp"), ("none", 0.0, "warp"), ("mis", 0.0, "megakernel")])
+                                           ("ris", 0.0, "warp"), ("none", 0.0, "warp"), ("mis", 0.0, "megakernel"),
+                                           ("mis", 0.0, "wavefront")])
 def test_white_furnace_cluster(vp_ctx, nee, hg, engine):
     """Albedo 1 everywhere in a unit constant environment: every pixel must be 1
     (Russian roulette from depth 12 keeps it unbiased)."""
