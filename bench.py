@@ -213,7 +213,8 @@ def run_ours(args):
     img = vp.ProgressiveImage(ctx, W, H)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    base = rank * args.spp
+    from volprim_b200 import distributed as D
+    base, _ = D.sample_range(rank, world, args.spp)
 
     def step(i):  # one launch batch of BATCH_SPP samples
         off = base + (i * BATCH_SPP) % args.spp
@@ -245,14 +246,13 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             ends[i].record(stream)
     reduce_ms = 0.0
-    if dist:  # the job's one exchange: mean of the per-rank images (equal sample counts)
+    if dist:  # the job's one exchange: count-weighted mean of the per-rank images
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         acc = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
         ev0.record(stream)
         _capi.check(_capi.lib.vp_image_read(img.handle, acc.data_ptr(), _capi.VP_MEMORY_DEVICE))
         with torch.cuda.stream(stream):
-            dist.all_reduce(acc)
-            acc /= world
+            acc = D.combine(acc, BATCH_SPP * args.steps)
             ev1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall

@@ -146,6 +146,19 @@ vp_status check_params(const vp_render_params* p) {
   return VP_OK;
 }
 
+__global__ void k_camera_rays(CameraView C, ParamsView P, const uint32_t* __restrict__ px,
+                              const uint32_t* __restrict__ py, const uint32_t* __restrict__ sample, uint32_t n,
+                              float* __restrict__ o, float* __restrict__ d) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t pix = (uint64_t)py[i] * P.width + px[i];
+  Pcg32 rng = pcg_init(P.seed, seq_hash(pix * (uint64_t)P.spp_total + sample[i]));
+  float3 oo, dd;
+  camera_ray(C, P, px[i], py[i], rng, oo, dd);
+  o[3 * i] = oo.x, o[3 * i + 1] = oo.y, o[3 * i + 2] = oo.z;
+  d[3 * i] = dd.x, d[3 * i + 1] = dd.y, d[3 * i + 2] = dd.z;
+}
+
 __global__ void k_mean_to_rgba(const float4* __restrict__ mean, float4* __restrict__ out, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -504,6 +517,53 @@ vp_status vp_transmittance(vp_scene* s, const float* origins, const float* dirs,
   Counters c{};
   VP_CUDA(cudaMemcpy(&c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost));
   if (c.status) return fail(VP_ERROR_DEVICE_STATUS, "transmittance kernel raised device status " + std::to_string(c.status));
+  return VP_OK;
+}
+
+vp_status vp_camera_rays(vp_context* ctx, const vp_camera* cam, const vp_render_params* p, const uint32_t* px,
+                         const uint32_t* py, const uint32_t* sample, uint32_t n, float* out_o, float* out_d,
+                         int32_t memory) {
+  if (!ctx || !cam || !p || (n > 0 && (!px || !py || !sample || !out_o || !out_d)))
+    return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (p->width == 0 || p->height == 0 || p->spp == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "bad params");
+  if (n == 0) return VP_OK;
+  VP_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  CameraView cv;
+  build_camera(*cam, p->width, p->height, cv);
+  ParamsView P{};
+  P.width = p->width;
+  P.height = p->height;
+  P.spp_total = p->spp;
+  P.seed = p->seed;
+  P.filter_stddev = p->pixel_filter_stddev;
+  if (memory == VP_MEMORY_DEVICE) {
+    k_camera_rays<<<(n + 127) / 128, 128, 0, st>>>(cv, P, px, py, sample, n, out_o, out_d);
+    VP_CUDA(cudaGetLastError());
+    VP_CUDA(cudaStreamSynchronize(st));
+    return VP_OK;
+  }
+  if (memory != VP_MEMORY_HOST) return fail(VP_ERROR_INVALID_ARGUMENT, "bad memory kind");
+  uint32_t *dx = nullptr, *dy = nullptr, *ds = nullptr;
+  float *dof = nullptr, *ddf = nullptr;
+  vp_status r;
+  if ((r = dev_alloc(&dx, n, st)) || (r = dev_alloc(&dy, n, st)) || (r = dev_alloc(&ds, n, st)) ||
+      (r = dev_alloc(&dof, 3ull * n, st)) || (r = dev_alloc(&ddf, 3ull * n, st))) {
+    dev_free(dx, st), dev_free(dy, st), dev_free(ds, st), dev_free(dof, st), dev_free(ddf, st);
+    return r;
+  }
+  cudaError_t e = cudaMemcpyAsync(dx, px, 4ull * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, py, 4ull * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ds, sample, 4ull * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    k_camera_rays<<<(n + 127) / 128, 128, 0, st>>>(cv, P, dx, dy, ds, n, dof, ddf);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out_o, dof, 12ull * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out_d, ddf, 12ull * n, cudaMemcpyDeviceToHost, st);
+  dev_free(dx, st), dev_free(dy, st), dev_free(ds, st), dev_free(dof, st), dev_free(ddf, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "vp_camera_rays");
   return VP_OK;
 }
 

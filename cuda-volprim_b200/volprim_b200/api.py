@@ -60,6 +60,17 @@ class Context:
     def synchronize(self) -> None:
         check(lib.vp_context_synchronize(self.handle))
 
+    def camera_rays(self, camera: "Camera", config: "Config", px, py, sample):
+        """Camera rays of (pixel x, pixel y, sample) triples, as the renderer generates them."""
+        px, py, sample = (np.ascontiguousarray(a, dtype=np.uint32).reshape(-1) for a in (px, py, sample))
+        n = px.size
+        o = np.empty((n, 3), np.float32)
+        d = np.empty((n, 3), np.float32)
+        cam, p = camera.to_c(), config.to_c()
+        check(lib.vp_camera_rays(self.handle, C.byref(cam), C.byref(p), px.ctypes.data, py.ctypes.data,
+                                 sample.ctypes.data, n, o.ctypes.data, d.ctypes.data, _capi.VP_MEMORY_HOST))
+        return o, d
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             lib.vp_context_destroy(self.handle)

@@ -260,6 +260,14 @@ vp_status vp_transmittance(vp_scene* scene, const float* origins, const float* d
                            int32_t precision, int32_t engine, float* out_transmittance,
                            int32_t memory);
 
+/* Camera rays of n (pixel x, pixel y, sample index) triples for a params->spp-sample render:
+ * the per-(pixel, sample) PCG32 stream seeded as the reference's raygen
+ * (device/entry/raygen.cuh:82-99, device/core/random.cuh:33-72) and the jittered ray of
+ * device/params/camera.h:43-57.  origins[3n], dirs[3n]. */
+vp_status vp_camera_rays(vp_context* ctx, const vp_camera* camera, const vp_render_params* params,
+                         const uint32_t* px, const uint32_t* py, const uint32_t* sample, uint32_t n,
+                         float* out_origins, float* out_dirs, int32_t memory);
+
 /* Albedo at n points: the sigma_t * pdf-weighted mean albedo of the Gaussians whose 3-sigma
  * ellipsoid contains each point, and how many contain it.  Replaces evaluate_albedo over the
  * active set (device/core/sampling.cuh:257-283, 422-458) and point_inside_bvh_bound

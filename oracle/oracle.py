@@ -68,6 +68,10 @@ def lib() -> C.CDLL:
         L.or_render.argtypes = [C.c_void_p, C.c_void_p, F, U, F, C.c_uint32, C.c_uint32, C.c_uint32,
                                 C.c_uint32, C.c_int, F]
         L.or_albedo_at.argtypes = [C.c_void_p, F, C.c_uint32, F, U]
+        L.or_transform.argtypes = [C.c_void_p, C.c_uint32, F, F, F]
+        L.or_morton3d.restype = C.c_uint32
+        L.or_morton3d.argtypes = [F, F, F]
+        L.or_scene_order.argtypes = [C.c_void_p, U]
         L.or_max_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -96,6 +100,16 @@ class OracleScene:
         tau = np.empty(n, np.float64)
         lib().or_transmittance_fp64(self.h, _p(o), _p(d), n, _p(T, D), _p(tau, D))
         return T, tau
+
+    def transform(self, index, pos, direction):
+        out = np.empty(7, np.float32)
+        lib().or_transform(self.h, int(index), _p(_f(pos)), _p(_f(direction)), _p(out))
+        return out
+
+    def order(self):
+        out = np.empty(self.n, np.uint32)
+        lib().or_scene_order(self.h, _p(out, U))
+        return out
 
     def albedo_at(self, points):
         p = _f(points).reshape(-1)
@@ -207,6 +221,10 @@ def render(scene: OracleScene, env: OracleEnv, cam16, config, y0=0, y1=None, s0=
     out = np.empty((y1 - y0) * W * 3, np.float32)
     secs = lib().or_render(scene.h, env.h, _p(_f(cam16)), _p(pu, U), _p(pf), y0, y1, s0, s1, int(threads), _p(out))
     return out.reshape(y1 - y0, W, 3), secs
+
+
+def morton3d(pos, scene_min, inv_extent) -> int:
+    return int(lib().or_morton3d(_p(_f(pos)), _p(_f(scene_min)), _p(_f(inv_extent))))
 
 
 def max_threads() -> int:

@@ -655,8 +655,23 @@ struct Bvh {
   }
 };
 
+// Morton code of the reference's host sort (include/thesis/host/utils/math.h:103-131).
+inline uint32_t expand_bits(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+inline uint32_t morton3d(F3 pos, F3 scene_min, F3 inv_extent) {
+  const F3 n = (pos - scene_min) * inv_extent;
+  auto q = [](float x) { return static_cast<uint32_t>(std::min(std::max(x, 0.0f), 1.0f) * 1023.0f); };
+  return (expand_bits(q(n.z)) << 2) | (expand_bits(q(n.y)) << 1) | expand_bits(q(n.x));
+}
+
 struct Scene {
   std::vector<Prim> prims;
+  std::vector<uint32_t> orig;  // scene order -> caller's index (keys the free-flight draws)
   // FP64 geometry for the closed-form oracle.
   std::vector<double> c64, W64, norm64;  // centre, whitening matrix (row-major 3x3), M/(2 pi prod s)
   std::vector<Box> boxes;
@@ -822,7 +837,7 @@ struct Tracer {
       }
       auto tau_of = [&](uint32_t i) {
         float chi;
-        if (alias) chi = static_cast<float>(keyed_u32(key, i)) * 2.3283064365386963e-10f;
+        if (alias) chi = static_cast<float>(keyed_u32(key, S.orig[i])) * 2.3283064365386963e-10f;
         else chi = rng.uniform();
         return -std::log(std::max(1.0f - chi, 1e-10f));
       };
@@ -1046,11 +1061,62 @@ void* or_scene_create(uint32_t n, const float* mean, const float* scale, const f
       b.hi[k] = mean[3 * i + k] + e + pad;
     }
   }
+  // The reference renders the Gaussians in its host Morton order (renderer.cpp:91-121: 30-bit
+  // codes of the centres over their bounds); its origin-inside scan draws in that order.  Ties
+  // keep the caller's order here (the reference's std::sort leaves them unspecified).
+  S->orig.resize(n);
+  std::iota(S->orig.begin(), S->orig.end(), 0u);
+  if (n > 1) {
+    F3 mn = mk(FLT_MAX, FLT_MAX, FLT_MAX), mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    for (const Prim& p : S->prims) {
+      mn = mk(std::min(mn.x, p.center.x), std::min(mn.y, p.center.y), std::min(mn.z, p.center.z));
+      mx = mk(std::max(mx.x, p.center.x), std::max(mx.y, p.center.y), std::max(mx.z, p.center.z));
+    }
+    const F3 ext = mx - mn;
+    const F3 inv = mk(1.0f / std::max(ext.x, 1e-30f), 1.0f / std::max(ext.y, 1e-30f), 1.0f / std::max(ext.z, 1e-30f));
+    std::vector<uint32_t> code(n);
+    for (uint32_t i = 0; i < n; ++i) code[i] = morton3d(S->prims[i].center, mn, inv);
+    std::stable_sort(S->orig.begin(), S->orig.end(), [&](uint32_t a, uint32_t b) { return code[a] < code[b]; });
+    Scene T;
+    T.prims.resize(n), T.c64.resize(3ull * n), T.W64.resize(9ull * n), T.norm64.resize(n), T.boxes.resize(n);
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t i = S->orig[k];
+      T.prims[k] = S->prims[i];
+      T.norm64[k] = S->norm64[i];
+      T.boxes[k] = S->boxes[i];
+      for (int c = 0; c < 3; ++c) T.c64[3ull * k + c] = S->c64[3ull * i + c];
+      for (int c = 0; c < 9; ++c) T.W64[9ull * k + c] = S->W64[9ull * i + c];
+    }
+    S->prims.swap(T.prims), S->c64.swap(T.c64), S->W64.swap(T.W64), S->norm64.swap(T.norm64), S->boxes.swap(T.boxes);
+  }
   if (use_bvh) S->bvh.build(S->boxes);
   return S;
 }
 
 void or_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+// Whitened position and direction of (pos, dir) for the caller's Gaussian `index`, and
+// point_inside_bvh_bound(pos): out7 = pos_local[3], dir_local[3], inside.
+void or_transform(void* sv, uint32_t index, const float* pos, const float* dir, float* out7) {
+  const Scene& S = *static_cast<Scene*>(sv);
+  uint32_t k = 0;
+  while (k < S.orig.size() && S.orig[k] != index) ++k;
+  const Prim& p = S.prims[k];
+  const F3 a = p.pos_local(mk(pos[0], pos[1], pos[2])), b = p.dir_local(mk(dir[0], dir[1], dir[2]));
+  out7[0] = a.x, out7[1] = a.y, out7[2] = a.z, out7[3] = b.x, out7[4] = b.y, out7[5] = b.z;
+  out7[6] = point_inside(mk(pos[0], pos[1], pos[2]), p) ? 1.0f : 0.0f;
+}
+
+uint32_t or_morton3d(const float* pos, const float* scene_min, const float* inv_extent) {
+  return morton3d(mk(pos[0], pos[1], pos[2]), mk(scene_min[0], scene_min[1], scene_min[2]),
+                  mk(inv_extent[0], inv_extent[1], inv_extent[2]));
+}
+
+// Scene order (the reference's Morton order) as caller indices.
+void or_scene_order(void* sv, uint32_t* out) {
+  const Scene& S = *static_cast<Scene*>(sv);
+  std::copy(S.orig.begin(), S.orig.end(), out);
+}
 
 void* or_env_create(const float* rgb, uint32_t W, uint32_t H, uint32_t ch) {
   auto* e = new Env();

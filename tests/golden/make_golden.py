@@ -1,0 +1,118 @@
+"""Generates tests/golden/reference_pin.json from the reference's OWN code.
+
+The reference's host-compilable headers (Primitive constructor and whitening transforms,
+include/thesis/device/params/primitive.h:70-122; point_inside_bvh_bound,
+include/thesis/common/geometry/intersection.h:56-61; host camera build,
+include/thesis/host/params/camera.h:106-216; morton3D, include/thesis/host/utils/math.h:103-131)
+are compiled by oracle/Makefile into oracle/_ref/libref_pin.so; this script calls them on fixed
+inputs and stores inputs and outputs (float32 bit patterns, so comparisons are exact).  It also
+stores the single-Gaussian closed form of experiments/mitsuba-reference/single_gaussian_analytic.py
+:78-80 (with the renderer's 3-sigma truncation) and the published PCG32 test vector.
+
+Run from the repository root (needs the reference sources, so only where they are mounted):
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path[:0] = [str(ROOT / "oracle"), str(ROOT / "cuda-volprim_b200")]
+
+import oracle as O  # noqa: E402
+from volprim_b200 import scenes  # noqa: E402
+
+
+def bits(a) -> list[int]:
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).reshape(-1).tolist()
+
+
+def f32p(a):
+    return O._p(O._f(a))
+
+
+def primitive_cases():
+    rng = np.random.default_rng(2024)
+    g = scenes.absorption_gaussians(256, 0)
+    cases = []
+    for i in range(24):  # the 256-Gaussian absorption workload's first Gaussians
+        cases.append((g.mean[i], g.scale[i], g.quat_wxyz[i], rng.uniform(0, 1, 3), float(g.density[i])))
+    half = 0.5 * math.radians(30.0)  # SG_TRANSFORMED (test/scenes/single_gaussian.cpp:128-139)
+    cases.append(((0, 0, 0), (1.0, 0.5, 0.75), (math.cos(half), 0, 0, math.sin(half)), (0.9, 0.9, 0.9), 7.5))
+    cases.append(((0, 0, 0), (1, 1, 1), (1, 0, 0, 0), (0, 0, 0), 7.5))
+    cases.append(((0.3, -0.2, 1.7), (0.02, 0.3, 0.004), (2.0, -1.0, 0.5, 3.0), (1, 0.5, 0.25), 0.125))
+    cases.append(((-5.0, 4.0, 2.5), (3.0, 2.0, 1.0), (0.1, 0.2, 0.3, 0.4), (0.2, 0.4, 0.6), 1e3))
+    for _ in range(8):
+        q = rng.normal(size=4)
+        cases.append((rng.uniform(-2, 2, 3), np.exp(rng.normal(math.log(0.05), 0.8, 3)), q * rng.uniform(0.5, 2.0),
+                      rng.uniform(0, 1, 3), float(np.exp(rng.normal(0, 1)))))
+    return cases
+
+
+def main():
+    O.build()
+    R = O.ref_lib()
+    if R is None:
+        raise SystemExit("oracle/_ref/libref_pin.so is missing: the reference sources are needed")
+    out = {"source": "reference headers compiled by oracle/Makefile (oracle/ref_pin.cpp)"}
+    prims = []
+    rec = np.empty(20, np.float32)
+    tr = np.empty(7, np.float32)
+    rng = np.random.default_rng(7)
+    for (m, s, q, a, M) in primitive_cases():
+        R.ref_primitive(f32p(m), f32p(s), f32p(q), f32p(a), float(np.float32(M)), O._p(rec))
+        pts = []
+        for _ in range(4):
+            pos = np.asarray(m, np.float32) + rng.normal(0, 2.0 * float(np.max(s)), 3).astype(np.float32)
+            d = rng.normal(size=3)
+            d = (d / np.linalg.norm(d)).astype(np.float32)
+            R.ref_transform(f32p(m), f32p(s), f32p(q), float(np.float32(M)), f32p(pos), f32p(d), O._p(tr))
+            pts.append({"pos": bits(pos), "dir": bits(d), "out": bits(tr)})
+        prims.append({"mean": bits(m), "scale": bits(s), "quat_wxyz": bits(q), "albedo": bits(a),
+                      "density": bits([M])[0], "record": bits(rec), "transforms": pts})
+    out["primitives"] = prims
+    cams = []
+    cam_cases = [
+        ("absorption_256 negz", (0, 0, -3.5), (0, 0, 0), (0, 1, 0), 40.0, 2.0, 0, 128, 128),
+        ("default", (0, 0, -1), (0, 0, 0), (0, 1, 0), 90.0, 2.0, 0, 1000, 750),
+        ("asset diag", (2.1, 1.75, -2.1), (0, 0, 0), (0, 1, 0), 40.0, 2.0, 0, 512, 512),
+        ("asset posy", (0, 3.5, 0), (0, 0, 0), (0, 0, 1), 40.0, 2.0, 0, 512, 512),
+        ("showcase 900x600", (0.7, 0.3, -3.2), (0.1, -0.1, 0.2), (0, 1, 0), 35.0, 2.0, 0, 900, 600),
+        ("single_gaussian ortho", (0, 0, -5), (0, 0, 0), (0, 1, 0), 90.0, 6.0, 1, 256, 256),
+        ("cluster n5 ortho", (0, 0, -6), (0, 0, 0), (0, 1, 0), 90.0, 8.0, 1, 256, 256),
+        ("ortho oblique", (3, 2, -4), (0, 0.5, 0), (0, 1, 0), 90.0, 4.5, 1, 320, 200),
+    ]
+    c16 = np.empty(16, np.float32)
+    for name, eye, at, up, fov, oh, ortho, W, H in cam_cases:
+        R.ref_camera(f32p(eye), f32p(at), f32p(up), float(fov), float(oh), int(ortho), W, H, O._p(c16))
+        cams.append({"name": name, "eye": bits(eye), "lookat": bits(at), "up": bits(up), "vfov": bits([fov])[0],
+                     "ortho_height": bits([oh])[0], "orthographic": ortho, "width": W, "height": H,
+                     "out": bits(c16)})
+    out["cameras"] = cams
+    mort = []
+    smin = np.array([-1.0, -0.5, -0.7], np.float32)
+    inv = (1.0 / np.array([2.0, 1.0, 1.4], np.float32)).astype(np.float32)
+    for p in rng.uniform([-1.1, -0.6, -0.8], [1.1, 0.6, 0.8], (32, 3)).astype(np.float32):
+        mort.append({"pos": bits(p), "code": int(R.ref_morton3d(f32p(p), f32p(smin), f32p(inv)))})
+    out["morton"] = {"scene_min": bits(smin), "inv_extent": bits(inv), "cases": mort}
+    # closed form: unit isotropic Gaussian of mass M, 3-sigma truncated chord at distance d
+    M = 7.5
+    ds = np.linspace(0.0, 2.99, 24)
+    out["single_gaussian"] = {"mass": M, "d": ds.tolist(),
+                              "tau": [M / (2 * math.pi) * math.exp(-d * d / 2) * math.erf(math.sqrt((9 - d * d) / 2))
+                                      for d in ds]}
+    # PCG32 reference implementation demo (pcg32_srandom_r(42, 54)): first six outputs
+    out["pcg32"] = {"seed": 42, "sequence": 54,
+                    "outputs": [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]}
+    path = Path(__file__).resolve().parent / "reference_pin.json"
+    path.write_text(json.dumps(out, indent=1))
+    print(f"wrote {path} ({path.stat().st_size} bytes)")
+
+
+if __name__ == "__main__":
+    main()

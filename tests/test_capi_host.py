@@ -1,0 +1,85 @@
+"""CPU: the C-ABI library loads, exports every entry point include/volprim_b200.h declares, and its
+host-only entry points behave (no device work is issued here)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import volprim_b200 as vp
+from volprim_b200 import _capi
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "volprim_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:vp_status|const char\*)\s+(vp_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for must in ("vp_context_create", "vp_scene_create", "vp_env_create", "vp_render", "vp_render_accumulate",
+                 "vp_transmittance", "vp_albedo_at", "vp_camera_rays", "vp_normalize_accumulator",
+                 "vp_last_error_string"):
+        assert must in names
+    assert len(names) >= 25
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(str(_capi.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    nm = subprocess.run(["nm", "-D", "--defined-only", str(_capi.LIB_PATH)], capture_output=True, text=True)
+    if nm.returncode == 0:
+        exported = {ln.split()[-1] for ln in nm.stdout.splitlines() if ln.strip()}
+        assert set(declared_functions()) <= exported
+
+
+def test_python_bindings_cover_the_header():
+    assert set(declared_functions()) == set(_capi.SIGNATURES)
+
+
+def test_version_and_defaults():
+    mj, mn = C.c_int32(), C.c_int32()
+    _capi.check(_capi.lib.vp_version(C.byref(mj), C.byref(mn)))
+    assert (mj.value, mn.value) == (0, 1)
+    p = _capi.vp_render_params()
+    _capi.check(_capi.lib.vp_render_params_default(C.byref(p)))
+    # app::Config defaults (include/thesis/host/app/config.h:119-136), BATCH_SIZE (renderer.cpp:32)
+    assert (p.width, p.height, p.spp, p.seed, p.max_bounces, p.rr_depth) == (1000, 750, 1, 42, 128, 12)
+    assert abs(p.rr_max_survival - 0.99) < 1e-7 and abs(p.hg_g - 0.85) < 1e-7
+    assert p.firefly_clamp == 0.0 and p.pixel_filter_stddev == 0.0
+    assert p.nee_mode == vp.VP_NEE_MIS and p.ris_candidates == 6 and p.batch_spp == 16
+    assert p.engine == _capi.VP_ENGINE_WAVEFRONT
+
+
+def test_null_arguments_are_errors_not_crashes():
+    assert _capi.lib.vp_context_create(0, None) == -1
+    assert b"NULL" in _capi.lib.vp_last_error_string() or _capi.lib.vp_last_error_string()
+    assert _capi.lib.vp_scene_create(None, None, C.c_float(1.0), None) == -1
+    assert _capi.lib.vp_render(None, None, None, None, None, 0, None) == -1
+    assert _capi.lib.vp_render_params_default(None) == -1
+    with pytest.raises(_capi.VpError):
+        _capi.check(_capi.lib.vp_render_params_default(None))
+
+
+def test_config_maps_to_c_params():
+    cfg = vp.Config(num_samples_per_pixel=256, image_width=512, image_height=256, seed=9, max_bounces=64,
+                    rr_depth=12, hg_g=0.0, use_ris=True, ris_num_candidates=4, engine="megakernel",
+                    precision="accurate", batch_spp=8, measure_caps=True)
+    p = cfg.to_c()
+    assert (p.width, p.height, p.spp, p.seed, p.max_bounces) == (512, 256, 256, 9, 64)
+    assert p.nee_mode == vp.VP_NEE_RIS and p.ris_candidates == 4
+    assert p.engine == vp.VP_ENGINE_MEGAKERNEL and p.precision == vp.VP_PRECISION_ACCURATE
+    assert p.batch_spp == 8 and p.measure == 1
+
+
+def test_struct_layouts_match_header():
+    # sizes of the C structs as the header lays them out (x86-64 System V)
+    assert C.sizeof(_capi.vp_gaussians) == 56
+    assert C.sizeof(_capi.vp_camera) == 48
+    assert C.sizeof(_capi.vp_render_params) == 64

@@ -299,6 +299,25 @@ def test_leaf_boundaries(vp_ctx, n):
     assert info["count"] == n and info["wide_depth"] >= 1
 
 
+@pytest.mark.parametrize("ortho", [False, True])
+def test_camera_rays_bit_exact(vp_ctx, ortho):
+    """Host camera build + device jitter/ray generation equal the oracle (whose camera equals the
+    reference's headers bit for bit) exactly, for the box filter."""
+    cam = (vp.Camera.orthographic_camera((0.5, 1.0, -5.0), (0, 0, 0), (0, 1, 0), 6.0) if ortho
+           else vp.Camera.perspective((0.7, 0.3, -3.2), (0.1, -0.1, 0.2), (0, 1, 0), 35.0))
+    cfg = vp.Config(num_samples_per_pixel=16, image_width=90, image_height=60, seed=1234)
+    rng = np.random.default_rng(0)
+    px, py, sm = rng.integers(0, 90, 5000), rng.integers(0, 60, 5000), rng.integers(0, 16, 5000)
+    o, d = vp_ctx.camera_rays(cam, cfg, px, py, sm)
+    oo, od = O.camera_rays(O.camera16(cam, 90, 60), 90, 16, 1234, px, py, sm)
+    assert np.array_equal(o.view(np.uint32), oo.view(np.uint32))
+    assert np.array_equal(d.view(np.uint32), od.view(np.uint32))
+    cfg.pixel_filter_stddev = 0.5  # Gaussian pixel filter: libm vs CUDA log/sin/cos, ~ulp
+    o, d = vp_ctx.camera_rays(cam, cfg, px, py, sm)
+    oo, od = O.camera_rays(O.camera16(cam, 90, 60), 90, 16, 1234, px, py, sm, filter_stddev=0.5)
+    np.testing.assert_allclose(d, od, atol=2e-6)
+
+
 def test_invalid_inputs_raise(vp_ctx):
     g = vp.Gaussians(np.zeros((3, 3)), np.array([[1, 1, 1], [1, -1, 1], [1, 1, 1]]), np.tile([1.0, 0, 0, 0], (3, 1)),
                      np.ones(3))
