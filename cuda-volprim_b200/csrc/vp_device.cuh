@@ -165,10 +165,25 @@ __device__ __forceinline__ uint32_t keyed_u32(uint64_t key, uint32_t idx) {
   z ^= z >> 31;
   return static_cast<uint32_t>(z >> 32);
 }
+// exp / log of the per-Gaussian terms: CUDA's full-accuracy functions for ACCURATE, the
+// hardware-approximation intrinsics for FAST (the reference builds with -use_fast_math, which
+// maps expf/logf to these, cmake/OptiX-IR.cmake:40-88).
+template <bool kAcc>
+__device__ __forceinline__ float vexp(float x) {
+  if constexpr (kAcc) return expf(x);
+  else return __expf(x);
+}
+template <bool kAcc>
+__device__ __forceinline__ float vlog(float x) {
+  if constexpr (kAcc) return logf(x);
+  else return __logf(x);
+}
+
 // tau = -log(max(1 - chi, 1e-10)), chi uniform (sample_free_flight_tau, sampling.cuh:310-313)
+template <bool kAcc>
 __device__ __forceinline__ float free_flight_tau(uint64_t key, uint32_t idx) {
   const float chi = __uint2float_rn(keyed_u32(key, idx)) * 2.3283064365386963e-10f;
-  return -logf(fmaxf(1.0f - chi, 1e-10f));
+  return -vlog<kAcc>(fmaxf(1.0f - chi, 1e-10f));
 }
 
 // ---- Gaussian record access ----------------------------------------------------------------
@@ -285,22 +300,24 @@ __device__ __forceinline__ float erf_diff(float a, float b) {
 
 // Optical depth of one Gaussian over the ray segment [max(t_in, t_lo), t_out]
 // (Primitive::optical_depth, primitive.h:249-318; zero below RAY_SEGMENT_MIN_LENGTH).
+template <bool kAcc>
 __device__ __forceinline__ float chord_tau(float tc, float rw, float d2, float h, float u0,
                                            float t_start, float t_out, float icf) {
   (void)tc;
   if (t_out - t_start <= kSegmentMin) return 0.0f;
-  return icf * rw * expf(-0.5f * d2) * erf_diff(u0, h);
+  return icf * rw * vexp<kAcc>(-0.5f * d2) * erf_diff(u0, h);
 }
 
 // Analog free flight inside one Gaussian, restricted to t >= segment start, with the
 // reference's acceptance rules (argmin_scatter_distance, sampling.cuh:350-415): +inf when the
 // remaining mass is below tau (primitive.h:174,235); an entry hit's FP undershoot below its
 // entry is clamped to the entry (sampling.cuh:392-394); valid only in [0, t_out].
+template <bool kAcc>
 __device__ __forceinline__ float chord_free_flight(float tc, float rw, float d2, float h,
                                                    float u0, float t_in, float t_out, float icf,
                                                    float tau) {
   (void)h;
-  const float K = icf * rw * expf(-0.5f * d2);
+  const float K = icf * rw * vexp<kAcc>(-0.5f * d2);
   const float raw = erff(u0 * kInvSqrt2) + tau / K;
   if (!(raw <= 1.0f)) return kInf;  // raw > 1 (or NaN): no scatter in this Gaussian
   const float arg = fmaxf(raw, -1.0f);

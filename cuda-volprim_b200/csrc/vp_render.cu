@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
                                                      Counters* __restrict__ ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap), S.stack_cap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, kHitCap), S.stack_cap, kHitCap);
   const uint32_t n_pix = P.width * P.height;
   uint32_t status = 0;
   WarpStats ws;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_tau_warp(SceneView S, const float* __re
                                                   Counters* __restrict__ ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap), S.stack_cap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, 32), S.stack_cap, 32);
   uint32_t status = 0;
   WarpStats ws;
   while (true) {
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_albedo_warp(SceneView S, const float* _
                                                      unsigned int* __restrict__ work, Counters* __restrict__ ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap), S.stack_cap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, 32), S.stack_cap, 32);
   uint32_t status = 0;
   WarpStats ws;
   while (true) {
@@ -294,7 +294,7 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
   cudaStream_t st = ctx->stream;
   if (engine == VP_ENGINE_WARP) {
     const int threads = 256;
-    const size_t smem = (size_t)(threads / 32) * (s->view.stack_cap * 8u + kHitCap * 9u * 4u);
+    const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kHitCap);
     if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the warp engine's shared-memory stack");
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
     if (P.accurate) {
@@ -330,7 +330,7 @@ vp_status launch_transmittance(vp_scene* s, const float* o, const float* d, uint
   if (n == 0) return VP_OK;
   if (engine == VP_ENGINE_WARP) {
     const int threads = 256;
-    const size_t smem = (size_t)(threads / 32) * (s->view.stack_cap * 8u + kHitCap * 9u * 4u);
+    const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, 32);
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
     if (accurate) {
       if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(k_tau_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -358,7 +358,7 @@ vp_status launch_albedo(vp_scene* s, const float* pts, uint32_t n, bool accurate
   if (n == 0) return VP_OK;
   if (engine == VP_ENGINE_WARP) {
     const int threads = 256;
-    const size_t smem = (size_t)(threads / 32) * (s->view.stack_cap * 8u + kHitCap * 9u * 4u);
+    const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, 32);
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
     if (accurate) {
       if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(k_albedo_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

