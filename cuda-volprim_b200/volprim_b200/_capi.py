@@ -152,6 +152,7 @@ SIGNATURES = {
                   C.POINTER(vp_render_stats)],
     "vp_transmittance": [P, P, P, C.c_uint32, C.c_int32, C.c_int32, P, C.c_int32],
     "vp_albedo_at": [P, P, C.c_uint32, C.c_int32, C.c_int32, P, P, C.c_int32],
+    "vp_transmittance_static": [P, P, P, C.c_uint32, C.c_int32, P, C.c_int32],
     "vp_camera_rays": [P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, P, P, C.c_uint32, P, P, C.c_int32],
     "vp_normalize_accumulator": [P, P, P, C.c_size_t, C.c_float, P],
 }

@@ -166,6 +166,26 @@ class Scene:
                                    out.ctypes.data, _capi.VP_MEMORY_HOST))
         return out
 
+    def transmittance_static(self, origins, dirs, precision: int = _capi.VP_PRECISION_AUTO):
+        """vp_transmittance_static: the transmittance query with no device allocation (its scratch
+        is a static device array for at most 65536 rays per call; calls must not overlap)."""
+        if _is_cuda_tensor(origins):
+            import torch
+            o = origins.detach().to(torch.float32).contiguous()
+            d = dirs.detach().to(torch.float32).contiguous()
+            n = o.numel() // 3
+            out = torch.empty(n, dtype=torch.float32, device=o.device)
+            check(lib.vp_transmittance_static(self.handle, o.data_ptr(), d.data_ptr(), n, precision, out.data_ptr(),
+                                              _capi.VP_MEMORY_DEVICE))
+            return out
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1)
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1)
+        n = o.size // 3
+        out = np.empty(n, dtype=np.float32)
+        check(lib.vp_transmittance_static(self.handle, o.ctypes.data, d.ctypes.data, n, precision, out.ctypes.data,
+                                          _capi.VP_MEMORY_HOST))
+        return out
+
     def albedo_at(self, points, precision: int = _capi.VP_PRECISION_AUTO, engine: int = _capi.VP_ENGINE_WARP):
         """(albedo rgb (n, 3), overlap count (n,)) at points (vp_albedo_at)."""
         p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1)

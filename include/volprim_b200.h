@@ -260,6 +260,20 @@ vp_status vp_transmittance(vp_scene* scene, const float* origins, const float* d
                            int32_t precision, int32_t engine, float* out_transmittance,
                            int32_t memory);
 
+/* The same transmittance query as vp_transmittance, for callers that cannot allocate device
+ * memory (a plug-in whose host application owns the device-memory budget, or a loop where a
+ * cudaMalloc / cudaFree would synchronise the device).  It calls no allocator: its scratch -- the
+ * staged host rays and results, the work-queue head and the status word -- is one file-scope
+ * static __device__ array sized for at most 65536 rays (about 1.8 MB), which every GPU that loads
+ * the library holds until the process exits.  n > 65536 returns VP_ERROR_LIMIT.  The first call
+ * on a device looks up the array's address on that device; make it before any stream capture.
+ * All calls share the array and leave their data in it (the queue head and status word are
+ * cleared at the start of each call): calls whose work overlaps on the GPU race and must be
+ * serialised by the caller.  No counterpart in the reference. */
+vp_status vp_transmittance_static(vp_scene* scene, const float* origins, const float* dirs,
+                                  uint32_t n, int32_t precision, float* out_transmittance,
+                                  int32_t memory);
+
 /* Camera rays of n (pixel x, pixel y, sample index) triples for a params->spp-sample render:
  * the per-(pixel, sample) PCG32 stream seeded as the reference's raygen
  * (device/entry/raygen.cuh:82-99, device/core/random.cuh:33-72) and the jittered ray of
