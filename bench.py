@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-baseline-engine", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the differentiation and serving forms")
+    ap.add_argument("--serving-requests", type=int, default=64)
     return ap.parse_args()
 
 
@@ -184,6 +186,73 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# Algorithmic bytes of one traversal query's work: a Gaussian's 3-sigma box (2 float4) per box
+# test, its whitening record (4 float4) per box hit, a BVH32 inner node (32 child boxes, 64 float4)
+# per visit; binary LBVH nodes are 4 float4.
+BOX_BYTES, RECORD_BYTES, WIDE_NODE_BYTES, BINARY_NODE_BYTES = 32, 64, 1024, 64
+# Per-item path state the wavefront kernels move: extend reads the queue entry, origin, direction,
+# key, bounce word and writes albedo + t* (4+16+16+8+4+16); shadow reads the queue entry, origin,
+# direction and writes the transmittance (4+16+16+4).
+EXTEND_STATE_BYTES, SHADOW_STATE_BYTES = 64, 40
+
+
+def roofline(args, m, step_stats):
+    """Roofline of the dominant kernel, from the counters of one measured batch (m) and the CUDA-event
+    stage times of the timed steps (the steps are the same batch size over the same image)."""
+    peak, peak_kind = measured_peaks()
+
+    def query_bytes(k):
+        node = BINARY_NODE_BYTES if args.engine == "megakernel" else WIDE_NODE_BYTES
+        return m["query_prim_tests"][k] * BOX_BYTES + m["query_geo_loads"][k] * RECORD_BYTES + m["query_nodes"][k] * node
+
+    n = len(step_stats)
+    if args.engine == "wavefront":
+        ms = [sum(st["ms_stage"][k] for st in step_stats) / n for k in range(3)]
+        nl = [sum(st["stage_launches"][k] for st in step_stats) / n for k in range(3)]
+        kern = [("k_wf_extend", query_bytes(0) + query_bytes(2) + m["bounces"] * EXTEND_STATE_BYTES,
+                 "free-flight argmin + scatter-point albedo", m["bounces"], "path bounces"),
+                ("k_wf_shadow", query_bytes(1) + m["shadow_rays"] * SHADOW_STATE_BYTES,
+                 "transmittance (NEE shadow rays)", m["shadow_rays"], "shadow rays")]
+        k = 0 if ms[0] >= ms[1] else 1
+        name, alg, what, units, unit_name = kern[k]
+        step_ms, launches = ms[k], nl[k]
+        share = ms[k] / max(1e-9, sum(st["ms_kernels"] for st in step_stats) / n)
+    else:
+        name = "k_render_mega" if args.engine == "megakernel" else "k_render_warp"
+        alg = query_bytes(0) + query_bytes(1) + query_bytes(2)
+        what, units, unit_name = "whole path loop", m["paths"], "paths"
+        step_ms = sum(st["ms_kernels"] for st in step_stats) / n
+        launches, share = 1, 1.0
+    achieved = alg / (step_ms / 1e3) / 1e9  # per-launch bytes / per-launch time = per-step ratio
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": peak_kind, "kernel": name, "kernel_work": what,
+            "kernel_share_of_step": share, "launches_per_step": launches,
+            "algorithmic_bytes_per_launch": alg / launches, "kernel_ms_per_launch": step_ms / launches,
+            "units_per_launch": units / launches, "units": unit_name,
+            "note": "achieved = algorithmic bytes of the kernel's launches in one step (3-sigma boxes tested x 32 B + "
+                    "Gaussian records loaded x 64 B + BVH32 inner nodes x 1 KiB + per-item path state) / their "
+                    "CUDA-event time in the timed steps; the 70 MB scene is L2-resident, so most of these bytes "
+                    "are L2 hits (traffic = DRAM bytes from ncu)",
+            "per_step": {"crossings": m["crossings"], "bounces": m["bounces"], "shadow_rays": m["shadow_rays"],
+                         "query_nodes[argmin,tau,albedo]": m["query_nodes"],
+                         "query_leaves[argmin,tau,albedo]": m["query_leaves"],
+                         "query_box_tests[argmin,tau,albedo]": m["query_prim_tests"],
+                         "query_record_loads[argmin,tau,albedo]": m["query_geo_loads"],
+                         "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"]}}
+    if args.engine == "wavefront":
+        roof["stage_ms_per_step[extend,shadow,other]"] = ms
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        try:
+            tr = json.loads(traffic_file.read_text()).get(name)
+            if tr:  # DRAM bytes per unit from an ncu capture, scaled to this launch's units
+                roof["traffic"] = tr["dram_bytes_per_unit"] * units / launches
+                roof["traffic_source"] = tr["source"]
+        except (ValueError, KeyError, TypeError):
+            pass
+    return roof
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -216,9 +285,11 @@ def run_ours(args):
     from volprim_b200 import distributed as D
     base, _ = D.sample_range(rank, world, args.spp)
 
+    tcfg = vp.Config(**{**cfg.__dict__, "time_stages": True})  # CUDA events around the traversal kernels
+
     def step(i):  # one launch batch of BATCH_SPP samples
         off = base + (i * BATCH_SPP) % args.spp
-        return img.accumulate(scene, env, w.camera, cfg, off, BATCH_SPP)
+        return img.accumulate(scene, env, w.camera, tcfg, off, BATCH_SPP)
 
     # warm-up (also the first steps of the image)
     for i in range(args.warmup):
@@ -238,11 +309,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks.start()
     t_wall = time.perf_counter()
+    step_stats = []
     for i in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(float(i))  # L2 flush, outside the step's events
             starts[i].record(stream)
-        step(i)
+        step_stats.append(step(i))
         with torch.cuda.stream(stream):
             ends[i].record(stream)
     reduce_ms = 0.0
@@ -269,32 +341,8 @@ def run_ours(args):
     value = paths_per_rank * world / (total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
 
-    # roofline of the dominant kernel (k_render_warp): algorithmic bytes per launch (one batch) =
-    # Gaussian boxes tested x 32 B + Gaussian records loaded x 64 B + inner-node visits x node
-    # bytes (BVH32: 32 child boxes = 1 KiB; binary LBVH: 64 B)
-    node_bytes = 64 if args.engine == "megakernel" else 1024
-    alg_bytes = mstats["prim_tests"] * 32 + mstats["geo_loads"] * 64 + mstats["nodes_visited"] * node_bytes
-    launch_ms = statistics.mean(step_ms)
-    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": peak_kind,
-            "note": "achieved = (Gaussian boxes tested x 32 B + records loaded x 64 B + BVH32 inner nodes x 1 KiB) per launch / mean "
-                    "launch time; the scene is L2-resident, so most of these bytes are L2 hits",
-            "per_launch": {"prim_tests": mstats["prim_tests"], "geo_loads": mstats["geo_loads"], "crossings": mstats["crossings"],
-                           "inner_nodes": mstats["nodes_visited"], "leaves": mstats["leaves_visited"],
-                           "bounces": mstats["bounces"], "shadow_rays": mstats["shadow_rays"],
-                           "max_point_overlap": mstats["max_point_overlap"], "max_hits_per_ray": mstats["max_hits_per_ray"],
-                           "query_nodes[argmin,tau,albedo]": mstats["query_nodes"],
-                           "query_leaves[argmin,tau,albedo]": mstats["query_leaves"]}}
-    traffic_file = ROOT / "profiles" / "traffic.json"
-    if traffic_file.exists():
-        try:
-            tr = json.loads(traffic_file.read_text()).get(args.engine)
-            if tr:
-                roof["traffic"] = tr["bytes_per_launch"]
-        except Exception:
-            pass
+    roof = roofline(args, mstats, step_stats)
+    launches = sum(st["launches"] for st in step_stats)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -304,7 +352,7 @@ def run_ours(args):
                        "max_depth": cfg.max_bounces, "rr_depth": cfg.rr_depth, "env": "procedural 2048x1024",
                        "engine": args.engine, "precision": "fast (FP32)",
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"samples x{world}"},
-            "clocks": clk, "gpu_launches": args.steps, "roofline": roof,
+            "clocks": clk, "gpu_launches": launches, "roofline": roof,
             "scene": scene.info(), "env_build_ms": env.build_ms, "wall_s": wall}
     if rank == 0 and not args.no_baseline_engine and args.engine != "megakernel" and world == 1:
         # the plain per-pixel megakernel of the same method on the same batches (for the ratio)
@@ -321,6 +369,9 @@ def run_ours(args):
                                        "ms_per_step": statistics.mean(ms)}
     if not args.no_e2e and world == 1:
         line["e2e"] = e2e_run(args, w, local)
+    if rank == 0 and not args.no_forms and world == 1:
+        line["differentiation"] = differentiation_form(local)
+        line["serving"] = serving_form(local, args.serving_requests)
     if rank == 0 and not args.no_cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
@@ -362,6 +413,124 @@ def e2e_run(args, w, device):
     return {"value": paths / min(times) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(out.nbytes), "seconds": min(times),
             "note": "one step here = the whole job (upload, BVH + env builds, 256 spp, read-back)"}
+
+
+def differentiation_form(device):
+    """grad/s of the differentiation workload (100k Gaussians, absorption + emission, 4 cameras at
+    256x256 x 8 spp, L2 loss against a render of perturbed parameters): one gradient = the
+    autograd Function's scene build + 4 forward renders + 4 adjoint renders, timed on the host
+    around torch.cuda.synchronize (the library calls are synchronous)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import volprim_b200 as vp
+    from volprim_b200 import _capi, scenes
+    from volprim_b200.autograd import render_emission_images
+    from volprim_b200.emission import render_emission, render_emission_backward
+
+    w = scenes.emission_100k()
+    ctx = vp.Context(device)
+    env = vp.Environment(ctx, constant=w.env_constant)
+    dev = torch.device("cuda", device)
+    tg, te = scenes.perturbed(w)
+    ts = vp.Scene(ctx, tg, w.sigma_multiplier)
+    ts.set_emission(te)
+    target = torch.stack([torch.from_numpy(render_emission(ts, env, c, w.config)[..., :3]) for c in w.cameras]).to(dev)
+    ts.close()
+    g = w.gaussians
+    t = [torch.tensor(np.asarray(a, np.float32), device=dev, requires_grad=True)
+         for a in (g.mean, g.scale, g.quat_wxyz, g.density, w.emission)]
+
+    def one():
+        for x in t:
+            x.grad = None
+        imgs = render_emission_images(*t, w.cameras, w.config, env, w.sigma_multiplier, ctx)
+        loss = ((imgs - target) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        return float(loss)
+
+    one()
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+    # kernel split on the built scene
+    sc = vp.Scene(ctx, g, w.sigma_multiplier)
+    sc.set_emission(w.emission)
+    n = g.count
+    grads = {k: np.zeros(m * n, np.float32) for k, m in (("mean", 3), ("scale", 3), ("quat_wxyz", 4), ("density", 1),
+                                                          ("emission", 3))}
+    img = torch.empty((w.config.image_height, w.config.image_width, 4), device=dev)
+    fwd_ms = bwd_ms = 0.0
+    for cam in w.cameras:
+        st = _capi.vp_render_stats()
+        p, cc = w.config.to_c(), cam.to_c()
+        _capi.check(_capi.lib.vp_render_emission(sc.handle, env.handle, C.byref(cc), C.byref(p), img.data_ptr(),
+                                                 _capi.VP_MEMORY_DEVICE, C.byref(st)))
+        fwd_ms += st.ms_kernels
+        dl = np.full((w.config.image_height, w.config.image_width, 4), 1e-3, np.float32)
+        bwd_ms += render_emission_backward(sc, env, cam, w.config, dl, grads)["ms_kernels"]
+    info = sc.info()
+    sc.close()
+    env.close()
+    ctx.close()
+    paths = len(w.cameras) * w.config.image_width * w.config.image_height * w.config.num_samples_per_pixel
+    return {"metric": "grad/s", "value": 1.0 / statistics.mean(times), "unit": "grad/s",
+            "ms_per_grad": 1e3 * statistics.mean(times), "workload": "emission_100k (100k Gaussians, 4 cameras, "
+            "256x256, 8 spp, FAST)", "paths_per_forward": paths, "forward_kernel_ms": fwd_ms,
+            "backward_kernel_ms": bwd_ms, "scene_build_ms": info["build_ms"],
+            "note": "one gradient = scene build from the parameter tensors + 4 forward + 4 adjoint renders "
+                    "(autograd Function), host-timed around torch.cuda.synchronize; kernel split from CUDA events"}
+
+
+def serving_form(device, n_requests):
+    """The serving workload on its 4 resident scenes (50k / 100k / 250k / 500k Gaussians, seeds 1-4):
+    the first n_requests of the seeded request stream, (1) all at t = 0 (offline throughput),
+    (2) with Poisson arrivals at 80% of that throughput (p50 / p99 latency, served Mpaths/s) and
+    (3) the same arrivals through one vp_render per request (the plain per-request launch)."""
+    import volprim_b200 as vp
+    from volprim_b200 import scenes
+    from volprim_b200.serving import Server, make_trace, run_trace, run_trace_plain
+
+    ctx = vp.Context(device)
+    gs, sigma, env_img = scenes.serving_scenes()
+    scs = [vp.Scene(ctx, g, sigma) for g in gs]
+    env = vp.Environment(ctx, rgb=env_img)
+    envs = [env] * len(scs)
+
+    def server():
+        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9)
+        for sc in scs:
+            s.add_scene(sc, env)
+        return s
+
+    burst = make_trace(2024, n_requests, rate=0.0, n_scenes=len(scs))
+    srv = server()
+    off = run_trace(srv, burst)
+    srv.close()
+    mean_paths = off["paths"] / n_requests
+    rate = 0.8 * off["mpaths_per_s"] * 1e6 / mean_paths
+    trace = make_trace(2024, n_requests, rate=rate, n_scenes=len(scs))
+    srv = server()
+    served = run_trace(srv, trace)
+    srv.close()
+    plain = run_trace_plain(scs, envs, trace)
+    for s in scs:
+        s.close()
+    env.close()
+    ctx.close()
+    return {"metric": "p50/p99 request latency", "unit": "s", "p50_s": served["p50_s"], "p99_s": served["p99_s"],
+            "mpaths_per_s": served["mpaths_per_s"], "offline_mpaths_per_s": off["mpaths_per_s"],
+            "fraction_of_offline": served["mpaths_per_s"] / off["mpaths_per_s"],
+            "arrival_rate_per_s": rate, "requests": n_requests, "paths": served["paths"],
+            "plain_per_request": {"p50_s": plain["p50_s"], "p99_s": plain["p99_s"],
+                                  "mpaths_per_s": plain["mpaths_per_s"]},
+            "workload": "4 resident scenes (50k/100k/250k/500k Gaussians), requests: resolution in "
+                        "{64,128,256,512}^2, spp in {1,4,16,64}, random camera at distance 3.5; Poisson arrivals at "
+                        "80% of the offline throughput; 150 GB budget"}
 
 
 def main():

@@ -198,6 +198,16 @@ __global__ void k_gather(uint32_t n, const uint32_t* __restrict__ order, const f
   pbox[2 * i + 1] = hi_in[s];
 }
 
+__global__ void k_gather_raw(uint32_t n, const uint32_t* __restrict__ order, const float* __restrict__ scale,
+                             const float* __restrict__ quat, const float* __restrict__ density,
+                             float4* __restrict__ raw) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = order[i];
+  raw[2 * i] = make_float4(quat[4 * s], quat[4 * s + 1], quat[4 * s + 2], quat[4 * s + 3]);
+  raw[2 * i + 1] = make_float4(scale[3 * s], scale[3 * s + 1], scale[3 * s + 2], density[s]);
+}
+
 __device__ __forceinline__ int karras_delta(const uint64_t* __restrict__ codes, int n, int i, int j) {
   if (j < 0 || j >= n) return -1;
   const uint64_t a = codes[i], b = codes[j];
@@ -537,6 +547,13 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   sc->pbox = pbox;
   k_gather<<<nb, TB, 0, st>>>(n, perm, rec0.p, lo0.p, hi0.p, prims, plo.p, phi.p, pbox);
   VP_CUDA(cudaGetLastError());
+  float4* raw = nullptr;
+  if ((s = dev_alloc(&raw, 2ull * n, st))) return s;
+  sc->raw = raw;
+  sc->scale_is_log = g->scale_is_log ? 1 : 0;
+  sc->sigma_multiplier = sigma_multiplier;
+  k_gather_raw<<<nb, TB, 0, st>>>(n, perm, scale, quat, dens, raw);
+  VP_CUDA(cudaGetLastError());
 
   // Binary radix tree + refit.
   const uint32_t ni = n > 1 ? n - 1 : 1;
@@ -652,7 +669,8 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     info.bounds_min[k] = o2f(bh[6 + k]);
     info.bounds_max[k] = o2f(bh[9 + k]);
   }
-  info.device_bytes = 64ull * n + 4ull * n + 1024ull * wide_nodes + 64ull * ni;
+  // records, order, per-Gaussian boxes, adjoint inputs, BVH32, binary LBVH
+  info.device_bytes = 64ull * n + 4ull * n + 32ull * n + 32ull * n + 1024ull * wide_nodes + 64ull * ni;
   return VP_OK;
 }
 

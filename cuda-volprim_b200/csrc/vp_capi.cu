@@ -126,7 +126,7 @@ ParamsView make_params(const vp_render_params& p, const vp_scene* s) {
   P.hg_phase_coeff = (1.0f / (4.0f * 3.14159265358979323846f)) * P.hg_one_minus_g2;
   P.accurate = p.precision == VP_PRECISION_ACCURATE ||
                (p.precision == VP_PRECISION_AUTO && s->view.albedo_all_zero);
-  P.measure = p.measure;
+  P.measure = p.measure & VP_MEASURE_COUNTERS;
   return P;
 }
 
@@ -213,6 +213,8 @@ vp_status vp_context_destroy(vp_context* c) {
   if (c->work_counter) cudaFree(c->work_counter);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t ev : c->stage_ev)
+    if (ev) cudaEventDestroy(ev);
   free_wavefront(c);
   if (c->wf.host_count) cudaFreeHost(c->wf.host_count);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -270,6 +272,8 @@ vp_status vp_scene_destroy(vp_scene* s) {
   dev_free(s->wide, st);
   dev_free(s->bin, st);
   dev_free(s->pbox, st);
+  dev_free(s->raw, st);
+  dev_free(s->emis, st);
   if (st) cudaStreamSynchronize(st);
   delete s;
   return VP_OK;
@@ -424,6 +428,10 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
   CameraView cv;
   build_camera(*cam, p->width, p->height, cv);
   const ParamsView P = make_params(*p, s);
+  ctx->launches = 0;
+  ctx->time_stages = (p->measure & VP_MEASURE_STAGES) != 0;
+  ctx->stage_ms[0] = ctx->stage_ms[1] = 0.0;
+  ctx->stage_launches[0] = ctx->stage_launches[1] = 0;
   VP_CUDA(cudaMemsetAsync(ctx->counters, 0, sizeof(Counters), ctx->stream));
   VP_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   const uint32_t batch = p->batch_spp ? p->batch_spp : spp_count;
@@ -451,16 +459,28 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
     stats->shadow_rays = c.shadow_rays;
     stats->nodes_visited = c.nodes;
     stats->leaves_visited = c.leaves;
-    stats->prim_tests = c.prim_tests;
-    stats->geo_loads = c.geo_loads;
     for (int k = 0; k < 3; ++k) {
       stats->query_nodes[k] = c.kind_nodes[k];
       stats->query_leaves[k] = c.kind_leaves[k];
+      stats->query_prim_tests[k] = c.kind_prims[k];
+      stats->query_geo_loads[k] = c.kind_geo[k];
+      stats->prim_tests += c.kind_prims[k];
+      stats->geo_loads += c.kind_geo[k];
     }
     stats->max_hits_per_ray = c.max_hits;
     stats->max_point_overlap = c.max_overlap;
     stats->device_status = c.status;
+    stats->launches = ctx->launches;
+    if (ctx->time_stages) {
+      stats->ms_stage[0] = ctx->stage_ms[0];
+      stats->ms_stage[1] = ctx->stage_ms[1];
+      stats->ms_stage[2] = std::max(0.0, (double)ms - ctx->stage_ms[0] - ctx->stage_ms[1]);
+      stats->stage_launches[0] = ctx->stage_launches[0];
+      stats->stage_launches[1] = ctx->stage_launches[1];
+      stats->stage_launches[2] = ctx->launches - ctx->stage_launches[0] - ctx->stage_launches[1];
+    }
   }
+  ctx->time_stages = false;
   if (c.status) return fail(VP_ERROR_DEVICE_STATUS, "a render kernel raised device status " + std::to_string(c.status));
   return VP_OK;
 }

@@ -99,8 +99,10 @@ struct ParamsView {
 };
 
 struct Counters {  // device-side statistics (only touched when ParamsView::measure)
-  unsigned long long bounces, scatters, crossings, shadow_rays, nodes, leaves, prim_tests, geo_loads;
-  unsigned long long kind_nodes[3], kind_leaves[3];  // per query kind: argmin, transmittance, albedo
+  unsigned long long bounces, scatters, crossings, shadow_rays, nodes, leaves;
+  // per query kind (argmin, transmittance, albedo): inner nodes, leaves, Gaussian boxes tested,
+  // Gaussian records loaded
+  unsigned long long kind_nodes[3], kind_leaves[3], kind_prims[3], kind_geo[3];
   unsigned int max_hits, max_overlap, status;
 };
 

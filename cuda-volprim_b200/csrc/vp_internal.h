@@ -72,6 +72,13 @@ struct vp_context {
   vp::Counters* counters = nullptr;   // device, one block of statistics per render call
   unsigned int* work_counter = nullptr;  // device, persistent-kernel work queue head
   vp::WfWorkspace wf;                 // wavefront engine buffers (grow-only)
+  // launch accounting of the current render call (reset by vp_render_accumulate)
+  uint32_t launches = 0;              // kernels launched
+  bool time_stages = false;           // VP_MEASURE_STAGES
+  double stage_ms[2] = {0.0, 0.0};    // wavefront extend, shadow
+  uint32_t stage_launches[2] = {0, 0};
+  static constexpr int kStageEvents = 16;  // 4 wavefront iterations x 4 events
+  cudaEvent_t stage_ev[kStageEvents] = {};
 };
 
 struct vp_scene {
@@ -82,6 +89,12 @@ struct vp_scene {
   float4* wide = nullptr;
   float4* bin = nullptr;
   float4* pbox = nullptr;
+  // as given by the caller, in the scene's order: quaternion (w,x,y,z), then scale (log or
+  // linear, as scale_is_log says) and density -- the chain-rule inputs of the adjoint
+  float4* raw = nullptr;
+  float4* emis = nullptr;  // RGB emission per unit optical depth (vp_scene_set_emission)
+  int32_t scale_is_log = 0;
+  float sigma_multiplier = 1.0f;
   vp_scene_info info{};
 };
 
@@ -109,6 +122,7 @@ vp_status build_env(vp_context* ctx, const float* rgb, uint32_t w, uint32_t h, u
 // Host restatement of host::params::Camera::build (camera.h:106-177).
 void build_camera(const vp_camera& cam, uint32_t width, uint32_t height, CameraView& out);
 ParamsView make_params(const vp_render_params& p, const vp_scene* s);
+vp_status check_params(const vp_render_params* p);
 vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const ParamsView& P,
                         int32_t engine, vp_image* img, uint32_t spp_offset, uint32_t spp_count);
 vp_status launch_transmittance(vp_scene* s, const float* o, const float* d, uint32_t n,

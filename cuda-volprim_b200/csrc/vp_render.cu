@@ -102,11 +102,11 @@ __device__ __forceinline__ void flush_stats(Counters* c, const PathStats& ps, co
   atomicAdd(&c->crossings, ws.crossings);
   atomicAdd(&c->nodes, ws.nodes);
   atomicAdd(&c->leaves, ws.leaves);
-  atomicAdd(&c->prim_tests, ws.prim_tests);
-  atomicAdd(&c->geo_loads, ws.geo_loads);
   for (int k = 0; k < 3; ++k) {
     atomicAdd(&c->kind_nodes[k], ws.kind_nodes[k]);
     atomicAdd(&c->kind_leaves[k], ws.kind_leaves[k]);
+    atomicAdd(&c->kind_prims[k], ws.kind_prims[k]);
+    atomicAdd(&c->kind_geo[k], ws.kind_geo[k]);
   }
   atomicMax(&c->max_hits, ws.max_hits);
   atomicMax(&c->max_overlap, ps.max_overlap);
@@ -319,6 +319,7 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
   } else {
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown engine");
   }
+  ctx->launches += 1;
   VP_CUDA(cudaGetLastError());
   return VP_OK;
 }

@@ -1,0 +1,780 @@
+// Serving runtime: continuous batching of render requests over resident scenes (the serving form;
+// the reference renders one configured image per process and has no counterpart).
+//
+// A pool of path slots runs the wavefront stages of the offline engine (vp_wavefront.cu) with
+// path regeneration: every iteration
+//   advance  (1 thread)          carry the survivors over; take min(free slots, unstarted paths)
+//                                new paths from the admitted range
+//   regen    (thread per path)   new paths: request lookup in the admission ring, camera ray,
+//                                PCG32 stream, first free-flight key -- appended to the queue
+//   extend   (warp per path)     free-flight argmin + scatter albedo on the path's own scene
+//   shade    (thread per path)   phase / NEE / roulette with the request's own controls
+//   shadow   (warp per query)    transmittance on the query's scene
+//   gather   (thread per path)   radiance += weight x T; a finished path adds its sample to its
+//                                request's pixel sum, counts itself done and frees its slot
+// so paths of different requests, scenes, resolutions and sample counts share every launch, and
+// a request admitted while others run starts as soon as slots free up.  The virtual path space is
+// the concatenation of the admitted requests' width*height*spp paths in admission order (pixel
+// major); a request's paths start in order.  Every per-path quantity comes from the request-table
+// entry the path carries, so a path computes exactly what the offline engine computes for the
+// same (scene, camera, params, pixel, sample).
+//
+// The host side admits from a FIFO when a table entry is free and the request's accumulator fits
+// the memory budget, replays the iterations as one captured CUDA graph (two iterations: the path
+// queues ping-pong), reads the per-request done counters, and completes requests whose paths have
+// all finished (mean = sum / spp into the caller's buffer).  Admission writes happen only while
+// the stream is idle (after the step's synchronisation), so the graph never sees a half-written
+// table entry.
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <vector>
+
+#include "vp_internal.h"
+#include "vp_path.cuh"
+#include "vp_traverse.cuh"
+
+namespace vp {
+namespace {
+
+constexpr uint32_t kAlive = 1u << 18;
+constexpr int kSrvHitCap = 64;        // extend hit buffer, as the offline wavefront's
+constexpr uint32_t kMaxScenes = 64;
+// Admission-ring entries per request-table entry.  The device's lookup window can trail the host
+// by the requests admitted since the last iteration plus those still unstarted, at most two table
+// capacities; the ring is larger, so the host never overwrites an entry the window still holds.
+constexpr uint32_t kRingPerEntry = 4;
+
+struct SrvRequest {  // device request-table entry
+  CameraView cam;
+  ParamsView P;
+  uint32_t scene;    // resident (scene, env) pair
+  uint32_t n_pix;
+  unsigned long long base, n_paths;  // virtual path range
+  float4* sum;       // per-pixel radiance sums
+};
+
+struct SrvCtl {  // device control block of the iteration
+  unsigned long long cursor;     // next virtual path to start
+  unsigned long long admit_end;  // end of the admitted virtual range (host-written)
+  unsigned long long regen_v0;   // first virtual path started by the current iteration
+  uint32_t free_count;           // free path slots (top of the free stack)
+  uint32_t regen_m;              // paths started by the current iteration
+  uint32_t regen_from;           // free-stack index of the first slot they take
+  uint32_t survivors;            // paths carried over from the previous iteration
+  uint32_t ring_lo;              // first admitted request whose paths are not all started
+  uint32_t ring_hi;              // admitted requests (host-written)
+  uint32_t ctr[8];               // [0] paths this iteration, [1] next, [2] shadow queries, [3..4] work heads
+};
+
+struct SrvPaths {  // per path slot
+  float4 *o4, *d4, *thr4, *rad4, *alb4;
+  uint4* rng4;
+  uint2* key2;
+  uint32_t* meta;  // bounce | shadow count << 16 | alive << 18
+  uint32_t *req, *pix;
+  float4 *so4, *sd4, *sw4;  // 3 transmittance queries per slot
+  uint32_t *qa, *qb, *qs, *free_stack;
+};
+
+__device__ __forceinline__ void srv_store(const SrvPaths& b, uint32_t p, const PathState& s) {
+  b.o4[p] = make_float4(s.o.x, s.o.y, s.o.z, 0.f);
+  b.d4[p] = make_float4(s.d.x, s.d.y, s.d.z, 0.f);
+  b.thr4[p] = make_float4(s.thr.x, s.thr.y, s.thr.z, 0.f);
+  b.rad4[p] = make_float4(s.rad.x, s.rad.y, s.rad.z, 0.f);
+  b.rng4[p] = make_uint4((uint32_t)s.rng.state, (uint32_t)(s.rng.state >> 32), (uint32_t)s.rng.inc,
+                         (uint32_t)(s.rng.inc >> 32));
+}
+
+__device__ __forceinline__ PathState srv_load(const SrvPaths& b, uint32_t p, uint32_t bounce) {
+  PathState s;
+  const float4 o = b.o4[p], d = b.d4[p], t = b.thr4[p], r = b.rad4[p];
+  const uint4 g = b.rng4[p];
+  s.o = f3(o.x, o.y, o.z);
+  s.d = f3(d.x, d.y, d.z);
+  s.thr = f3(t.x, t.y, t.z);
+  s.rad = f3(r.x, r.y, r.z);
+  s.rng.state = ((uint64_t)g.y << 32) | g.x;
+  s.rng.inc = ((uint64_t)g.w << 32) | g.z;
+  s.bounce = bounce;
+  return s;
+}
+
+// Warp-aggregated queue append (all 32 lanes call it): this lane's first slot for n entries.
+__device__ __forceinline__ uint32_t srv_reserve(uint32_t* counter, uint32_t n) {
+  const int lane = threadIdx.x & 31;
+  uint32_t incl = n;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  uint32_t base = 0;
+  if (lane == 31 && total) base = atomicAdd(counter, total);
+  base = __shfl_sync(kFull, base, 31);
+  return base + incl - n;
+}
+
+__global__ void k_srv_init(SrvCtl* c, uint32_t* free_stack, uint32_t slots) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(c);
+    for (uint32_t k = 0; k < sizeof(SrvCtl) / 4u; ++k) w[k] = 0u;
+    c->free_count = slots;
+  }
+  if (i < slots) free_stack[i] = slots - 1u - i;  // pops take the lowest slots first
+}
+
+__global__ void k_srv_advance(SrvCtl* c, const unsigned long long* __restrict__ ring_base,
+                              const unsigned long long* __restrict__ ring_n, uint32_t ring_cap) {
+  const uint32_t surv = c->ctr[1];
+  const unsigned long long avail = c->admit_end - c->cursor;
+  const uint32_t m = (uint32_t)min((unsigned long long)c->free_count, avail);
+  c->survivors = surv;
+  c->regen_m = m;
+  c->regen_from = c->free_count - m;
+  c->regen_v0 = c->cursor;
+  c->free_count -= m;
+  c->cursor += m;
+  c->ctr[0] = surv + m;
+  c->ctr[1] = c->ctr[2] = c->ctr[3] = c->ctr[4] = 0u;
+  // admitted requests whose paths all started before this iteration leave the lookup window
+  uint32_t lo = c->ring_lo;
+  const uint32_t hi = c->ring_hi;
+  while (lo + 1u < hi && ring_base[lo % ring_cap] + ring_n[lo % ring_cap] <= c->regen_v0) ++lo;
+  c->ring_lo = lo;
+}
+
+__global__ void k_srv_regen(const SrvCtl* __restrict__ c, const SrvRequest* __restrict__ table,
+                            const unsigned long long* __restrict__ ring_base, const uint32_t* __restrict__ ring_slot,
+                            uint32_t ring_cap, SrvPaths b, uint32_t* __restrict__ q) {
+  const uint32_t m = c->regen_m;
+  const uint32_t from = c->regen_from, surv = c->survivors;
+  const unsigned long long v0 = c->regen_v0;
+  const uint32_t lo0 = c->ring_lo, hi0 = c->ring_hi;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const uint32_t slot = b.free_stack[from + i];
+    const unsigned long long v = v0 + i;
+    uint32_t lo = lo0, hi = hi0;  // last admitted request with base <= v
+    while (hi - lo > 1u) {
+      const uint32_t mid = lo + (hi - lo) / 2u;
+      if (ring_base[mid % ring_cap] <= v) lo = mid;
+      else hi = mid;
+    }
+    const uint32_t e = ring_slot[lo % ring_cap];
+    const SrvRequest& r = table[e];
+    const unsigned long long local = v - r.base;
+    const uint32_t spp = r.P.spp_total;
+    const uint32_t pix = (uint32_t)(local / spp), s = (uint32_t)(local % spp);
+    PathState st = start_path(r.cam, r.P, pix % r.P.width, pix / r.P.width, s);
+    const uint64_t key = draw_bounce_key(st.rng);
+    srv_store(b, slot, st);
+    b.key2[slot] = make_uint2((uint32_t)key, (uint32_t)(key >> 32));
+    b.meta[slot] = kAlive;
+    b.req[slot] = e;
+    b.pix[slot] = pix;
+    q[surv + i] = slot;
+  }
+}
+
+template <bool kAcc>
+__global__ void __launch_bounds__(256, 4) k_srv_extend(const SceneView* __restrict__ scenes,
+                                                       const SrvRequest* __restrict__ table, SrvPaths b,
+                                                       const uint32_t* __restrict__ q, SrvCtl* c, uint32_t max_cap,
+                                                       Counters* ctr) {
+  extern __shared__ unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(max_cap, kSrvHitCap), max_cap, kSrvHitCap);
+  const uint32_t n = c->ctr[0];
+  uint32_t status = 0;
+  WarpStats ws;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&c->ctr[3], 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= n) break;
+    const uint32_t p = __ldg(q + item);
+    const SceneView S = scenes[table[b.req[p]].scene];
+    const float4 o = b.o4[p], d = b.d4[p];
+    const uint2 k2 = b.key2[p];
+    const uint32_t bounce = b.meta[p] & 0xFFFFu;
+    const float3 of = f3(o.x, o.y, o.z), df = f3(d.x, d.y, d.z);
+    float tstar = kInf;
+    ScatterAlbedo sa;
+    sa.valid = false;
+    if (!(bounce == 0 && S.albedo_all_zero))
+      tstar = warp_ray_query<kAcc, kArgmin>(S, W, of, df, ((uint64_t)k2.y << 32) | k2.x, status, ws, false, &sa);
+    float3 albedo = f3(0.f, 0.f, 0.f);
+    if (tstar < kInf) {
+      uint32_t ov = sa.overlap;
+      albedo = sa.valid ? sa.albedo : warp_albedo<kAcc>(S, W, fma3(tstar, df, of), ov, status, ws, false);
+    }
+    if (lane == 0) b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+    if (status) break;
+  }
+  if (lane == 0 && status) atomicOr(&ctr->status, status);
+}
+
+__global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ envs,
+                                                   const SrvRequest* __restrict__ table, SrvPaths b,
+                                                   const uint32_t* __restrict__ q, SrvCtl* c,
+                                                   uint32_t* __restrict__ qnext) {
+  const uint32_t n = c->ctr[0];
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x / 32);
+  const uint32_t wid = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  for (uint32_t base = wid * 32u; base < n; base += warps * 32u) {  // warp-uniform
+    const uint32_t i = base + lane;
+    uint32_t p = 0;
+    int ns = 0;
+    bool alive = false;
+    if (i < n) {
+      p = q[i];
+      const SrvRequest& r = table[b.req[p]];
+      PathState s = srv_load(b, p, b.meta[p] & 0xFFFFu);
+      const float4 a = b.alb4[p];
+      ShadowSet sh;
+      alive = shade_bounce(envs[r.scene], r.P, s, a.w < kInf, a.w, f3(a.x, a.y, a.z), sh);
+      ns = sh.n;
+      for (int k = 0; k < sh.n; ++k) {
+        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, 1.f);
+        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, 0.f);
+        b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
+      }
+      if (alive) {
+        const uint64_t key = draw_bounce_key(s.rng);
+        b.key2[p] = make_uint2((uint32_t)key, (uint32_t)(key >> 32));
+      }
+      srv_store(b, p, s);
+      b.meta[p] = (s.bounce & 0xFFFFu) | ((uint32_t)sh.n << 16) | (alive ? kAlive : 0u);
+    }
+    const uint32_t slot = srv_reserve(&c->ctr[2], (uint32_t)ns);
+    for (int k = 0; k < ns; ++k) b.qs[slot + k] = 3u * p + k;
+    const uint32_t qslot = srv_reserve(&c->ctr[1], alive ? 1u : 0u);
+    if (alive) qnext[qslot] = p;
+  }
+}
+
+template <bool kAcc>
+__global__ void __launch_bounds__(256, 4) k_srv_shadow(const SceneView* __restrict__ scenes,
+                                                       const SrvRequest* __restrict__ table, SrvPaths b, SrvCtl* c,
+                                                       uint32_t max_cap, Counters* ctr) {
+  extern __shared__ unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(max_cap, 32), max_cap, 32);
+  const uint32_t n = c->ctr[2];
+  uint32_t status = 0;
+  WarpStats ws;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&c->ctr[4], 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= n) break;
+    const uint32_t qslot = __ldg(b.qs + item);
+    const SceneView S = scenes[table[b.req[qslot / 3u]].scene];
+    const float4 o = b.so4[qslot], d = b.sd4[qslot];
+    const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws, false);
+    if (lane == 0) b.so4[qslot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
+    if (status) break;
+  }
+  if (lane == 0 && status) atomicOr(&ctr->status, status);
+}
+
+__global__ void __launch_bounds__(256) k_srv_gather(const SrvRequest* __restrict__ table, SrvPaths b,
+                                                    const uint32_t* __restrict__ q, SrvCtl* c,
+                                                    unsigned long long* __restrict__ done) {
+  const uint32_t n = c->ctr[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = q[i];
+    const uint32_t m = b.meta[p];
+    const int ns = (int)((m >> 16) & 3u);
+    const float4 r4 = b.rad4[p];
+    float3 rad = f3(r4.x, r4.y, r4.z);
+    for (int k = 0; k < ns; ++k) {
+      const float4 w = b.sw4[3u * p + k];
+      rad = add(rad, mul(f3(w.x, w.y, w.z), b.so4[3u * p + k].w));
+    }
+    if (m & kAlive) {
+      b.rad4[p] = make_float4(rad.x, rad.y, rad.z, 0.f);
+    } else {
+      const uint32_t e = b.req[p];
+      const SrvRequest& r = table[e];
+      const float3 L = finalize_sample(r.P, rad);
+      atomicAdd(r.sum + b.pix[p], make_float4(L.x, L.y, L.z, 0.f));
+      atomicAdd(done + e, 1ull);
+      b.free_stack[atomicAdd(&c->free_count, 1u)] = p;
+    }
+  }
+}
+
+__global__ void k_srv_finish(const float4* __restrict__ sum, uint32_t n_pix, float inv_spp, float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pix) return;
+  const float4 s = sum[i];
+  out[i] = make_float4(s.x * inv_spp, s.y * inv_spp, s.z * inv_spp, 1.0f);
+}
+
+template <class K>
+int srv_blocks(K kernel, int threads, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess) b = 1;
+  return b < 1 ? 1 : b;
+}
+
+template <class T>
+void srv_carve(char*& cur, T*& out, size_t count) {
+  out = reinterpret_cast<T*>(cur);
+  cur += (count * sizeof(T) + 255) & ~size_t(255);
+}
+
+constexpr size_t kSlotBytes = 5 * 16 + 16 + 8 + 4 + 4 + 4 + 3 * 48 + 4 * 2 + 3 * 4 + 4;
+
+}  // namespace
+}  // namespace vp
+
+using namespace vp;
+
+struct vp_server {
+  vp_context* ctx = nullptr;
+  vp_server_config cfg{};
+  bool accurate = false;
+  std::vector<vp_scene*> scenes;
+  std::vector<vp_env*> envs;
+  uint32_t max_cap = 0;
+  uint32_t ring_cap = 0;
+  // device
+  SceneView* d_scenes = nullptr;
+  EnvView* d_envs = nullptr;
+  SrvRequest* d_table = nullptr;
+  unsigned long long* d_done = nullptr;
+  unsigned long long *d_ring_base = nullptr, *d_ring_n = nullptr;
+  uint32_t* d_ring_slot = nullptr;
+  SrvCtl* d_ctl = nullptr;
+  void* path_mem = nullptr;
+  SrvPaths paths{};
+  // pinned staging (written only while the stream is idle)
+  SrvRequest* h_table = nullptr;
+  unsigned long long* h_done = nullptr;
+  unsigned long long *h_ring_base = nullptr, *h_ring_n = nullptr;
+  uint32_t* h_ring_slot = nullptr;
+  unsigned long long* h_admit_end = nullptr;
+  uint32_t* h_ring_hi = nullptr;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int ext_blocks = 0, shd_blocks = 0, thr_blocks = 0;
+  size_t smem_ext = 0, smem_shd = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // host bookkeeping
+  struct Active {
+    bool used = false;
+    uint64_t id = 0;
+    unsigned long long n_paths = 0;
+    uint32_t n_pix = 0, spp = 0;
+    float* out = nullptr;
+    int32_t memory = 0;
+    float4* sum = nullptr;
+    size_t bytes = 0;
+  };
+  std::vector<Active> active;
+  struct Pending {
+    uint64_t id;
+    vp_request r;
+  };
+  std::deque<Pending> pending;
+  std::vector<uint64_t> done_ids;
+  uint64_t next_id = 0, admitted = 0, completed = 0, paths_completed = 0, iterations = 0;
+  unsigned long long admit_end = 0;
+  uint32_t ring_hi = 0, n_active = 0;
+  size_t bytes_fixed = 0, bytes_active = 0;
+  double device_ms = 0.0;
+};
+
+namespace {
+
+size_t request_bytes(const vp_request& r) {
+  size_t b = (size_t)r.params.width * r.params.height * 16u;
+  if (r.memory == VP_MEMORY_HOST) b += (size_t)r.params.width * r.params.height * 16u;  // output staging
+  return b;
+}
+
+void srv_free(vp_server* s) {
+  if (!s) return;
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t st = s->ctx->stream;
+  if (st) cudaStreamSynchronize(st);
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  for (auto& a : s->active)
+    if (a.sum) cudaFree(a.sum);
+  cudaFree(s->d_scenes);
+  cudaFree(s->d_envs);
+  cudaFree(s->d_table);
+  cudaFree(s->d_done);
+  cudaFree(s->d_ring_base);
+  cudaFree(s->d_ring_n);
+  cudaFree(s->d_ring_slot);
+  cudaFree(s->d_ctl);
+  cudaFree(s->path_mem);
+  cudaFreeHost(s->h_table);
+  cudaFreeHost(s->h_done);
+  cudaFreeHost(s->h_ring_base);
+  cudaFreeHost(s->h_ring_n);
+  cudaFreeHost(s->h_ring_slot);
+  cudaFreeHost(s->h_admit_end);
+  cudaFreeHost(s->h_ring_hi);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  delete s;
+}
+
+// One wavefront iteration with the queues in the given roles.
+vp_status enqueue_iteration(vp_server* s, bool even) {
+  cudaStream_t st = s->ctx->stream;
+  const uint32_t R = s->ring_cap;
+  uint32_t* qcur = even ? s->paths.qa : s->paths.qb;
+  uint32_t* qnext = even ? s->paths.qb : s->paths.qa;
+  Counters* ctr = s->ctx->counters;
+  k_srv_advance<<<1, 1, 0, st>>>(s->d_ctl, s->d_ring_base, s->d_ring_n, R);
+  k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_ring_base, s->d_ring_slot, R, s->paths, qcur);
+  if (s->accurate)
+    k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
+                                                               s->max_cap, ctr);
+  else
+    k_srv_extend<false><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
+                                                                s->max_cap, ctr);
+  k_srv_shade<<<s->thr_blocks, 256, 0, st>>>(s->d_envs, s->d_table, s->paths, qcur, s->d_ctl, qnext);
+  if (s->accurate)
+    k_srv_shadow<true><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, s->paths, s->d_ctl,
+                                                               s->max_cap, ctr);
+  else
+    k_srv_shadow<false><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, s->paths, s->d_ctl,
+                                                                s->max_cap, ctr);
+  k_srv_gather<<<s->thr_blocks, 256, 0, st>>>(s->d_table, s->paths, qcur, s->d_ctl, s->d_done);
+  VP_CUDA(cudaGetLastError());
+  return VP_OK;
+}
+
+// Kernel configuration and (once) the graph of two iterations; needs every scene added.
+vp_status prepare_launch(vp_server* s) {
+  if (s->thr_blocks) return VP_OK;
+  vp_context* ctx = s->ctx;
+  s->max_cap = 2;
+  for (vp_scene* sc : s->scenes) s->max_cap = std::max(s->max_cap, sc->view.stack_cap);
+  s->smem_ext = (size_t)8 * warp_smem_bytes(s->max_cap, kSrvHitCap);
+  s->smem_shd = (size_t)8 * warp_smem_bytes(s->max_cap, 32);
+  if (s->smem_ext > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the shared-memory stack");
+  auto ext = s->accurate ? k_srv_extend<true> : k_srv_extend<false>;
+  auto shd = s->accurate ? k_srv_shadow<true> : k_srv_shadow<false>;
+  if (s->smem_ext > 48 * 1024)
+    VP_CUDA(cudaFuncSetAttribute(ext, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_ext));
+  if (s->smem_shd > 48 * 1024)
+    VP_CUDA(cudaFuncSetAttribute(shd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_shd));
+  s->ext_blocks = ctx->sm_count * srv_blocks(ext, 256, s->smem_ext);
+  s->shd_blocks = ctx->sm_count * srv_blocks(shd, 256, s->smem_shd);
+  s->thr_blocks = ctx->sm_count * 8;
+  if (s->cfg.use_graph) {
+    cudaStream_t st = ctx->stream;
+    VP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    vp_status r1 = enqueue_iteration(s, true);
+    vp_status r2 = r1 == VP_OK ? enqueue_iteration(s, false) : r1;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (r2 != VP_OK) {
+      if (g) cudaGraphDestroy(g);
+      return r2;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    s->graph = g;
+    VP_CUDA(cudaGraphInstantiate(&s->graph_exec, g, 0));
+  }
+  return VP_OK;
+}
+
+vp_status admit(vp_server* s) {
+  cudaStream_t st = s->ctx->stream;
+  const uint32_t R = s->ring_cap;
+  bool any = false;
+  while (!s->pending.empty() && s->n_active < s->cfg.max_requests) {
+    const vp_request& rq = s->pending.front().r;
+    const size_t need = request_bytes(rq);
+    if (s->cfg.memory_budget_bytes && s->bytes_fixed + s->bytes_active + need > s->cfg.memory_budget_bytes) break;
+    uint32_t e = 0;
+    while (s->active[e].used) ++e;
+    vp_server::Active& a = s->active[e];
+    const uint32_t n_pix = rq.params.width * rq.params.height;
+    float4* sum = nullptr;
+    VP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sum), 16ull * n_pix, st));
+    VP_CUDA(cudaMemsetAsync(sum, 0, 16ull * n_pix, st));
+    VP_CUDA(cudaMemsetAsync(s->d_done + e, 0, sizeof(unsigned long long), st));
+    SrvRequest& t = s->h_table[e];
+    std::memset(&t, 0, sizeof(t));
+    build_camera(rq.camera, rq.params.width, rq.params.height, t.cam);
+    t.P = make_params(rq.params, s->scenes[rq.scene_id]);
+    t.P.accurate = s->accurate ? 1 : 0;
+    t.P.measure = 0;
+    t.scene = rq.scene_id;
+    t.n_pix = n_pix;
+    t.base = s->admit_end;
+    t.n_paths = (unsigned long long)n_pix * rq.params.spp;
+    t.sum = sum;
+    VP_CUDA(cudaMemcpyAsync(s->d_table + e, &t, sizeof(t), cudaMemcpyHostToDevice, st));
+    const uint32_t j = s->ring_hi % R;
+    s->h_ring_base[j] = t.base;
+    s->h_ring_n[j] = t.n_paths;
+    s->h_ring_slot[j] = e;
+    VP_CUDA(cudaMemcpyAsync(s->d_ring_base + j, s->h_ring_base + j, 8, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(s->d_ring_n + j, s->h_ring_n + j, 8, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(s->d_ring_slot + j, s->h_ring_slot + j, 4, cudaMemcpyHostToDevice, st));
+    a.used = true;
+    a.id = s->pending.front().id;
+    a.n_paths = t.n_paths;
+    a.n_pix = n_pix;
+    a.spp = rq.params.spp;
+    a.out = rq.out_rgba;
+    a.memory = rq.memory;
+    a.sum = sum;
+    a.bytes = need;
+    s->bytes_active += need;
+    s->admit_end += t.n_paths;
+    s->ring_hi += 1;
+    s->n_active += 1;
+    s->admitted += 1;
+    s->pending.pop_front();
+    any = true;
+  }
+  if (any) {
+    *s->h_admit_end = s->admit_end;
+    *s->h_ring_hi = s->ring_hi;
+    VP_CUDA(cudaMemcpyAsync(&s->d_ctl->admit_end, s->h_admit_end, 8, cudaMemcpyHostToDevice, st));
+    VP_CUDA(cudaMemcpyAsync(&s->d_ctl->ring_hi, s->h_ring_hi, 4, cudaMemcpyHostToDevice, st));
+  }
+  return VP_OK;
+}
+
+vp_status complete(vp_server* s, uint32_t* n_done) {
+  cudaStream_t st = s->ctx->stream;
+  const uint32_t R = s->cfg.max_requests;
+  uint32_t nd = 0;
+  for (uint32_t e = 0; e < R; ++e) {
+    vp_server::Active& a = s->active[e];
+    if (!a.used || s->h_done[e] < a.n_paths) continue;
+    const float inv = 1.0f / (float)a.spp;
+    const unsigned nb = (a.n_pix + 255u) / 256u;
+    if (a.memory == VP_MEMORY_DEVICE) {
+      k_srv_finish<<<nb, 256, 0, st>>>(a.sum, a.n_pix, inv, reinterpret_cast<float4*>(a.out));
+      VP_CUDA(cudaGetLastError());
+    } else {
+      float4* tmp = nullptr;
+      VP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp), 16ull * a.n_pix, st));
+      k_srv_finish<<<nb, 256, 0, st>>>(a.sum, a.n_pix, inv, tmp);
+      VP_CUDA(cudaGetLastError());
+      VP_CUDA(cudaMemcpyAsync(a.out, tmp, 16ull * a.n_pix, cudaMemcpyDeviceToHost, st));
+      VP_CUDA(cudaFreeAsync(tmp, st));
+    }
+    VP_CUDA(cudaFreeAsync(a.sum, st));
+    s->bytes_active -= a.bytes;
+    s->paths_completed += a.n_paths;
+    s->done_ids.push_back(a.id);
+    a = vp_server::Active{};
+    s->n_active -= 1;
+    s->completed += 1;
+    ++nd;
+  }
+  if (nd) VP_CUDA(cudaStreamSynchronize(st));
+  *n_done = nd;
+  return VP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_server** out) {
+  if (!ctx || !out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  VP_CUDA(cudaSetDevice(ctx->device));
+  auto* s = new (std::nothrow) vp_server();
+  if (!s) return fail(VP_ERROR_OUT_OF_MEMORY, "host allocation failed");
+  s->ctx = ctx;
+  if (config) s->cfg = *config;
+  vp_server_config& c = s->cfg;
+  if (c.path_slots == 0) c.path_slots = 1u << 21;
+  if (c.max_requests == 0) c.max_requests = 256;
+  if (c.iterations_per_step == 0) c.iterations_per_step = 4;
+  c.iterations_per_step = (c.iterations_per_step + 1u) & ~1u;
+  if (c.path_slots > (1u << 28)) {
+    srv_free(s);
+    return fail(VP_ERROR_LIMIT, "path_slots above 2^28");
+  }
+  s->accurate = c.precision == VP_PRECISION_ACCURATE;
+  const uint32_t R = c.max_requests, P = c.path_slots;
+  s->ring_cap = kRingPerEntry * R + 2u;
+  const uint32_t RC = s->ring_cap;
+  s->active.resize(R);
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  chk(cudaMalloc(&s->d_scenes, kMaxScenes * sizeof(SceneView)));
+  chk(cudaMalloc(&s->d_envs, kMaxScenes * sizeof(EnvView)));
+  chk(cudaMalloc(&s->d_table, R * sizeof(SrvRequest)));
+  chk(cudaMalloc(&s->d_done, R * sizeof(unsigned long long)));
+  chk(cudaMalloc(&s->d_ring_base, RC * 8ull));
+  chk(cudaMalloc(&s->d_ring_n, RC * 8ull));
+  chk(cudaMalloc(&s->d_ring_slot, RC * 4ull));
+  chk(cudaMalloc(&s->d_ctl, sizeof(SrvCtl)));
+  chk(cudaMallocHost(&s->h_table, R * sizeof(SrvRequest)));
+  chk(cudaMallocHost(&s->h_done, R * sizeof(unsigned long long)));
+  chk(cudaMallocHost(&s->h_ring_base, RC * 8ull));
+  chk(cudaMallocHost(&s->h_ring_n, RC * 8ull));
+  chk(cudaMallocHost(&s->h_ring_slot, RC * 4ull));
+  chk(cudaMallocHost(&s->h_admit_end, 8));
+  chk(cudaMallocHost(&s->h_ring_hi, 4));
+  chk(cudaEventCreate(&s->ev0));
+  chk(cudaEventCreate(&s->ev1));
+  const size_t slot_bytes = (size_t)P * kSlotBytes + 32 * 256;
+  chk(cudaMalloc(&s->path_mem, slot_bytes));
+  if (e != cudaSuccess) {
+    srv_free(s);
+    return cuda_fail(e, "vp_server_create");
+  }
+  char* cur = static_cast<char*>(s->path_mem);
+  SrvPaths& b = s->paths;
+  srv_carve(cur, b.o4, P);
+  srv_carve(cur, b.d4, P);
+  srv_carve(cur, b.thr4, P);
+  srv_carve(cur, b.rad4, P);
+  srv_carve(cur, b.alb4, P);
+  srv_carve(cur, b.rng4, P);
+  srv_carve(cur, b.key2, P);
+  srv_carve(cur, b.meta, P);
+  srv_carve(cur, b.req, P);
+  srv_carve(cur, b.pix, P);
+  srv_carve(cur, b.so4, 3ull * P);
+  srv_carve(cur, b.sd4, 3ull * P);
+  srv_carve(cur, b.sw4, 3ull * P);
+  srv_carve(cur, b.qa, P);
+  srv_carve(cur, b.qb, P);
+  srv_carve(cur, b.qs, 3ull * P);
+  srv_carve(cur, b.free_stack, P);
+  s->bytes_fixed = slot_bytes + R * (sizeof(SrvRequest) + 8ull) + RC * 20ull;
+  cudaStream_t st = ctx->stream;
+  k_srv_init<<<(P + 255) / 256, 256, 0, st>>>(s->d_ctl, b.free_stack, P);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, R * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    srv_free(s);
+    return cuda_fail(e, "vp_server_create");
+  }
+  if (c.memory_budget_bytes && s->bytes_fixed > c.memory_budget_bytes) {
+    srv_free(s);
+    return fail(VP_ERROR_LIMIT, "memory budget below the server's path slots");
+  }
+  *out = s;
+  return VP_OK;
+}
+
+vp_status vp_server_add_scene(vp_server* s, vp_scene* scene, vp_env* env, uint32_t* scene_id) {
+  if (!s || !scene || !env || !scene_id) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (scene->ctx != s->ctx || env->ctx != s->ctx) return fail(VP_ERROR_INVALID_ARGUMENT, "objects belong to different contexts");
+  if (s->thr_blocks) return fail(VP_ERROR_INVALID_ARGUMENT, "scenes must be added before the first vp_server_step");
+  if (s->scenes.size() >= kMaxScenes) return fail(VP_ERROR_LIMIT, "too many resident scenes");
+  const size_t need = scene->info.device_bytes;
+  if (s->cfg.memory_budget_bytes && s->bytes_fixed + need > s->cfg.memory_budget_bytes)
+    return fail(VP_ERROR_LIMIT, "scene does not fit the memory budget");
+  const uint32_t id = (uint32_t)s->scenes.size();
+  VP_CUDA(cudaSetDevice(s->ctx->device));
+  VP_CUDA(cudaMemcpy(s->d_scenes + id, &scene->view, sizeof(SceneView), cudaMemcpyHostToDevice));
+  VP_CUDA(cudaMemcpy(s->d_envs + id, &env->view, sizeof(EnvView), cudaMemcpyHostToDevice));
+  s->scenes.push_back(scene);
+  s->envs.push_back(env);
+  s->bytes_fixed += need;
+  *scene_id = id;
+  return VP_OK;
+}
+
+vp_status vp_server_submit(vp_server* s, const vp_request* r, uint64_t* request_id) {
+  if (!s || !r) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (r->scene_id >= s->scenes.size()) return fail(VP_ERROR_INVALID_ARGUMENT, "unknown scene_id");
+  if (!r->out_rgba) return fail(VP_ERROR_INVALID_ARGUMENT, "out_rgba is NULL");
+  if (r->memory != VP_MEMORY_HOST && r->memory != VP_MEMORY_DEVICE) return fail(VP_ERROR_INVALID_ARGUMENT, "bad memory kind");
+  vp_status st;
+  if ((st = check_params(&r->params))) return st;
+  if (r->params.max_bounces == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "max_bounces must be positive for a served request");
+  if (s->cfg.memory_budget_bytes && s->bytes_fixed + request_bytes(*r) > s->cfg.memory_budget_bytes)
+    return fail(VP_ERROR_LIMIT, "request does not fit the memory budget");
+  const uint64_t id = s->next_id++;
+  s->pending.push_back({id, *r});
+  if (request_id) *request_id = id;
+  return VP_OK;
+}
+
+vp_status vp_server_step(vp_server* s, uint32_t* completed) {
+  if (!s) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (completed) *completed = 0;
+  if (s->scenes.empty()) return fail(VP_ERROR_INVALID_ARGUMENT, "no resident scene");
+  VP_CUDA(cudaSetDevice(s->ctx->device));
+  vp_status r;
+  if ((r = prepare_launch(s))) return r;
+  if ((r = admit(s))) return r;
+  if (s->n_active == 0) return VP_OK;
+  cudaStream_t st = s->ctx->stream;
+  VP_CUDA(cudaMemsetAsync(s->ctx->counters, 0, sizeof(Counters), st));
+  VP_CUDA(cudaEventRecord(s->ev0, st));
+  for (uint32_t k = 0; k < s->cfg.iterations_per_step; k += 2) {
+    if (s->graph_exec) {
+      VP_CUDA(cudaGraphLaunch(s->graph_exec, st));
+    } else {
+      if ((r = enqueue_iteration(s, true))) return r;
+      if ((r = enqueue_iteration(s, false))) return r;
+    }
+  }
+  VP_CUDA(cudaEventRecord(s->ev1, st));
+  VP_CUDA(cudaMemcpyAsync(s->h_done, s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+  VP_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  VP_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+  s->device_ms += ms;
+  s->iterations += s->cfg.iterations_per_step;
+  Counters c{};
+  VP_CUDA(cudaMemcpy(&c, s->ctx->counters, sizeof(c), cudaMemcpyDeviceToHost));
+  if (c.status) return fail(VP_ERROR_DEVICE_STATUS, "a serving kernel raised device status " + std::to_string(c.status));
+  uint32_t nd = 0;
+  if ((r = complete(s, &nd))) return r;
+  if (completed) *completed = nd;
+  return VP_OK;
+}
+
+vp_status vp_server_poll(vp_server* s, uint64_t* ids, uint32_t cap, uint32_t* n) {
+  if (!s || !n || (cap && !ids)) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done_ids.size());
+  for (uint32_t i = 0; i < k; ++i) ids[i] = s->done_ids[i];
+  s->done_ids.erase(s->done_ids.begin(), s->done_ids.begin() + k);
+  *n = k;
+  return VP_OK;
+}
+
+vp_status vp_server_get_stats(vp_server* s, vp_server_stats* out) {
+  if (!s || !out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  out->submitted = s->next_id;
+  out->admitted = s->admitted;
+  out->completed = s->completed;
+  out->paths_completed = s->paths_completed;
+  out->iterations = s->iterations;
+  out->active = s->n_active;
+  out->pending = (uint32_t)s->pending.size();
+  out->bytes_in_use = s->bytes_fixed + s->bytes_active;
+  out->device_ms = s->device_ms;
+  return VP_OK;
+}
+
+vp_status vp_server_destroy(vp_server* s) {
+  srv_free(s);
+  return VP_OK;
+}
+
+}  // extern "C"

@@ -78,8 +78,9 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_ca
 enum QueryKind { kArgmin = 0, kTau = 1 };
 
 struct WarpStats {
-  unsigned long long crossings = 0, nodes = 0, leaves = 0, prim_tests = 0, geo_loads = 0;
+  unsigned long long crossings = 0, nodes = 0, leaves = 0;
   unsigned long long kind_nodes[3] = {0, 0, 0}, kind_leaves[3] = {0, 0, 0};
+  unsigned long long kind_prims[3] = {0, 0, 0}, kind_geo[3] = {0, 0, 0};  // boxes tested, records loaded
   unsigned int max_hits = 0;
 };
 
@@ -179,7 +180,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       if (measure) {
         ws.leaves++;
         ws.kind_leaves[kKind]++;
-        ws.prim_tests += total;
+        ws.kind_prims[kKind] += total;
       }
       bool hit = false;
       Chord ch;
@@ -197,7 +198,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           icf = g.icf;
         }
       }
-      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
+      if (measure) ws.kind_geo[kKind] += __popc(__ballot_sync(kFull, boxed));
       const unsigned m = __ballot_sync(kFull, hit);
       if (keep && m != 0u && hb + 32 > W.hit_cap) {  // make room for up to 32 new chords
         compact();
@@ -327,12 +328,12 @@ __device__ float3 warp_albedo(const SceneView& S, const WarpSmem& W, float3 x, u
       if (measure) {
         ws.leaves++;
         ws.kind_leaves[2]++;
-        ws.prim_tests += count;
+        ws.kind_prims[2] += count;
       }
       const uint32_t pi = first + lane;
       const bool boxed = (uint32_t)lane < count &&
                          box_contains(__ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), x);
-      if (measure) ws.geo_loads += __popc(__ballot_sync(kFull, boxed));
+      if (measure) ws.kind_geo[2] += __popc(__ballot_sync(kFull, boxed));
       if (boxed) {
         const PrimGeo g = load_geo(S.prims, pi);
         float r2;
@@ -420,7 +421,10 @@ struct ThreadQueries {
         if (!hit[c]) continue;
         if (ref_is_leaf(refs[c])) {
           const uint32_t pi = refs[c] & ~kLeafBit;
-          if (measure) ws.geo_loads++;
+          if (measure) {
+            ws.kind_prims[kKind]++;
+            ws.kind_geo[kKind]++;
+          }
           const PrimGeo g = load_geo(S.prims, pi);
           Chord ch;
           if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.f && ch.t_in <= t_hi) {
@@ -488,7 +492,10 @@ struct ThreadQueries {
         if (r == kEmptyRef || !box_contains(bl[c], bh[c], x)) continue;
         if (ref_is_leaf(r)) {
           const uint32_t pi = r & ~kLeafBit;
-          if (measure) ws.geo_loads++;
+          if (measure) {
+            ws.kind_prims[2]++;
+            ws.kind_geo[2]++;
+          }
           const PrimGeo g = load_geo(S.prims, pi);
           float r2;
           if constexpr (kAcc) {

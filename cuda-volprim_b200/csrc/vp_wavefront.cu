@@ -151,12 +151,12 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
       atomicAdd(&ctr->crossings, ws.crossings);
       atomicAdd(&ctr->nodes, ws.nodes);
       atomicAdd(&ctr->leaves, ws.leaves);
-      atomicAdd(&ctr->prim_tests, ws.prim_tests);
-      atomicAdd(&ctr->geo_loads, ws.geo_loads);
       atomicMax(&ctr->max_hits, ws.max_hits);
       for (int k = 0; k < 3; ++k) {
         atomicAdd(&ctr->kind_nodes[k], ws.kind_nodes[k]);
         atomicAdd(&ctr->kind_leaves[k], ws.kind_leaves[k]);
+        atomicAdd(&ctr->kind_prims[k], ws.kind_prims[k]);
+        atomicAdd(&ctr->kind_geo[k], ws.kind_geo[k]);
       }
     }
   }
@@ -237,12 +237,12 @@ __global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(Scen
       atomicAdd(&ctr->crossings, ws.crossings);
       atomicAdd(&ctr->nodes, ws.nodes);
       atomicAdd(&ctr->leaves, ws.leaves);
-      atomicAdd(&ctr->prim_tests, ws.prim_tests);
-      atomicAdd(&ctr->geo_loads, ws.geo_loads);
       atomicMax(&ctr->max_hits, ws.max_hits);
       for (int k = 0; k < 3; ++k) {
         atomicAdd(&ctr->kind_nodes[k], ws.kind_nodes[k]);
         atomicAdd(&ctr->kind_leaves[k], ws.kind_leaves[k]);
+        atomicAdd(&ctr->kind_prims[k], ws.kind_prims[k]);
+        atomicAdd(&ctr->kind_geo[k], ws.kind_geo[k]);
       }
     }
   }
@@ -380,26 +380,61 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   const int ext_blocks = ctx->sm_count * resident_blocks(ext, threads, smem);
   const int shd_blocks = ctx->sm_count * resident_blocks(shd, threads, smem_sh);
   const int thr_blocks = ctx->sm_count * 8;
+  // VP_MEASURE_STAGES: events around the extend and shadow launches of each iteration (a ring of 4 iterations,
+  // read back at every poll, when the stream has drained)
+  cudaEvent_t* ev = ctx->stage_ev;
+  const bool timed = ctx->time_stages;
+  if (timed && !ev[0])
+    for (int i = 0; i < vp_context::kStageEvents; ++i) VP_CUDA(cudaEventCreate(&ev[i]));
+  uint32_t pending = 0;  // iterations whose events are recorded but not yet read
+  auto harvest = [&]() -> cudaError_t {
+    for (uint32_t j = 0; j < pending; ++j) {
+      float a = 0.f, c = 0.f;
+      cudaError_t er = cudaEventElapsedTime(&a, ev[4 * j + 0], ev[4 * j + 1]);
+      if (er == cudaSuccess) er = cudaEventElapsedTime(&c, ev[4 * j + 2], ev[4 * j + 3]);
+      if (er != cudaSuccess) return er;
+      ctx->stage_ms[0] += a;
+      ctx->stage_ms[1] += c;
+    }
+    pending = 0;
+    return cudaSuccess;
+  };
   k_wf_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, P, spp_offset, spp_count, paths, b);
   VP_CUDA(cudaGetLastError());
+  ctx->launches += 1;
   uint32_t* qcur = b.qa;
   uint32_t* qnext = b.qb;
   for (uint32_t it = 0; it < P.max_bounces; ++it) {
+    cudaEvent_t* e4 = ev + 4 * (it & 3u);
+    if (timed) VP_CUDA(cudaEventRecord(e4[0], st));
     ext<<<ext_blocks, threads, smem, st>>>(s->view, P, b, qcur, b.ctr + 0, b.ctr + 3, ctx->counters);
+    if (timed) VP_CUDA(cudaEventRecord(e4[1], st));
     k_wf_shade<<<thr_blocks, threads, 0, st>>>(e->view, P, b, qcur, b.ctr + 0, qnext, b.ctr + 1, ctx->counters);
+    if (timed) VP_CUDA(cudaEventRecord(e4[2], st));
     shd<<<shd_blocks, threads, smem_sh, st>>>(s->view, b, b.ctr + 2, b.ctr + 4, ctx->counters, P.measure);
+    if (timed) VP_CUDA(cudaEventRecord(e4[3], st));
     k_wf_gather<<<thr_blocks, threads, 0, st>>>(P, b, qcur, b.ctr + 0);
     k_wf_advance<<<1, 1, 0, st>>>(b.ctr);
     VP_CUDA(cudaGetLastError());
+    ctx->launches += 5;
+    ctx->stage_launches[0] += 1;
+    ctx->stage_launches[1] += 1;
+    if (timed) ++pending;
     std::swap(qcur, qnext);
     if ((it & 3u) == 3u) {  // stop once no path is alive
       VP_CUDA(cudaMemcpyAsync(ctx->wf.host_count, b.ctr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
       VP_CUDA(cudaStreamSynchronize(st));
+      VP_CUDA(harvest());
       if (*ctx->wf.host_count == 0u) break;
     }
   }
   k_wf_welford<<<(n_pix + 255) / 256, 256, 0, st>>>(b, spp_count, n_pix, img->mean, img->count);
   VP_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  if (timed && pending) {
+    VP_CUDA(cudaStreamSynchronize(st));
+    VP_CUDA(harvest());
+  }
   return VP_OK;
 }
 

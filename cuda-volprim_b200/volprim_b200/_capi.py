@@ -15,6 +15,7 @@ VP_MEMORY_HOST, VP_MEMORY_DEVICE = 0, 1
 VP_NEE_MIS, VP_NEE_PHASE, VP_NEE_RIS, VP_NEE_NONE = 0, 1, 2, 3
 VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL, VP_ENGINE_WAVEFRONT = 0, 1, 2
 VP_PRECISION_AUTO, VP_PRECISION_FAST, VP_PRECISION_ACCURATE = 0, 1, 2
+VP_MEASURE_COUNTERS, VP_MEASURE_STAGES = 1, 2
 
 ERROR_NAMES = {
     -1: "VP_ERROR_INVALID_ARGUMENT", -2: "VP_ERROR_CUDA", -3: "VP_ERROR_OUT_OF_MEMORY",
@@ -108,6 +109,11 @@ class vp_render_stats(C.Structure):
         ("max_hits_per_ray", C.c_uint32),
         ("max_point_overlap", C.c_uint32),
         ("device_status", C.c_uint32),
+        ("launches", C.c_uint32),
+        ("query_prim_tests", C.c_uint64 * 3),
+        ("query_geo_loads", C.c_uint64 * 3),
+        ("ms_stage", C.c_double * 3),
+        ("stage_launches", C.c_uint32 * 3),
         ("reserved", C.c_uint32),
     ]
 
@@ -119,6 +125,54 @@ class vp_render_stats(C.Structure):
             v = getattr(self, name)
             out[name] = list(v) if isinstance(v, C.Array) else v
         return out
+
+
+class vp_gaussian_grads(C.Structure):
+    _fields_ = [
+        ("mean", C.c_void_p),
+        ("scale", C.c_void_p),
+        ("quat_wxyz", C.c_void_p),
+        ("density", C.c_void_p),
+        ("emission", C.c_void_p),
+        ("memory", C.c_int32),
+    ]
+
+
+class vp_server_config(C.Structure):
+    _fields_ = [
+        ("memory_budget_bytes", C.c_uint64),
+        ("path_slots", C.c_uint32),
+        ("max_requests", C.c_uint32),
+        ("iterations_per_step", C.c_uint32),
+        ("precision", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class vp_request(C.Structure):
+    _fields_ = [
+        ("scene_id", C.c_uint32),
+        ("camera", vp_camera),
+        ("params", vp_render_params),
+        ("out_rgba", C.c_void_p),
+        ("memory", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class vp_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("admitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("paths_completed", C.c_uint64),
+        ("iterations", C.c_uint64),
+        ("active", C.c_uint32),
+        ("pending", C.c_uint32),
+        ("bytes_in_use", C.c_uint64),
+        ("device_ms", C.c_double),
+    ]
 
 
 P = C.c_void_p
@@ -155,6 +209,18 @@ SIGNATURES = {
     "vp_transmittance_static": [P, P, P, C.c_uint32, C.c_int32, P, C.c_int32],
     "vp_camera_rays": [P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, P, P, C.c_uint32, P, P, C.c_int32],
     "vp_normalize_accumulator": [P, P, P, C.c_size_t, C.c_float, P],
+    "vp_scene_set_emission": [P, P, C.c_int32],
+    "vp_render_emission": [P, P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, C.c_int32,
+                           C.POINTER(vp_render_stats)],
+    "vp_render_emission_backward": [P, P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, C.c_int32,
+                                    C.POINTER(vp_gaussian_grads), C.POINTER(vp_render_stats)],
+    "vp_server_create": [P, C.POINTER(vp_server_config), PP],
+    "vp_server_add_scene": [P, P, P, C.POINTER(C.c_uint32)],
+    "vp_server_submit": [P, C.POINTER(vp_request), C.POINTER(C.c_uint64)],
+    "vp_server_step": [P, C.POINTER(C.c_uint32)],
+    "vp_server_poll": [P, C.POINTER(C.c_uint64), C.c_uint32, C.POINTER(C.c_uint32)],
+    "vp_server_get_stats": [P, C.POINTER(vp_server_stats)],
+    "vp_server_destroy": [P],
 }
 _RESTYPES = {"vp_last_error_string": C.c_char_p}
 

@@ -29,6 +29,21 @@ def _is_cuda_tensor(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+def _sync_torch(*xs) -> None:
+    """Wait for torch's current stream on the devices of the CUDA tensors among xs: the library
+    runs on its own stream, so torch's pending writes to memory it reads must be complete."""
+    import torch
+    for dev in {x.device for x in xs if _is_cuda_tensor(x)}:
+        torch.cuda.current_stream(dev).synchronize()
+
+
+def _alive(ctx) -> bool:
+    """Whether a wrapper's context is still open.  Scenes, environments, images and servers hold
+    a pointer to their vp_context; once it is destroyed they cannot be destroyed safely, so a
+    wrapper closed after its context only drops its handle (the memory goes with the process)."""
+    return ctx is not None and getattr(ctx, "handle", None) is not None
+
+
 def _host_f32(x, n: int, what: str) -> np.ndarray:
     a = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).reshape(-1)
     if a.size != n:
@@ -123,6 +138,7 @@ class Scene:
             s.mean, s.scale = dptr(g.mean, 3 * n), dptr(g.scale, 3 * n)
             s.quat_wxyz, s.density = dptr(g.quat_wxyz, 4 * n), dptr(g.density, n)
             s.albedo = dptr(g.albedo, 3 * n) if g.albedo is not None else None
+            _sync_torch(*self._keep)
         else:
             arrs = [_host_f32(g.mean, 3 * n, "mean"), _host_f32(g.scale, 3 * n, "scale"),
                     _host_f32(g.quat_wxyz, 4 * n, "quat_wxyz"), _host_f32(g.density, n, "density")]
@@ -186,6 +202,21 @@ class Scene:
                                           _capi.VP_MEMORY_HOST))
         return out
 
+    def set_emission(self, rgb):
+        """RGB emission per unit optical depth, (count, 3) in the order the scene was built from
+        (vp_scene_set_emission); a host array or a CUDA tensor."""
+        n = self.info()["count"]
+        if _is_cuda_tensor(rgb):
+            import torch
+            t = rgb.detach().to(torch.float32).contiguous().reshape(-1)
+            if t.numel() != 3 * n:
+                raise ValueError(f"emission: expected {3 * n} floats, got {t.numel()}")
+            _sync_torch(t)
+            check(lib.vp_scene_set_emission(self.handle, t.data_ptr(), _capi.VP_MEMORY_DEVICE))
+            return
+        a = _host_f32(rgb, 3 * n, "emission")
+        check(lib.vp_scene_set_emission(self.handle, a.ctypes.data, _capi.VP_MEMORY_HOST))
+
     def albedo_at(self, points, precision: int = _capi.VP_PRECISION_AUTO, engine: int = _capi.VP_ENGINE_WARP):
         """(albedo rgb (n, 3), overlap count (n,)) at points (vp_albedo_at)."""
         p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1)
@@ -198,7 +229,8 @@ class Scene:
 
     def close(self):
         if getattr(self, "handle", None):
-            lib.vp_scene_destroy(self.handle)
+            if _alive(self.ctx):
+                lib.vp_scene_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -239,7 +271,8 @@ class Environment:
 
     def close(self):
         if getattr(self, "handle", None):
-            lib.vp_env_destroy(self.handle)
+            if _alive(self.ctx):
+                lib.vp_env_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -299,7 +332,8 @@ class Config:
     hg_g: float = 0.85
     use_ris: bool = False
     ris_num_candidates: int = 6
-    measure_caps: bool = False
+    measure_caps: bool = False  # device counters (VP_MEASURE_COUNTERS)
+    time_stages: bool = False   # CUDA-event time of the wavefront stages (VP_MEASURE_STAGES)
     nee: str = "mis"            # "mis" | "phase" | "ris" | "none"  (use_ris=True selects "ris")
     engine: str = "wavefront"   # "wavefront" | "warp" | "megakernel"
     precision: str = "auto"     # "auto" | "fast" | "accurate"
@@ -319,7 +353,8 @@ class Config:
         p.batch_spp = self.batch_spp
         p.engine = {"warp": 0, "megakernel": 1, "wavefront": 2}[self.engine]
         p.precision = {"auto": 0, "fast": 1, "accurate": 2}[self.precision]
-        p.measure = 1 if self.measure_caps else 0
+        p.measure = ((_capi.VP_MEASURE_COUNTERS if self.measure_caps else 0)
+                     | (_capi.VP_MEASURE_STAGES if self.time_stages else 0))
         return p
 
 
@@ -388,7 +423,8 @@ class ProgressiveImage:
 
     def close(self):
         if getattr(self, "handle", None):
-            lib.vp_image_destroy(self.handle)
+            if _alive(self.ctx):
+                lib.vp_image_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

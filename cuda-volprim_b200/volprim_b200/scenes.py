@@ -14,6 +14,13 @@ are absent), so every scene here is generated from a seed with the stated distri
   stress_2m          2M Gaussians around 16 isotropic normal clusters (std 0.15), scales
                      logN(ln 0.05, 0.3), densities logN(ln 2, 0.5), albedo 0.8, same env,
                      1024x1024, 64 spp.
+  serving_4          the serving form's resident scenes: showcase_500k's generator at 50k, 100k,
+                     250k and 500k Gaussians with seeds 1-4 (sigma-multiplier 7.5), each with the
+                     procedural environment; requests from volprim_b200.serving.make_trace.
+  emission_100k      the differentiation form: 100k Gaussians with showcase_500k's distributions
+                     (log-scales as the parameters), RGB emission U[0,1], sigma-multiplier 7.5,
+                     4 cameras at distance 3.5 in seeded directions looking at the origin,
+                     256x256, 8 spp, constant white environment.
 Densities are the reference's mass convention (ply.cpp:107-116).
 """
 from __future__ import annotations
@@ -177,3 +184,53 @@ def stress_2m(seed: int = 0, n: int = 2_000_000, res: int = 1024, spp: int = 64,
                  max_bounces=64, rr_depth=12, nee="mis")
     env = procedural_env(*env_size)
     return Workload("stress_2m", stress_gaussians(n, seed), 1.0, negz_camera(), cfg, env)
+
+
+@dataclass
+class EmissionWorkload:
+    name: str
+    gaussians: Gaussians     # scale_is_log=True: the log-scales are the differentiated parameters
+    emission: np.ndarray     # (N, 3) RGB per unit optical depth
+    sigma_multiplier: float
+    cameras: list
+    config: Config
+    env_constant: tuple      # constant environment radiance (RGB)
+
+
+def sphere_cameras(rng: np.random.Generator, k: int, distance: float = 3.5, vfov: float = 40.0) -> list:
+    """k pinhole cameras at `distance` from the origin in uniform random directions, looking at it."""
+    cams = []
+    for _ in range(k):
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        up = (0.0, 1.0, 0.0) if abs(v[1]) < 0.95 else (0.0, 0.0, 1.0)
+        cams.append(Camera.perspective(tuple(float(x) for x in distance * v), (0.0, 0.0, 0.0), up, vfov))
+    return cams
+
+
+def emission_100k(seed: int = 0, n: int = 100_000, res: int = 256, spp: int = 8, n_cams: int = 4) -> EmissionWorkload:
+    g = showcase_gaussians(n, seed)
+    rng = np.random.default_rng(seed + 101)
+    emission = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+    gl = Gaussians(g.mean, np.log(g.scale).astype(np.float32), g.quat_wxyz, g.density, None, scale_is_log=True)
+    cfg = Config(num_samples_per_pixel=spp, image_width=res, image_height=res, seed=seed, precision="fast")
+    return EmissionWorkload("emission_100k", gl, emission, 7.5, sphere_cameras(rng, n_cams), cfg, (1.0, 1.0, 1.0))
+
+
+def perturbed(w: EmissionWorkload, seed: int = 1) -> tuple:
+    """Seeded perturbation of a workload's parameters (the target of the image loss):
+    (Gaussians, emission)."""
+    rng = np.random.default_rng(seed)
+    g = w.gaussians
+    n = g.count
+    mean = (g.mean + rng.normal(0.0, 0.005, (n, 3))).astype(np.float32)
+    ls = (g.scale + rng.normal(0.0, 0.05, (n, 3))).astype(np.float32)
+    q = (g.quat_wxyz + rng.normal(0.0, 0.05, (n, 4))).astype(np.float32)
+    dens = (g.density * np.exp(rng.normal(0.0, 0.1, n))).astype(np.float32)
+    em = np.clip(w.emission + rng.normal(0.0, 0.05, (n, 3)), 0.0, 1.0).astype(np.float32)
+    return Gaussians(mean, ls, q, dens, None, scale_is_log=True), em
+
+
+def serving_scenes(sizes=(50_000, 100_000, 250_000, 500_000), seeds=(1, 2, 3, 4), env_size=(2048, 1024)) -> tuple:
+    """([Gaussians per scene], sigma_multiplier, environment image) of the serving workload."""
+    return [showcase_gaussians(n, s) for n, s in zip(sizes, seeds)], 7.5, procedural_env(*env_size)

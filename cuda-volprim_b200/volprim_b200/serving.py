@@ -1,0 +1,219 @@
+"""Serving over the C ABI (vp_server_*): several scenes resident on the device, a request FIFO
+admitted by a device-memory budget, and continuous batching of every admitted request's paths
+into the same wavefront launches (replayed as a captured CUDA graph).
+
+`make_trace` builds the serving workload's request stream (Poisson arrivals; scene, square
+resolution and spp drawn uniformly; a random camera on a sphere around the scene) and
+`run_trace` replays it in real time against a Server, recording each request's latency from its
+arrival to the moment the host sees it complete.  `run_trace_plain` replays the same stream with
+one vp_render call per request in arrival order (the plain per-request launch).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, lib
+from .api import Camera, Config, Context, Environment, Scene, _alive, _is_cuda_tensor, _sync_torch
+
+
+class Server:
+    """vp_server_create / add_scene / submit / step / poll."""
+
+    def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 21,
+                 max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
+                 use_graph: bool = True):
+        c = _capi.vp_server_config()
+        c.memory_budget_bytes = int(memory_budget_bytes)
+        c.path_slots = int(path_slots)
+        c.max_requests = int(max_requests)
+        c.iterations_per_step = int(iterations_per_step)
+        c.precision = {"auto": 0, "fast": 1, "accurate": 2}[precision]
+        c.use_graph = 1 if use_graph else 0
+        h = C.c_void_p()
+        check(lib.vp_server_create(ctx.handle, C.byref(c), C.byref(h)))
+        self.handle, self.ctx = h, ctx
+        self._outs = {}
+
+    def add_scene(self, scene: Scene, env: Environment) -> int:
+        sid = C.c_uint32()
+        check(lib.vp_server_add_scene(self.handle, scene.handle, env.handle, C.byref(sid)))
+        return sid.value
+
+    def submit(self, scene_id: int, camera: Camera, config: Config, out=None) -> int:
+        """Queues a request; its (H, W, 4) mean image lands in `out` (a host array or a CUDA
+        tensor; a new host array when None) when it completes.  Returns the request id."""
+        r = _capi.vp_request()
+        r.scene_id = int(scene_id)
+        r.camera = camera.to_c()
+        r.params = config.to_c()
+        shape = (config.image_height, config.image_width, 4)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        if _is_cuda_tensor(out):
+            if not out.is_contiguous() or tuple(out.shape) != shape:
+                raise ValueError("out must be a contiguous (H, W, 4) float32 CUDA tensor")
+            _sync_torch(out)
+            r.out_rgba, r.memory = out.data_ptr(), _capi.VP_MEMORY_DEVICE
+        else:
+            if out.dtype != np.float32 or not out.flags.c_contiguous or out.shape != shape:
+                raise ValueError("out must be a contiguous (H, W, 4) float32 array")
+            r.out_rgba, r.memory = out.ctypes.data, _capi.VP_MEMORY_HOST
+        rid = C.c_uint64()
+        check(lib.vp_server_submit(self.handle, C.byref(r), C.byref(rid)))
+        self._outs[rid.value] = out
+        return rid.value
+
+    def step(self) -> int:
+        n = C.c_uint32()
+        check(lib.vp_server_step(self.handle, C.byref(n)))
+        return n.value
+
+    def poll(self) -> list:
+        ids = (C.c_uint64 * 1024)()
+        out = []
+        while True:
+            n = C.c_uint32()
+            check(lib.vp_server_poll(self.handle, ids, 1024, C.byref(n)))
+            out.extend(ids[i] for i in range(n.value))
+            if n.value < 1024:
+                return out
+
+    def result(self, request_id: int):
+        """The output buffer of a completed request (released from the server's bookkeeping)."""
+        return self._outs.pop(request_id)
+
+    def stats(self) -> dict:
+        s = _capi.vp_server_stats()
+        check(lib.vp_server_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            if _alive(self.ctx):
+                lib.vp_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Request:
+    arrival: float          # seconds from the trace start
+    scene_id: int
+    camera: Camera
+    config: Config
+
+    @property
+    def paths(self) -> int:
+        c = self.config
+        return c.image_width * c.image_height * c.num_samples_per_pixel
+
+
+def random_camera(rng: np.random.Generator, distance: float = 3.5, vfov: float = 40.0) -> Camera:
+    v = rng.normal(size=3)
+    v /= np.linalg.norm(v)
+    up = (0.0, 1.0, 0.0) if abs(v[1]) < 0.95 else (0.0, 0.0, 1.0)
+    return Camera.perspective(tuple(float(x) for x in distance * v), (0.0, 0.0, 0.0), up, vfov)
+
+
+def make_trace(seed: int, n: int, rate: float, n_scenes: int, resolutions=(64, 128, 256, 512),
+               spps=(1, 4, 16, 64), max_bounces: int = 64) -> list:
+    """n requests with exponential inter-arrival times of mean 1/rate: scene, square resolution and
+    spp uniform over the given choices, camera uniform on the sphere of radius 3.5 looking at the
+    origin, the scattering controls of the 500k showcase (MIS NEE, isotropic phase, roulette from
+    depth 12), seed = request index."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        res = int(rng.choice(resolutions))
+        spp = int(rng.choice(spps))
+        cfg = Config(num_samples_per_pixel=spp, image_width=res, image_height=res, seed=i, hg_g=0.0,
+                     max_bounces=max_bounces, rr_depth=12, nee="mis", precision="fast", batch_spp=16)
+        out.append(Request(t, int(rng.integers(n_scenes)), random_camera(rng), cfg))
+    return out
+
+
+def percentile(values, q: float) -> float:
+    """The q-th percentile (nearest rank on the sorted values)."""
+    v = sorted(values)
+    if not v:
+        return float("nan")
+    k = max(0, min(len(v) - 1, int(math.ceil(q / 100.0 * len(v))) - 1))
+    return float(v[k])
+
+
+def run_trace(server: Server, trace: list, keep_outputs: bool = False, out_factory=None) -> dict:
+    """Replays the trace in real time: each request is submitted once its arrival time has passed,
+    the server steps while anything is pending or active, and a request's latency runs from its
+    arrival to the step that completes it.  Returns latencies (s), makespan, paths and (optional)
+    outputs by trace index."""
+    t0 = time.perf_counter()
+    nxt = 0
+    ids = {}
+    lat = [None] * len(trace)
+    outs = {}
+    remaining = len(trace)
+    while remaining:
+        now = time.perf_counter() - t0
+        while nxt < len(trace) and trace[nxt].arrival <= now:
+            r = trace[nxt]
+            out = out_factory(r) if out_factory else None
+            ids[server.submit(r.scene_id, r.camera, r.config, out)] = nxt
+            nxt += 1
+        st = server.stats()
+        if st["active"] == 0 and st["pending"] == 0:
+            if nxt < len(trace):  # idle until the next arrival
+                time.sleep(max(0.0, trace[nxt].arrival - (time.perf_counter() - t0)))
+            continue
+        server.step()
+        done_t = time.perf_counter() - t0
+        for rid in server.poll():
+            k = ids.pop(rid)
+            lat[k] = done_t - trace[k].arrival
+            o = server.result(rid)
+            if keep_outputs:
+                outs[k] = o
+            remaining -= 1
+    makespan = time.perf_counter() - t0
+    paths = sum(r.paths for r in trace)
+    return {"latency_s": lat, "makespan_s": makespan, "paths": paths, "outputs": outs,
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99),
+            "mpaths_per_s": paths / makespan / 1e6, "server": server.stats()}
+
+
+def run_trace_plain(scenes: list, envs: list, trace: list) -> dict:
+    """The same stream through one vp_render per request, in arrival order (a request starts when
+    it has arrived and the previous one has finished)."""
+    t0 = time.perf_counter()
+    lat = []
+    busy = 0.0
+    for r in trace:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        a = time.perf_counter()
+        p = r.config.to_c()
+        cam = r.camera.to_c()
+        out = np.empty((r.config.image_height, r.config.image_width, 4), np.float32)
+        st = _capi.vp_render_stats()
+        check(lib.vp_render(scenes[r.scene_id].handle, envs[r.scene_id].handle, C.byref(cam), C.byref(p),
+                            out.ctypes.data, _capi.VP_MEMORY_HOST, C.byref(st)))
+        b = time.perf_counter()
+        busy += b - a
+        lat.append(b - t0 - r.arrival)
+    makespan = time.perf_counter() - t0
+    paths = sum(r.paths for r in trace)
+    return {"latency_s": lat, "makespan_s": makespan, "paths": paths, "busy_s": busy,
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "mpaths_per_s": paths / makespan / 1e6}

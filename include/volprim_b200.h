@@ -73,6 +73,12 @@ typedef enum vp_precision {
   VP_PRECISION_ACCURATE = 2 /* FP64 chord set-up; meets 1e-5 relative transmittance */
 } vp_precision;
 
+/* Bits of vp_render_params.measure. */
+typedef enum vp_measure {
+  VP_MEASURE_COUNTERS = 1,  /* device counters (the reference's --measure-caps and more) */
+  VP_MEASURE_STAGES = 2     /* per-stage CUDA-event timing of the wavefront launches */
+} vp_measure;
+
 typedef struct vp_context vp_context;
 typedef struct vp_scene vp_scene;
 typedef struct vp_env vp_env;
@@ -195,7 +201,9 @@ typedef struct vp_render_params {
   uint32_t batch_spp;      /* samples per launch (reference BATCH_SIZE = 16) */
   int32_t engine;          /* vp_engine */
   int32_t precision;       /* vp_precision */
-  int32_t measure;         /* 1: count crossings/bounces/shadow rays and maxima (costs atomics) */
+  int32_t measure;         /* bit set: VP_MEASURE_COUNTERS counts crossings, bounces, shadow rays
+                              and maxima (costs atomics); VP_MEASURE_STAGES times the wavefront
+                              stages with CUDA events (no device-side cost) */
 } vp_render_params;
 
 /* Fills the reference's defaults (config.h:119-136, launch_params.h:38-58). */
@@ -219,6 +227,14 @@ typedef struct vp_render_stats {
   uint32_t max_hits_per_ray;   /* largest candidate count of one query (measure != 0) */
   uint32_t max_point_overlap;  /* largest Gaussian overlap at a path vertex (measure != 0) */
   uint32_t device_status;      /* 0 = fine; else an error word raised by a kernel */
+  uint32_t launches;           /* kernels launched by the call (always counted) */
+  uint64_t query_prim_tests[3];/* Gaussian boxes tested per query kind        (measure counters) */
+  uint64_t query_geo_loads[3]; /* Gaussian records loaded per query kind       (measure counters) */
+  double ms_stage[3];          /* device time of the wavefront's [0] extend (free-flight argmin),
+                                  [1] shadow (transmittance) and [2] all other launches; the
+                                  warp and megakernel engines put their one kernel in [2]
+                                                                             (measure stages) */
+  uint32_t stage_launches[3];  /* launches in each ms_stage bucket            (measure stages) */
   uint32_t reserved;
 } vp_render_stats;
 
@@ -289,6 +305,113 @@ vp_status vp_camera_rays(vp_context* ctx, const vp_camera* camera, const vp_rend
  * Gaussian contains the point), out_overlap[n]. */
 vp_status vp_albedo_at(vp_scene* scene, const float* points, uint32_t n, int32_t precision,
                        int32_t engine, float* out_rgb, uint32_t* out_overlap, int32_t memory);
+
+/* ---------------------------------------------------------------------------------------- */
+/* absorption-plus-emission image and its adjoint (the differentiation form; no counterpart  */
+/* in the reference, which has neither emission nor gradients)                               */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Image model.  Along a camera ray, Gaussian i contributes the closed-form optical depth tau_i
+ * of its 3-sigma chord over [0, inf) (the vp_transmittance sum) and emits RGB e_i per unit
+ * optical depth.  With S = sum tau_i, C = sum tau_i e_i and T = exp(-S) the ray's radiance is
+ *     L = (1 - T) C / S + T env(d)          (L = env(d) when S = 0),
+ * the exact emission-absorption integral when the emission-to-extinction ratio along the ray
+ * is its tau-weighted mean C / S (exact for one Gaussian and in the optically thin limit).  It
+ * is independent of the order of the Gaussians along the ray.  A pixel is the mean of
+ * params->spp jittered camera rays seeded as vp_render's (box filter); only width, height, spp,
+ * seed, pixel_filter_stddev, precision and measure of params are read. */
+
+/* Sets the emission (RGB per unit optical depth, [3 * count] in the order the scene was built
+ * from).  A scene's emission is 0 until set. */
+vp_status vp_scene_set_emission(vp_scene* scene, const float* rgb, int32_t memory);
+
+/* Renders the absorption-plus-emission image: width*height*4 floats (alpha = 1). */
+vp_status vp_render_emission(vp_scene* scene, vp_env* env, const vp_camera* camera,
+                             const vp_render_params* params, float* out_rgba, int32_t memory,
+                             vp_render_stats* stats);
+
+/* Gradients of a loss with respect to the arrays the scene was built from (caller order). */
+typedef struct vp_gaussian_grads {
+  float* mean;      /* [3 * count] */
+  float* scale;     /* [3 * count]: d/d(log scale) if the scene was built with scale_is_log,
+                       else d/d(scale) */
+  float* quat_wxyz; /* [4 * count]: w.r.t. the quaternion as given (before normalisation) */
+  float* density;   /* [count]: w.r.t. the density as given (before sigma_multiplier) */
+  float* emission;  /* [3 * count] or NULL */
+  int32_t memory;   /* vp_memory of all five arrays */
+} vp_gaussian_grads;
+
+/* Adjoint of vp_render_emission.  dloss_drgba holds dLoss/d(out_rgba) (width*height*4; alpha
+ * ignored; pixels whose RGB gradient is 0 are skipped).  ADDS dLoss/d(parameter) into every
+ * array of grads, so calls for several cameras accumulate.  Each ray's Gaussians are found again
+ * by traversal (twice: once for the ray's sums, once to scatter gradients); nothing is stored
+ * between the forward and backward calls. */
+vp_status vp_render_emission_backward(vp_scene* scene, vp_env* env, const vp_camera* camera,
+                                      const vp_render_params* params, const float* dloss_drgba,
+                                      int32_t memory, vp_gaussian_grads* grads,
+                                      vp_render_stats* stats);
+
+/* ---------------------------------------------------------------------------------------- */
+/* serving: continuous batching of render requests over resident scenes (the serving form;   */
+/* no counterpart in the reference, which renders one configured image per process)          */
+/* ---------------------------------------------------------------------------------------- */
+
+/* A server owns a pool of path slots and the wavefront stage kernels over them.  Each iteration
+ * refills the slots freed by finished paths with new (pixel, sample) paths of the admitted
+ * requests in admission order, then extends, shades, traces shadow rays and gathers every path
+ * in flight -- paths of different requests, scenes, resolutions and sample counts share the same
+ * launches.  The iteration is captured once as a CUDA graph.  Requests wait in a FIFO until the
+ * request table has a free entry and their image accumulator fits the memory budget.  A finished
+ * path adds its sample to its request's per-pixel sum; a request completes when all its
+ * width*height*spp paths have finished, and its mean image is written to its output buffer.
+ * Each path's result is the one vp_render computes for the same scene, camera and params
+ * (the same PCG32 stream per (pixel, sample)); only the order of the per-pixel FP32 sums differs. */
+typedef struct vp_server vp_server;
+
+typedef struct vp_server_config {
+  uint64_t memory_budget_bytes;  /* device bytes for resident scenes + path slots + request
+                                    accumulators (0 = no limit) */
+  uint32_t path_slots;           /* paths in flight (0 = 2^21) */
+  uint32_t max_requests;         /* request table entries (0 = 256) */
+  uint32_t iterations_per_step;  /* wavefront iterations per vp_server_step (0 = 4; even) */
+  int32_t precision;             /* vp_precision of every request: FAST or ACCURATE (AUTO = FAST) */
+  int32_t use_graph;             /* 1: replay the iterations as a captured CUDA graph */
+  int32_t reserved;
+} vp_server_config;
+
+typedef struct vp_request {
+  uint32_t scene_id;             /* from vp_server_add_scene */
+  vp_camera camera;
+  vp_render_params params;       /* width, height, spp, seed and the path-tracing controls;
+                                    engine, batch_spp and precision are ignored */
+  float* out_rgba;               /* width*height*4 floats, written when the request completes */
+  int32_t memory;                /* vp_memory of out_rgba */
+  int32_t reserved;
+} vp_request;
+
+typedef struct vp_server_stats {
+  uint64_t submitted, admitted, completed;
+  uint64_t paths_completed;
+  uint64_t iterations;
+  uint32_t active;               /* admitted, not completed */
+  uint32_t pending;              /* submitted, not admitted */
+  uint64_t bytes_in_use;         /* scenes + slots + active accumulators (the budget's measure) */
+  double device_ms;              /* device time of the iterations run so far (CUDA events) */
+} vp_server_stats;
+
+vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_server** out);
+/* Makes (scene, env) resident under the returned id.  The scene and env must outlive the server.
+ * Call before the first vp_server_step (the graph is captured then). */
+vp_status vp_server_add_scene(vp_server* server, vp_scene* scene, vp_env* env, uint32_t* scene_id);
+/* Queues a request (copied); returns its id (submission order, from 0). */
+vp_status vp_server_submit(vp_server* server, const vp_request* request, uint64_t* request_id);
+/* Admits what fits, runs iterations_per_step wavefront iterations (nothing if idle), then
+ * completes finished requests.  *completed = requests completed by this call. */
+vp_status vp_server_step(vp_server* server, uint32_t* completed);
+/* Ids of requests completed since the last call (up to cap; the rest stay queued). */
+vp_status vp_server_poll(vp_server* server, uint64_t* ids, uint32_t cap, uint32_t* n);
+vp_status vp_server_get_stats(vp_server* server, vp_server_stats* out);
+vp_status vp_server_destroy(vp_server* server);
 
 /* Grid-stride copy out[i] = accumulator[i] * normalization_factor over n float4 pixels on the
  * context's stream (or `stream` when non-NULL).  Same contract as the reference's

@@ -73,6 +73,8 @@ def lib() -> C.CDLL:
         L.or_morton3d.argtypes = [F, F, F]
         L.or_scene_order.argtypes = [C.c_void_p, U]
         L.or_max_threads.restype = C.c_int
+        L.or_ray_candidates.argtypes = [C.c_void_p, F, F, C.c_uint32, U, C.POINTER(C.c_uint64), U]
+        L.or_emission_sums.argtypes = [C.c_void_p, F, F, F, C.c_uint32, C.c_int64, D, D]
         _lib = L
     return _lib
 
@@ -118,6 +120,31 @@ class OracleScene:
         cnt = np.empty(n, np.uint32)
         lib().or_albedo_at(self.h, _p(p), n, _p(rgb), _p(cnt, U))
         return rgb.reshape(n, 3), cnt
+
+    def ray_candidates(self, origins, dirs):
+        """(ray index, caller's Gaussian index) pairs of every Gaussian whose padded 3-sigma box
+        each ray meets over [0, inf) (needs use_bvh=True for large scenes)."""
+        o, d = _f(origins).reshape(-1), _f(dirs).reshape(-1)
+        n = o.size // 3
+        counts = np.empty(n, np.uint32)
+        lib().or_ray_candidates(self.h, _p(o), _p(d), n, _p(counts, U), None, None)
+        offsets = np.zeros(n, np.uint64)
+        np.cumsum(counts[:-1], out=offsets[1:])
+        idx = np.empty(int(counts.sum()), np.uint32)
+        lib().or_ray_candidates(self.h, _p(o), _p(d), n, _p(counts, U), offsets.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                _p(idx, U))
+        return np.repeat(np.arange(n, dtype=np.int64), counts.astype(np.int64)), idx.astype(np.int64)
+
+    def emission_sums(self, emission, origins, dirs, exclude=-1):
+        """FP64 (S = sum tau, C = sum tau e) per ray over every Gaussian but the caller's index
+        `exclude` (the absorption-plus-emission model's ray sums)."""
+        o, d = _f(origins).reshape(-1), _f(dirs).reshape(-1)
+        e = _f(emission).reshape(-1)
+        n = o.size // 3
+        S = np.empty(n, np.float64)
+        Cs = np.empty(3 * n, np.float64)
+        lib().or_emission_sums(self.h, _p(e), _p(o), _p(d), n, int(exclude), _p(S, D), _p(Cs, D))
+        return S, Cs.reshape(n, 3)
 
     def transmittance_fp32(self, origins, dirs):
         o, d = _f(origins).reshape(-1), _f(dirs).reshape(-1)

@@ -1326,6 +1326,68 @@ double or_render(void* sv, void* ev, const float* cam16, const uint32_t* pu, con
   return omp_get_wtime() - t0;
 }
 
+// Candidate Gaussians of n rays over [0, inf): the caller's indices of every Gaussian whose padded
+// 3-sigma box the ray meets (CPU BVH; all Gaussians without one).  Two passes: with idx == NULL
+// it writes counts[n]; then, with offsets[n] = exclusive prefix sums of counts, it fills idx.
+void or_ray_candidates(void* sv, const float* o, const float* d, uint32_t n, uint32_t* counts,
+                       const uint64_t* offsets, uint32_t* idx) {
+  const Scene& S = *static_cast<Scene*>(sv);
+#pragma omp parallel
+  {
+    std::vector<uint32_t> cand;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+      cand.clear();
+      if (S.bvh.enabled) {
+        S.bvh.ray(mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]), cand);
+      } else {
+        cand.resize(S.prims.size());
+        std::iota(cand.begin(), cand.end(), 0u);
+      }
+      if (!idx) {
+        counts[i] = static_cast<uint32_t>(cand.size());
+      } else {
+        uint32_t* out = idx + offsets[i];
+        for (size_t k = 0; k < cand.size(); ++k) out[k] = S.orig[cand[k]];
+      }
+    }
+  }
+}
+
+// FP64 sums of the absorption-plus-emission model per ray: S = sum tau_i and C = sum tau_i e_i
+// (tau_i as tau64: the 3-sigma chord over [0, inf)), over every Gaussian except the caller's
+// index `exclude` (-1: none).  emission: [3 * count] in the caller's order; out_S[n], out_C[3n].
+void or_emission_sums(void* sv, const float* emission, const float* o, const float* d, uint32_t n, int64_t exclude,
+                      double* out_S, double* out_C) {
+  const Scene& S = *static_cast<Scene*>(sv);
+#pragma omp parallel
+  {
+    std::vector<uint32_t> cand, one(1);
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+      const double oo[3] = {o[3 * i], o[3 * i + 1], o[3 * i + 2]}, dd[3] = {d[3 * i], d[3 * i + 1], d[3 * i + 2]};
+      cand.clear();
+      if (S.bvh.enabled) {
+        S.bvh.ray(mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]), cand);
+      } else {
+        cand.resize(S.prims.size());
+        std::iota(cand.begin(), cand.end(), 0u);
+      }
+      double s = 0.0, c[3] = {0.0, 0.0, 0.0};
+      for (uint32_t k : cand) {
+        const uint32_t orig = S.orig[k];
+        if (static_cast<int64_t>(orig) == exclude) continue;
+        one[0] = k;
+        const double t = tau64(S, oo, dd, &one);
+        s += t;
+        for (int ch = 0; ch < 3; ++ch) c[ch] += t * emission[3ull * orig + ch];
+      }
+      out_S[i] = s;
+      for (int ch = 0; ch < 3; ++ch) out_C[3 * i + ch] = c[ch];
+    }
+  }
+}
+
 int or_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -78,8 +78,32 @@ def test_config_maps_to_c_params():
     assert p.batch_spp == 8 and p.measure == 1
 
 
-def test_struct_layouts_match_header():
-    # sizes of the C structs as the header lays them out (x86-64 System V)
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets that gcc gives the header's structs."""
+    structs = {"vp_gaussians": _capi.vp_gaussians, "vp_scene_info": _capi.vp_scene_info,
+               "vp_camera": _capi.vp_camera, "vp_render_params": _capi.vp_render_params,
+               "vp_render_stats": _capi.vp_render_stats, "vp_gaussian_grads": _capi.vp_gaussian_grads,
+               "vp_server_config": _capi.vp_server_config, "vp_request": _capi.vp_request,
+               "vp_server_stats": _capi.vp_server_stats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    cc = subprocess.run(["gcc", "-std=c11", "-I", "/usr/local/cuda/include", str(src), "-o", str(exe)],
+                        capture_output=True, text=True)
+    if cc.returncode != 0:
+        pytest.skip("no C compiler for the header: " + cc.stderr[:200])
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    for name, cls in structs.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(got[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
     assert C.sizeof(_capi.vp_gaussians) == 56
     assert C.sizeof(_capi.vp_camera) == 48
     assert C.sizeof(_capi.vp_render_params) == 64

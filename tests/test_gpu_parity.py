@@ -173,6 +173,41 @@ def test_engines_agree(vp_ctx):
     assert np.abs(imgs["warp"] - imgs["megakernel"]).mean() / scale < 1e-4
 
 
+def test_measurement_bits(vp_ctx):
+    """VP_MEASURE_STAGES and VP_MEASURE_COUNTERS leave the image bit-identical; the per-kind
+    counters add up to the totals; stage times and launch counts are consistent."""
+    g, cfg, env = small_scatter_workload(seed=6, spp=16)
+    cfg.batch_spp = 8
+    cam = scenes.negz_camera(3.0, 40.0)
+    sc = vp.Scene(vp_ctx, g, 2.0)
+    en = vp.Environment(vp_ctx, rgb=env)
+    out = {}
+    for name, kw in {"plain": {}, "stages": {"time_stages": True}, "counters": {"measure_caps": True},
+                     "both": {"time_stages": True, "measure_caps": True}}.items():
+        c = vp.Config(**{**cfg.__dict__, **kw})
+        im = vp.ProgressiveImage(vp_ctx, cfg.image_width, cfg.image_height)
+        st = im.accumulate(sc, en, cam, c, 0, cfg.num_samples_per_pixel)
+        out[name] = (im.read(), st)
+        im.close()
+    base = out["plain"][0]
+    for name in ("stages", "counters", "both"):
+        assert np.array_equal(out[name][0], base), name
+    st = out["both"][1]
+    assert st["device_status"] == 0
+    assert st["prim_tests"] == sum(st["query_prim_tests"]) > 0
+    assert st["geo_loads"] == sum(st["query_geo_loads"]) > 0
+    assert st["query_prim_tests"][1] > 0 and st["query_nodes"][1] > 0  # shadow rays traversed
+    # two batches: generate + welford and 5 launches per iteration each
+    it = st["stage_launches"][0]
+    assert st["stage_launches"][1] == it and it >= 2
+    assert st["launches"] == 2 * 2 + 5 * it == sum(st["stage_launches"])
+    assert 0.0 < st["ms_stage"][0] and 0.0 < st["ms_stage"][1]
+    assert sum(st["ms_stage"]) <= st["ms_kernels"] * 1.001 + 1e-3
+    assert out["plain"][1]["ms_stage"] == [0.0, 0.0, 0.0] and out["plain"][1]["launches"] == st["launches"]
+    en.close()
+    sc.close()
+
+
 def test_scatter_statistical_vs_reference_order(vp_ctx):
     """Seed stack: GPU (keyed draws, alias-table env sampling) vs the oracle with the reference's
     sequential free-flight draws and CDF env sampling."""
