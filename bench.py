@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-baseline-engine", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the differentiation and serving forms")
-    ap.add_argument("--serving-requests", type=int, default=64)
+    ap.add_argument("--serving-requests", type=int, default=128)
     return ap.parse_args()
 
 

@@ -41,6 +41,7 @@ constexpr float kInvSqrt2 = 1.0f / 1.41421356237309504880f;
 
 // Child-reference encoding of both BVHs.
 constexpr uint32_t kEmptyRef = 0xFFFFFFFFu;
+constexpr uint32_t kNoGauss = 0xFFFFFFFFu;  // no Gaussian (scene order)
 constexpr uint32_t kLeafBit = 0x80000000u;
 __host__ __device__ inline bool ref_is_leaf(uint32_t r) { return (r & kLeafBit) != 0u; }
 // BVH32 leaf: bit31 | (count-1) << 26 | first

@@ -51,7 +51,9 @@ struct WfBuffers {
   uint2* key2;                    // free-flight key of the next bounce
   uint32_t* meta;                 // bounce | shadow count << 16 | alive << 18
   float4* alb4;                   // albedo at the scatter point, scatter distance
-  float4 *so4, *sd4, *sw4;        // 3 transmittance queries per path: origin (+T in .w), dir, weight
+  uint32_t* sg;                   // the Gaussian of the scatter (scene order) or kNoGauss
+  float4 *so4, *sd4, *sw4;        // 3 transmittance queries per path: origin (+T in .w), dir (+ the
+                                  // seed Gaussian's bits in .w), weight
   float4* L4;                     // finished sample radiance
   uint32_t *qa, *qb, *qs;         // path queues (current / next) and shadow-query queue
   uint32_t* ctr;                  // [0] paths now, [1] paths next, [2] shadow queries, [3..4] work heads

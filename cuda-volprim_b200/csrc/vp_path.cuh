@@ -20,6 +20,10 @@ struct PathState {
 
 struct ShadowSet {  // transmittance queries of one bounce: rad += w[k] * T(o[k], d[k])
   float3 o[3], d[3], w[3];
+  // The Gaussian whose free flight put the query's origin there (the NEE rays start inside it),
+  // or kNoGauss: the transmittance query evaluates it first and stops at once when its chord
+  // alone reaches MAX_OPTICAL_DEPTH.
+  uint32_t seed[3];
   int n;
 };
 
@@ -43,9 +47,11 @@ __device__ __forceinline__ PathState start_path(const CameraView& C, const Param
 }
 
 // Returns true when the path continues (s.o / s.d then hold the next ray); the caller adds
-// sh.w[k] * T(sh.o[k], sh.d[k]) to s.rad for k < sh.n either way.
+// sh.w[k] * T(sh.o[k], sh.d[k]) to s.rad for k < sh.n either way.  scatter_gauss is the Gaussian
+// whose free flight gave tstar (kNoGauss if unknown).
 __device__ __forceinline__ bool shade_bounce(const EnvView& E, const ParamsView& P, PathState& s,
-                                             bool scattered, float tstar, float3 albedo, ShadowSet& sh) {
+                                             bool scattered, float tstar, float3 albedo, ShadowSet& sh,
+                                             uint32_t scatter_gauss = kNoGauss) {
   sh.n = 0;
   float3 pos = s.o, dir_next = s.d;
   if (scattered) {
@@ -57,6 +63,7 @@ __device__ __forceinline__ bool shade_bounce(const EnvView& E, const ParamsView&
     sh.o[0] = s.o;
     sh.d[0] = s.d;
     sh.w[0] = mul(s.thr, env_lookup(E, s.d));
+    sh.seed[0] = kNoGauss;
     sh.n = 1;
   }
   if (!scattered) {  // accumulate_escape_radiance (path_stages.cuh:368-386)
@@ -77,14 +84,14 @@ __device__ __forceinline__ bool shade_bounce(const EnvView& E, const ParamsView&
       const float ph_b = hg_eval(P, s.d, wb);
       const float w_b = mis_balance(pdf_b, ph_b);
       const float3 c_b = mul(mul(base, env_lookup(E, wb)), w_b * ph_b * __frcp_rn(pdf_b));
-      sh.o[sh.n] = pos, sh.d[sh.n] = wa, sh.w[sh.n] = c_a;
+      sh.o[sh.n] = pos, sh.d[sh.n] = wa, sh.w[sh.n] = c_a, sh.seed[sh.n] = scatter_gauss;
       ++sh.n;
-      sh.o[sh.n] = pos, sh.d[sh.n] = wb, sh.w[sh.n] = c_b;
+      sh.o[sh.n] = pos, sh.d[sh.n] = wb, sh.w[sh.n] = c_b, sh.seed[sh.n] = scatter_gauss;
       ++sh.n;
     } else if (P.nee_mode == VP_NEE_PHASE) {
       float pdf;
       const float3 wp = hg_sample(P, s.d, s.rng, pdf);
-      sh.o[sh.n] = pos, sh.d[sh.n] = wp, sh.w[sh.n] = mul(base, env_lookup(E, wp));
+      sh.o[sh.n] = pos, sh.d[sh.n] = wp, sh.w[sh.n] = mul(base, env_lookup(E, wp)), sh.seed[sh.n] = scatter_gauss;
       ++sh.n;
     } else {  // VP_NEE_RIS: product RIS over ris_k env-IS candidates, 1 shadow ray
       const float3 luma = f3(0.2126f, 0.7152f, 0.0722f);
@@ -109,6 +116,7 @@ __device__ __forceinline__ bool shade_bounce(const EnvView& E, const ParamsView&
         if (lum_y > 0.f) {
           const float W_ris = wsum * __frcp_rn((float)P.ris_k);
           sh.o[sh.n] = pos, sh.d[sh.n] = y_dir, sh.w[sh.n] = mul(mul(base, mul(y_env, __frcp_rn(lum_y))), W_ris);
+          sh.seed[sh.n] = scatter_gauss;
           ++sh.n;
         }
       }

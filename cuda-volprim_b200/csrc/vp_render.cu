@@ -63,10 +63,10 @@ __device__ float3 trace_path(const SceneView& S, const EnvView& E, const CameraV
       if (scattered) ps.scatters++;
     }
     ShadowSet sh;
-    alive = shade_bounce(E, P, s, scattered, tstar, albedo, sh);
+    alive = shade_bounce(E, P, s, scattered, tstar, albedo, sh, scattered ? sa.gauss : kNoGauss);
 #pragma unroll 1
     for (int k = 0; k < sh.n; ++k) {  // compute_transmittance_to_env (sampling.cuh:548-583)
-      s.rad = add(s.rad, mul(sh.w[k], q.transmittance(sh.o[k], sh.d[k])));
+      s.rad = add(s.rad, mul(sh.w[k], q.transmittance(sh.o[k], sh.d[k], sh.seed[k])));
       if (P.measure) ps.shadow++;
     }
   }
@@ -83,8 +83,8 @@ struct WarpQueries {
   __device__ float argmin(float3 o, float3 d, uint64_t key, ScatterAlbedo* sa) {
     return warp_ray_query<kAcc, kArgmin>(S, W, o, d, key, status, ws, measure, sa);
   }
-  __device__ float transmittance(float3 o, float3 d) {
-    const float tau = warp_ray_query<kAcc, kTau>(S, W, o, d, 0ull, status, ws, measure);
+  __device__ float transmittance(float3 o, float3 d, uint32_t seed = kNoGauss) {
+    const float tau = warp_ray_query<kAcc, kTau>(S, W, o, d, 0ull, status, ws, measure, nullptr, seed);
     return tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
   }
   __device__ float3 albedo(float3 x, uint32_t& overlap) {

@@ -3,21 +3,22 @@
 //
 // A pool of path slots runs the wavefront stages of the offline engine (vp_wavefront.cu) with
 // path regeneration: every iteration
-//   advance  (1 thread)          carry the survivors over; take min(free slots, unstarted paths)
-//                                new paths from the admitted range
-//   regen    (thread per path)   new paths: request lookup in the admission ring, camera ray,
-//                                PCG32 stream, first free-flight key -- appended to the queue
+//   advance  (1 block)           carry the survivors over; hand the free slots to the admitted
+//                                requests that still have unstarted paths (the schedule)
+//   regen    (thread per path)   new paths: owning request from the share prefix sums, camera
+//                                ray, PCG32 stream, first free-flight key -- appended to the queue
 //   extend   (warp per path)     free-flight argmin + scatter albedo on the path's own scene
 //   shade    (thread per path)   phase / NEE / roulette with the request's own controls
 //   shadow   (warp per query)    transmittance on the query's scene
 //   gather   (thread per path)   radiance += weight x T; a finished path adds its sample to its
 //                                request's pixel sum, counts itself done and frees its slot
 // so paths of different requests, scenes, resolutions and sample counts share every launch, and
-// a request admitted while others run starts as soon as slots free up.  The virtual path space is
-// the concatenation of the admitted requests' width*height*spp paths in admission order (pixel
-// major); a request's paths start in order.  Every per-path quantity comes from the request-table
-// entry the path carries, so a path computes exactly what the offline engine computes for the
-// same (scene, camera, params, pixel, sample).
+// a request admitted while others run starts as soon as free slots reach it.  How free slots are
+// shared among the requests with unstarted paths is the server's schedule (admission order by
+// default; equal shares; or fewest remaining first).  A request's paths start in pixel-major
+// order.  Every per-path quantity comes from the request-table entry the path
+// carries, so a path computes exactly what the offline engine computes for the same (scene,
+// camera, params, pixel, sample).
 //
 // The host side admits from a FIFO when a table entry is free and the request's accumulator fits
 // the memory budget, replays the iterations as one captured CUDA graph (two iterations: the path
@@ -40,35 +41,29 @@ namespace {
 constexpr uint32_t kAlive = 1u << 18;
 constexpr int kSrvHitCap = 64;        // extend hit buffer, as the offline wavefront's
 constexpr uint32_t kMaxScenes = 64;
-// Admission-ring entries per request-table entry.  The device's lookup window can trail the host
-// by the requests admitted since the last iteration plus those still unstarted, at most two table
-// capacities; the ring is larger, so the host never overwrites an entry the window still holds.
-constexpr uint32_t kRingPerEntry = 4;
+constexpr uint32_t kMaxRequests = 1024;  // the share computation is one block
 
-struct SrvRequest {  // device request-table entry
+struct SrvRequest {  // device request-table entry (all zero while unused)
   CameraView cam;
   ParamsView P;
   uint32_t scene;    // resident (scene, env) pair
   uint32_t n_pix;
-  unsigned long long base, n_paths;  // virtual path range
+  unsigned long long n_paths;  // width * height * spp
+  unsigned long long seq;      // admission order
   float4* sum;       // per-pixel radiance sums
 };
 
 struct SrvCtl {  // device control block of the iteration
-  unsigned long long cursor;     // next virtual path to start
-  unsigned long long admit_end;  // end of the admitted virtual range (host-written)
-  unsigned long long regen_v0;   // first virtual path started by the current iteration
-  uint32_t free_count;           // free path slots (top of the free stack)
-  uint32_t regen_m;              // paths started by the current iteration
-  uint32_t regen_from;           // free-stack index of the first slot they take
-  uint32_t survivors;            // paths carried over from the previous iteration
-  uint32_t ring_lo;              // first admitted request whose paths are not all started
-  uint32_t ring_hi;              // admitted requests (host-written)
-  uint32_t ctr[8];               // [0] paths this iteration, [1] next, [2] shadow queries, [3..4] work heads
+  uint32_t free_count;  // free path slots (top of the free stack)
+  uint32_t regen_m;     // paths started by the current iteration
+  uint32_t regen_from;  // free-stack index of the first slot they take
+  uint32_t survivors;   // paths carried over from the previous iteration
+  uint32_t ctr[8];      // [0] paths this iteration, [1] next, [2] shadow queries, [3..4] work heads
 };
 
 struct SrvPaths {  // per path slot
   float4 *o4, *d4, *thr4, *rad4, *alb4;
+  uint32_t* sg;  // the Gaussian of the scatter (scene order) or kNoGauss
   uint4* rng4;
   uint2* key2;
   uint32_t* meta;  // bounce | shadow count << 16 | alive << 18
@@ -125,45 +120,124 @@ __global__ void k_srv_init(SrvCtl* c, uint32_t* free_stack, uint32_t slots) {
   if (i < slots) free_stack[i] = slots - 1u - i;  // pops take the lowest slots first
 }
 
-__global__ void k_srv_advance(SrvCtl* c, const unsigned long long* __restrict__ ring_base,
-                              const unsigned long long* __restrict__ ring_n, uint32_t ring_cap) {
-  const uint32_t surv = c->ctr[1];
-  const unsigned long long avail = c->admit_end - c->cursor;
-  const uint32_t m = (uint32_t)min((unsigned long long)c->free_count, avail);
-  c->survivors = surv;
-  c->regen_m = m;
-  c->regen_from = c->free_count - m;
-  c->regen_v0 = c->cursor;
-  c->free_count -= m;
-  c->cursor += m;
-  c->ctr[0] = surv + m;
-  c->ctr[1] = c->ctr[2] = c->ctr[3] = c->ctr[4] = 0u;
-  // admitted requests whose paths all started before this iteration leave the lookup window
-  uint32_t lo = c->ring_lo;
-  const uint32_t hi = c->ring_hi;
-  while (lo + 1u < hi && ring_base[lo % ring_cap] + ring_n[lo % ring_cap] <= c->regen_v0) ++lo;
-  c->ring_lo = lo;
+// Exclusive block-wide prefix sum (blockDim.x <= 1024); also returns the total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t x = lane < nw ? warp_tot[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane < nw) warp_tot[lane] = x;  // inclusive over warps
+  }
+  __syncthreads();
+  total = warp_tot[nw - 1];
+  const uint32_t before = w ? warp_tot[w - 1] : 0u;
+  __syncthreads();
+  return before + incl - v;
+}
+
+// One block of max_requests threads, thread e = request-table entry e, shares the free slots
+// among the requests with unstarted paths by the server's schedule:
+//   VP_SCHEDULE_FIFO  in admission order, each request taking all it still has;
+//   VP_SCHEDULE_FAIR  an equal quota ceil(free / k) to each of the k requests (capped at what each
+//                     still has), then what is left over in table order;
+//   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order).
+// Writes the per-entry offsets of this iteration's new paths (alloc_off, size R + 1) and their
+// first pixel-major path index (alloc_start).
+__global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, unsigned long long* __restrict__ started,
+                              uint32_t* __restrict__ alloc_off, unsigned long long* __restrict__ alloc_start,
+                              int schedule) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t s_free, s_surv;
+  __shared__ unsigned long long s_key[kMaxRequests], s_seq[kMaxRequests];
+  __shared__ uint32_t s_by_rank[kMaxRequests];
+  const uint32_t e = threadIdx.x, R = blockDim.x;
+  if (e == 0) {
+    s_free = c->free_count;
+    s_surv = c->ctr[1];
+  }
+  __syncthreads();
+  const uint32_t F = s_free;
+  const unsigned long long st0 = started[e];
+  const unsigned long long rem64 = table[e].n_paths - st0;
+  const uint32_t rem = (uint32_t)min(rem64, (unsigned long long)F);
+  uint32_t a = 0;
+  if (schedule == VP_SCHEDULE_FAIR) {
+    uint32_t k = 0;
+    (void)block_exclusive_scan(rem ? 1u : 0u, warp_tot, k);
+    const uint32_t q = k ? (F + k - 1u) / k : 0u;
+    uint32_t tot1 = 0;
+    uint32_t a1 = min(rem, q);
+    const uint32_t off1 = block_exclusive_scan(a1, warp_tot, tot1);
+    a1 = off1 >= F ? 0u : min(a1, F - off1);
+    const uint32_t F2 = tot1 >= F ? 0u : F - tot1;
+    uint32_t tot2 = 0;
+    const uint32_t r2 = rem - a1;
+    const uint32_t off2 = block_exclusive_scan(r2, warp_tot, tot2);
+    a = a1 + (off2 >= F2 ? 0u : min(r2, F2 - off2));
+  } else {
+    // rank every entry by its key, then hand out the free slots in rank order
+    const unsigned long long seq = table[e].seq;
+    const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? rem64 : seq);
+    s_key[e] = key;
+    s_seq[e] = seq;
+    __syncthreads();
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < R; ++j) {
+      const unsigned long long kj = s_key[j], sj = s_seq[j];
+      rank += (kj < key || (kj == key && (sj < seq || (sj == seq && j < e)))) ? 1u : 0u;
+    }
+    s_by_rank[rank] = rem;
+    __syncthreads();
+    uint32_t tot = 0;
+    const uint32_t before = block_exclusive_scan(s_by_rank[e], warp_tot, tot);  // thread e = rank e here
+    __syncthreads();
+    s_by_rank[e] = before;  // offset of rank e
+    __syncthreads();
+    const uint32_t off = s_by_rank[rank];
+    a = off >= F ? 0u : min(rem, F - off);
+  }
+  uint32_t m = 0;
+  const uint32_t off = block_exclusive_scan(a, warp_tot, m);
+  alloc_off[e] = off;
+  alloc_start[e] = st0;
+  started[e] = st0 + a;
+  if (e == R - 1) alloc_off[R] = m;
+  if (e == 0) {
+    c->survivors = s_surv;
+    c->regen_m = m;
+    c->regen_from = F - m;
+    c->free_count = F - m;
+    c->ctr[0] = s_surv + m;
+    c->ctr[1] = c->ctr[2] = c->ctr[3] = c->ctr[4] = 0u;
+  }
 }
 
 __global__ void k_srv_regen(const SrvCtl* __restrict__ c, const SrvRequest* __restrict__ table,
-                            const unsigned long long* __restrict__ ring_base, const uint32_t* __restrict__ ring_slot,
-                            uint32_t ring_cap, SrvPaths b, uint32_t* __restrict__ q) {
+                            const uint32_t* __restrict__ alloc_off, const unsigned long long* __restrict__ alloc_start,
+                            uint32_t n_entries, SrvPaths b, uint32_t* __restrict__ q) {
   const uint32_t m = c->regen_m;
   const uint32_t from = c->regen_from, surv = c->survivors;
-  const unsigned long long v0 = c->regen_v0;
-  const uint32_t lo0 = c->ring_lo, hi0 = c->ring_hi;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     const uint32_t slot = b.free_stack[from + i];
-    const unsigned long long v = v0 + i;
-    uint32_t lo = lo0, hi = hi0;  // last admitted request with base <= v
+    uint32_t lo = 0, hi = n_entries;  // the entry e with alloc_off[e] <= i < alloc_off[e + 1]
     while (hi - lo > 1u) {
       const uint32_t mid = lo + (hi - lo) / 2u;
-      if (ring_base[mid % ring_cap] <= v) lo = mid;
+      if (alloc_off[mid] <= i) lo = mid;
       else hi = mid;
     }
-    const uint32_t e = ring_slot[lo % ring_cap];
+    const uint32_t e = lo;
     const SrvRequest& r = table[e];
-    const unsigned long long local = v - r.base;
+    const unsigned long long local = alloc_start[e] + (i - alloc_off[e]);
     const uint32_t spp = r.P.spp_total;
     const uint32_t pix = (uint32_t)(local / spp), s = (uint32_t)(local % spp);
     PathState st = start_path(r.cam, r.P, pix % r.P.width, pix / r.P.width, s);
@@ -209,7 +283,10 @@ __global__ void __launch_bounds__(256, 4) k_srv_extend(const SceneView* __restri
       uint32_t ov = sa.overlap;
       albedo = sa.valid ? sa.albedo : warp_albedo<kAcc>(S, W, fma3(tstar, df, of), ov, status, ws, false);
     }
-    if (lane == 0) b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+    if (lane == 0) {
+      b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+      b.sg[p] = tstar < kInf ? sa.gauss : kNoGauss;
+    }
     if (status) break;
   }
   if (lane == 0 && status) atomicOr(&ctr->status, status);
@@ -234,11 +311,11 @@ __global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ e
       PathState s = srv_load(b, p, b.meta[p] & 0xFFFFu);
       const float4 a = b.alb4[p];
       ShadowSet sh;
-      alive = shade_bounce(envs[r.scene], r.P, s, a.w < kInf, a.w, f3(a.x, a.y, a.z), sh);
+      alive = shade_bounce(envs[r.scene], r.P, s, a.w < kInf, a.w, f3(a.x, a.y, a.z), sh, b.sg[p]);
       ns = sh.n;
       for (int k = 0; k < sh.n; ++k) {
         b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, 1.f);
-        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, 0.f);
+        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k]));
         b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
       }
       if (alive) {
@@ -273,7 +350,8 @@ __global__ void __launch_bounds__(256, 4) k_srv_shadow(const SceneView* __restri
     const uint32_t qslot = __ldg(b.qs + item);
     const SceneView S = scenes[table[b.req[qslot / 3u]].scene];
     const float4 o = b.so4[qslot], d = b.sd4[qslot];
-    const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws, false);
+    const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws, false,
+                                                 nullptr, __float_as_uint(d.w));
     if (lane == 0) b.so4[qslot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
     if (status) break;
   }
@@ -327,7 +405,7 @@ void srv_carve(char*& cur, T*& out, size_t count) {
   cur += (count * sizeof(T) + 255) & ~size_t(255);
 }
 
-constexpr size_t kSlotBytes = 5 * 16 + 16 + 8 + 4 + 4 + 4 + 3 * 48 + 4 * 2 + 3 * 4 + 4;
+constexpr size_t kSlotBytes = 5 * 16 + 4 + 16 + 8 + 4 + 4 + 4 + 3 * 48 + 4 * 2 + 3 * 4 + 4;
 
 }  // namespace
 }  // namespace vp
@@ -341,24 +419,20 @@ struct vp_server {
   std::vector<vp_scene*> scenes;
   std::vector<vp_env*> envs;
   uint32_t max_cap = 0;
-  uint32_t ring_cap = 0;
   // device
   SceneView* d_scenes = nullptr;
   EnvView* d_envs = nullptr;
   SrvRequest* d_table = nullptr;
   unsigned long long* d_done = nullptr;
-  unsigned long long *d_ring_base = nullptr, *d_ring_n = nullptr;
-  uint32_t* d_ring_slot = nullptr;
+  unsigned long long* d_started = nullptr;      // paths started per table entry
+  uint32_t* d_alloc_off = nullptr;              // this iteration's new paths per entry (prefix, R + 1)
+  unsigned long long* d_alloc_start = nullptr;  // their first path index per entry
   SrvCtl* d_ctl = nullptr;
   void* path_mem = nullptr;
   SrvPaths paths{};
   // pinned staging (written only while the stream is idle)
   SrvRequest* h_table = nullptr;
   unsigned long long* h_done = nullptr;
-  unsigned long long *h_ring_base = nullptr, *h_ring_n = nullptr;
-  uint32_t* h_ring_slot = nullptr;
-  unsigned long long* h_admit_end = nullptr;
-  uint32_t* h_ring_hi = nullptr;
   // graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -384,8 +458,7 @@ struct vp_server {
   std::deque<Pending> pending;
   std::vector<uint64_t> done_ids;
   uint64_t next_id = 0, admitted = 0, completed = 0, paths_completed = 0, iterations = 0;
-  unsigned long long admit_end = 0;
-  uint32_t ring_hi = 0, n_active = 0;
+  uint32_t n_active = 0;
   size_t bytes_fixed = 0, bytes_active = 0;
   double device_ms = 0.0;
 };
@@ -411,18 +484,13 @@ void srv_free(vp_server* s) {
   cudaFree(s->d_envs);
   cudaFree(s->d_table);
   cudaFree(s->d_done);
-  cudaFree(s->d_ring_base);
-  cudaFree(s->d_ring_n);
-  cudaFree(s->d_ring_slot);
+  cudaFree(s->d_started);
+  cudaFree(s->d_alloc_off);
+  cudaFree(s->d_alloc_start);
   cudaFree(s->d_ctl);
   cudaFree(s->path_mem);
   cudaFreeHost(s->h_table);
   cudaFreeHost(s->h_done);
-  cudaFreeHost(s->h_ring_base);
-  cudaFreeHost(s->h_ring_n);
-  cudaFreeHost(s->h_ring_slot);
-  cudaFreeHost(s->h_admit_end);
-  cudaFreeHost(s->h_ring_hi);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   delete s;
@@ -431,12 +499,13 @@ void srv_free(vp_server* s) {
 // One wavefront iteration with the queues in the given roles.
 vp_status enqueue_iteration(vp_server* s, bool even) {
   cudaStream_t st = s->ctx->stream;
-  const uint32_t R = s->ring_cap;
+  const uint32_t R = s->cfg.max_requests;
   uint32_t* qcur = even ? s->paths.qa : s->paths.qb;
   uint32_t* qnext = even ? s->paths.qb : s->paths.qa;
   Counters* ctr = s->ctx->counters;
-  k_srv_advance<<<1, 1, 0, st>>>(s->d_ctl, s->d_ring_base, s->d_ring_n, R);
-  k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_ring_base, s->d_ring_slot, R, s->paths, qcur);
+  k_srv_advance<<<1, R, 0, st>>>(s->d_ctl, s->d_table, s->d_started, s->d_alloc_off, s->d_alloc_start,
+                                 s->cfg.schedule);
+  k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_alloc_off, s->d_alloc_start, R, s->paths, qcur);
   if (s->accurate)
     k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
                                                                s->max_cap, ctr);
@@ -493,8 +562,6 @@ vp_status prepare_launch(vp_server* s) {
 
 vp_status admit(vp_server* s) {
   cudaStream_t st = s->ctx->stream;
-  const uint32_t R = s->ring_cap;
-  bool any = false;
   while (!s->pending.empty() && s->n_active < s->cfg.max_requests) {
     const vp_request& rq = s->pending.front().r;
     const size_t need = request_bytes(rq);
@@ -507,6 +574,7 @@ vp_status admit(vp_server* s) {
     VP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sum), 16ull * n_pix, st));
     VP_CUDA(cudaMemsetAsync(sum, 0, 16ull * n_pix, st));
     VP_CUDA(cudaMemsetAsync(s->d_done + e, 0, sizeof(unsigned long long), st));
+    VP_CUDA(cudaMemsetAsync(s->d_started + e, 0, sizeof(unsigned long long), st));
     SrvRequest& t = s->h_table[e];
     std::memset(&t, 0, sizeof(t));
     build_camera(rq.camera, rq.params.width, rq.params.height, t.cam);
@@ -515,17 +583,10 @@ vp_status admit(vp_server* s) {
     t.P.measure = 0;
     t.scene = rq.scene_id;
     t.n_pix = n_pix;
-    t.base = s->admit_end;
     t.n_paths = (unsigned long long)n_pix * rq.params.spp;
+    t.seq = s->admitted;
     t.sum = sum;
     VP_CUDA(cudaMemcpyAsync(s->d_table + e, &t, sizeof(t), cudaMemcpyHostToDevice, st));
-    const uint32_t j = s->ring_hi % R;
-    s->h_ring_base[j] = t.base;
-    s->h_ring_n[j] = t.n_paths;
-    s->h_ring_slot[j] = e;
-    VP_CUDA(cudaMemcpyAsync(s->d_ring_base + j, s->h_ring_base + j, 8, cudaMemcpyHostToDevice, st));
-    VP_CUDA(cudaMemcpyAsync(s->d_ring_n + j, s->h_ring_n + j, 8, cudaMemcpyHostToDevice, st));
-    VP_CUDA(cudaMemcpyAsync(s->d_ring_slot + j, s->h_ring_slot + j, 4, cudaMemcpyHostToDevice, st));
     a.used = true;
     a.id = s->pending.front().id;
     a.n_paths = t.n_paths;
@@ -536,18 +597,9 @@ vp_status admit(vp_server* s) {
     a.sum = sum;
     a.bytes = need;
     s->bytes_active += need;
-    s->admit_end += t.n_paths;
-    s->ring_hi += 1;
     s->n_active += 1;
     s->admitted += 1;
     s->pending.pop_front();
-    any = true;
-  }
-  if (any) {
-    *s->h_admit_end = s->admit_end;
-    *s->h_ring_hi = s->ring_hi;
-    VP_CUDA(cudaMemcpyAsync(&s->d_ctl->admit_end, s->h_admit_end, 8, cudaMemcpyHostToDevice, st));
-    VP_CUDA(cudaMemcpyAsync(&s->d_ctl->ring_hi, s->h_ring_hi, 4, cudaMemcpyHostToDevice, st));
   }
   return VP_OK;
 }
@@ -601,6 +653,11 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   vp_server_config& c = s->cfg;
   if (c.path_slots == 0) c.path_slots = 1u << 21;
   if (c.max_requests == 0) c.max_requests = 256;
+  c.max_requests = (c.max_requests + 31u) & ~31u;  // the share computation runs one block of warps
+  if (c.max_requests > kMaxRequests) {
+    srv_free(s);
+    return fail(VP_ERROR_LIMIT, "max_requests above 1024");
+  }
   if (c.iterations_per_step == 0) c.iterations_per_step = 4;
   c.iterations_per_step = (c.iterations_per_step + 1u) & ~1u;
   if (c.path_slots > (1u << 28)) {
@@ -608,9 +665,11 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
     return fail(VP_ERROR_LIMIT, "path_slots above 2^28");
   }
   s->accurate = c.precision == VP_PRECISION_ACCURATE;
+  if (c.schedule < VP_SCHEDULE_FIFO || c.schedule > VP_SCHEDULE_SRPT) {
+    srv_free(s);
+    return fail(VP_ERROR_INVALID_ARGUMENT, "unknown schedule");
+  }
   const uint32_t R = c.max_requests, P = c.path_slots;
-  s->ring_cap = kRingPerEntry * R + 2u;
-  const uint32_t RC = s->ring_cap;
   s->active.resize(R);
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) {
@@ -620,17 +679,12 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   chk(cudaMalloc(&s->d_envs, kMaxScenes * sizeof(EnvView)));
   chk(cudaMalloc(&s->d_table, R * sizeof(SrvRequest)));
   chk(cudaMalloc(&s->d_done, R * sizeof(unsigned long long)));
-  chk(cudaMalloc(&s->d_ring_base, RC * 8ull));
-  chk(cudaMalloc(&s->d_ring_n, RC * 8ull));
-  chk(cudaMalloc(&s->d_ring_slot, RC * 4ull));
+  chk(cudaMalloc(&s->d_started, R * 8ull));
+  chk(cudaMalloc(&s->d_alloc_off, (R + 1ull) * 4ull));
+  chk(cudaMalloc(&s->d_alloc_start, R * 8ull));
   chk(cudaMalloc(&s->d_ctl, sizeof(SrvCtl)));
   chk(cudaMallocHost(&s->h_table, R * sizeof(SrvRequest)));
   chk(cudaMallocHost(&s->h_done, R * sizeof(unsigned long long)));
-  chk(cudaMallocHost(&s->h_ring_base, RC * 8ull));
-  chk(cudaMallocHost(&s->h_ring_n, RC * 8ull));
-  chk(cudaMallocHost(&s->h_ring_slot, RC * 4ull));
-  chk(cudaMallocHost(&s->h_admit_end, 8));
-  chk(cudaMallocHost(&s->h_ring_hi, 4));
   chk(cudaEventCreate(&s->ev0));
   chk(cudaEventCreate(&s->ev1));
   const size_t slot_bytes = (size_t)P * kSlotBytes + 32 * 256;
@@ -646,6 +700,7 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   srv_carve(cur, b.thr4, P);
   srv_carve(cur, b.rad4, P);
   srv_carve(cur, b.alb4, P);
+  srv_carve(cur, b.sg, P);
   srv_carve(cur, b.rng4, P);
   srv_carve(cur, b.key2, P);
   srv_carve(cur, b.meta, P);
@@ -658,11 +713,13 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   srv_carve(cur, b.qb, P);
   srv_carve(cur, b.qs, 3ull * P);
   srv_carve(cur, b.free_stack, P);
-  s->bytes_fixed = slot_bytes + R * (sizeof(SrvRequest) + 8ull) + RC * 20ull;
+  s->bytes_fixed = slot_bytes + R * (sizeof(SrvRequest) + 28ull);
   cudaStream_t st = ctx->stream;
   k_srv_init<<<(P + 255) / 256, 256, 0, st>>>(s->d_ctl, b.free_stack, P);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, R * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_started, 0, R * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_table, 0, R * sizeof(SrvRequest), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     srv_free(s);

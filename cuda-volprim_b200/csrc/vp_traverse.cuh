@@ -42,19 +42,18 @@ __device__ __forceinline__ bool box_contains(float4 lo, float4 hi, float3 p) {
 // ------------------------------------------------------------------------------------------
 // warp engine
 // ------------------------------------------------------------------------------------------
-// Per-warp shared memory: the traversal stack and the hit buffer.  A query that keeps no chords
-// (transmittance, point) needs 32 hit-buffer entries; the argmin that retains chords for the
-// scatter-point albedo uses more.
+// Per-warp shared memory: the traversal stack and the hit buffer of the chords the argmin retains
+// for the scatter-point albedo (the transmittance and point queries keep none).
 struct WarpSmem {
   uint32_t* st_ref;
   float* st_t;
   uint32_t* hb_idx;
-  float *hb_tc, *hb_rw, *hb_d2, *hb_h, *hb_u0, *hb_tin, *hb_tout, *hb_icf;
+  float *hb_tc, *hb_rw, *hb_d2, *hb_tin, *hb_tout, *hb_icf;
   int hit_cap;
 };
 
 __host__ __device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap, int hit_cap) {
-  return (size_t)stack_cap * 8u + (size_t)hit_cap * 9u * 4u;
+  return (size_t)stack_cap * 8u + (size_t)hit_cap * 7u * 4u;
 }
 
 __device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_cap, int hit_cap) {
@@ -66,11 +65,9 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_ca
   w.hb_tc = hb + 1 * hit_cap;
   w.hb_rw = hb + 2 * hit_cap;
   w.hb_d2 = hb + 3 * hit_cap;
-  w.hb_h = hb + 4 * hit_cap;
-  w.hb_u0 = hb + 5 * hit_cap;
-  w.hb_tin = hb + 6 * hit_cap;
-  w.hb_tout = hb + 7 * hit_cap;
-  w.hb_icf = hb + 8 * hit_cap;
+  w.hb_tin = hb + 4 * hit_cap;
+  w.hb_tout = hb + 5 * hit_cap;
+  w.hb_icf = hb + 6 * hit_cap;
   w.hit_cap = hit_cap;
   return w;
 }
@@ -84,10 +81,12 @@ struct WarpStats {
   unsigned int max_hits = 0;
 };
 
-// Albedo at the scatter point, when the argmin query could derive it from its own chords.
+// Albedo at the scatter point, when the argmin query could derive it from its own chords, and
+// the Gaussian whose free flight was the minimum (scene order; kNoGauss on escape).
 struct ScatterAlbedo {
   float3 albedo;
   uint32_t overlap;
+  uint32_t gauss;
   bool valid;
 };
 
@@ -95,23 +94,40 @@ struct ScatterAlbedo {
 // every Gaussian whose chord overlaps [0, t) (kInf = escape); kTau returns the optical depth
 // over [0, inf), stopping once it reaches MAX_OPTICAL_DEPTH.
 //
-// With `sa` (kArgmin only) the processed chords with t_in <= t stay in the hit buffer, and after
+// With `sa` (kArgmin only) the overlapping chords with t_in <= t stay in the hit buffer, and after
 // the traversal the albedo at the scatter distance t* is the sigma_t * pdf-weighted mean over
 // the chords containing t* -- the reference's rebuilt active set (sampling.cuh:422-458) and
 // evaluate_albedo (:257-283), with the whitened radius from the chord frame,
 // |y|^2 = d2 + ((t* - t_c)|w|)^2.  Every Gaussian containing the scatter point was processed (its
 // chord starts before t* <= t), so the set is complete; if the retained chords outgrow the
 // buffer, sa->valid stays false and the caller runs the point query instead.
+//
+// A kTau query whose origin lies inside a known Gaussian (`seed`, the one whose free flight put
+// the path there) evaluates that chord first: in a dense medium it alone usually reaches
+// MAX_OPTICAL_DEPTH and the traversal is skipped; otherwise the traversal skips it at its leaf.
 template <bool kAcc, int kKind>
 __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o, float3 d,
                                 uint64_t key, uint32_t& status, WarpStats& ws, bool measure,
-                                ScatterAlbedo* sa = nullptr) {
+                                ScatterAlbedo* sa = nullptr, uint32_t seed = kNoGauss) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const float3 inv = safe_inv(d);
   float t_hi = kInf;
   float acc = 0.0f;
-  int sp = 0, hb = 0, kept = 0;  // [0, kept) processed and retained, [kept, hb) pending
+  uint32_t arg = kNoGauss;  // kArgmin: the Gaussian of the current minimum
+  if (kKind == kTau && seed != kNoGauss) {
+    float v = 0.0f;
+    if (lane == 0) {
+      const PrimGeo g = load_geo(S.prims, seed);
+      Chord ch;
+      if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f)
+        v = chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, g.icf);
+    }
+    acc = __shfl_sync(kFull, v, 0);
+    if (measure) ws.crossings += 1;
+    if (acc >= kMaxOpticalDepth) return acc;
+  }
+  int sp = 0, hb = 0, kept = 0;  // retained chords [0, kept); hb == kept between leaves
   bool keep = (kKind == kArgmin) && sa != nullptr;
   unsigned int hits_seen = 0;
   // The node to visit next is kept in registers (the nearest hit child of the last inner node);
@@ -127,42 +143,24 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       const int e = base + lane;
       const bool keepit = e < kept && W.hb_tin[e] <= t_hi;
       uint32_t idx = 0;
-      float f[8];
+      float f[6];
       if (keepit) {
         idx = W.hb_idx[e];
-        f[0] = W.hb_tc[e], f[1] = W.hb_rw[e], f[2] = W.hb_d2[e], f[3] = W.hb_h[e];
-        f[4] = W.hb_u0[e], f[5] = W.hb_tin[e], f[6] = W.hb_tout[e], f[7] = W.hb_icf[e];
+        f[0] = W.hb_tc[e], f[1] = W.hb_rw[e], f[2] = W.hb_d2[e];
+        f[3] = W.hb_tin[e], f[4] = W.hb_tout[e], f[5] = W.hb_icf[e];
       }
       const unsigned m = __ballot_sync(kFull, keepit);
       __syncwarp();
       if (keepit) {
         const int p = w + __popc(m & lt_mask);
         W.hb_idx[p] = idx;
-        W.hb_tc[p] = f[0], W.hb_rw[p] = f[1], W.hb_d2[p] = f[2], W.hb_h[p] = f[3];
-        W.hb_u0[p] = f[4], W.hb_tin[p] = f[5], W.hb_tout[p] = f[6], W.hb_icf[p] = f[7];
+        W.hb_tc[p] = f[0], W.hb_rw[p] = f[1], W.hb_d2[p] = f[2];
+        W.hb_tin[p] = f[3], W.hb_tout[p] = f[4], W.hb_icf[p] = f[5];
       }
       w += __popc(m);
       __syncwarp();
     }
     kept = hb = w;
-  };
-
-  auto process = [&](int base, int cnt) {
-    float v = (kKind == kArgmin) ? kInf : 0.0f;
-    if (lane < cnt) {
-      const int e = base + lane;
-      const float tc = W.hb_tc[e], rw = W.hb_rw[e], d2 = W.hb_d2[e], h = W.hb_h[e], u0 = W.hb_u0[e];
-      const float tin = W.hb_tin[e], tout = W.hb_tout[e], icf = W.hb_icf[e];
-      if (kKind == kArgmin) {
-        const uint32_t orig = __ldg(S.perm + W.hb_idx[e]);
-        v = chord_free_flight<kAcc>(tc, rw, d2, h, u0, tin, tout, icf, free_flight_tau<kAcc>(key, orig));
-      } else {
-        v = chord_tau<kAcc>(tc, rw, d2, h, u0, fmaxf(tin, 0.0f), tout, icf);
-      }
-    }
-    if (kKind == kArgmin) t_hi = fminf(t_hi, warp_min(v));
-    else acc += warp_sum(v);
-    if (measure) ws.crossings += (unsigned)cnt;
   };
 
   while (true) {
@@ -187,7 +185,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       float icf = 0.f;
       const uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
       bool boxed = false;
-      if (lane < total) {  // the Gaussian's own 3-sigma box first (32 B), then its record
+      if (lane < total && pi != seed) {  // the Gaussian's own 3-sigma box first (32 B), then its record
         float tb;
         boxed = slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, t_hi, tb);
       }
@@ -200,36 +198,65 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       }
       if (measure) ws.kind_geo[kKind] += __popc(__ballot_sync(kFull, boxed));
       const unsigned m = __ballot_sync(kFull, hit);
-      if (keep && m != 0u && hb + 32 > W.hit_cap) {  // make room for up to 32 new chords
-        compact();
-        if (hb + 32 > W.hit_cap) {  // still full: stop retaining, the caller will query the point
-          keep = false;
-          kept = hb = 0;
+      if constexpr (kKind == kTau) {
+        // Transmittance keeps no chords: each lane evaluates its own and the warp sums them
+        // (no hit-buffer round trip through shared memory).
+        if (m != 0u) {
+          const float v = hit ? chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f),
+                                                ch.t_out, icf)
+                              : 0.0f;
+          acc += warp_sum(v);
+          hits_seen += __popc(m);
+          if (measure) ws.crossings += (unsigned)__popc(m);
+          if (acc >= kMaxOpticalDepth) break;
         }
+        continue;
       }
-      if (hit) {
-        const int pos = hb + __popc(m & lt_mask);
-        W.hb_idx[pos] = pi;
-        W.hb_tc[pos] = ch.tc;
-        W.hb_rw[pos] = ch.rw;
-        W.hb_d2[pos] = ch.d2;
-        W.hb_h[pos] = ch.h;
-        W.hb_u0[pos] = chord_u0(ch, 0.0f);
-        W.hb_tin[pos] = ch.t_in;
-        W.hb_tout[pos] = ch.t_out;
-        W.hb_icf[pos] = icf;
-      }
-      hb += __popc(m);
-      hits_seen += __popc(m);
-      __syncwarp();
-      // Evaluate the new chords after every leaf that produced any: the argmin bound t_hi and
-      // the shadow ray's optical depth must be current for pruning and early exit.
-      if (hb > kept) {
-        process(kept, hb - kept);
-        if (keep) kept = hb;
-        else hb = kept;
-        __syncwarp();
-        if (kKind == kTau && acc >= kMaxOpticalDepth) break;
+      // The argmin: each lane evaluates its own chord's free flight and the warp takes the
+      // minimum (the argmin does not depend on the order of the chords); the chords that can
+      // still contain the scatter point (t_in <= t_hi) are retained for its albedo.
+      if (m != 0u) {
+        float v = kInf;
+        if (hit) {
+          const uint32_t orig = __ldg(S.perm + pi);
+          v = chord_free_flight<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), ch.t_in, ch.t_out, icf,
+                                      free_flight_tau<kAcc>(key, orig));
+        }
+        const float mn = warp_min(v);
+        if (mn < t_hi) {
+          const unsigned wm = __ballot_sync(kFull, v == mn);
+          arg = __shfl_sync(kFull, pi, __ffs(wm) - 1);
+          t_hi = mn;
+        }
+        hits_seen += __popc(m);
+        if (measure) ws.crossings += (unsigned)__popc(m);
+        if (keep) {
+          const bool ret = hit && ch.t_in <= t_hi;
+          const unsigned rm = __ballot_sync(kFull, ret);
+          const int nr = __popc(rm);
+          if (nr != 0 && hb + nr > W.hit_cap) {  // make room: drop chords that start beyond t_hi
+            compact();
+            if (hb + nr > W.hit_cap) {  // still full: stop retaining, the caller will query the point
+              keep = false;
+              kept = hb = 0;
+            }
+          }
+          if (keep) {
+            if (ret) {
+              const int pos = hb + __popc(rm & lt_mask);
+              W.hb_idx[pos] = pi;
+              W.hb_tc[pos] = ch.tc;
+              W.hb_rw[pos] = ch.rw;
+              W.hb_d2[pos] = ch.d2;
+              W.hb_tin[pos] = ch.t_in;
+              W.hb_tout[pos] = ch.t_out;
+              W.hb_icf[pos] = icf;
+            }
+            hb += nr;
+            kept = hb;
+          }
+          __syncwarp();
+        }
       }
     } else {
       if (measure) {
@@ -274,6 +301,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   if constexpr (kKind == kArgmin) {
     if (sa != nullptr) {
       sa->valid = false;
+      sa->gauss = t_hi < kInf ? arg : kNoGauss;
       if (keep && t_hi < kInf) {
         const float ts = t_hi;
         float aw = 0.f, ar = 0.f, ag = 0.f, ab = 0.f;
@@ -467,9 +495,10 @@ struct ThreadQueries {
   }
   __device__ float argmin(float3 o, float3 d, uint64_t key, ScatterAlbedo* sa) {
     sa->valid = false;  // the plain megakernel evaluates the albedo with its own point query
+    sa->gauss = kNoGauss;
     return ray<kArgmin>(o, d, key);
   }
-  __device__ float transmittance(float3 o, float3 d) {
+  __device__ float transmittance(float3 o, float3 d, uint32_t /*seed: the plain megakernel traverses*/ = kNoGauss) {
     const float tau = ray<kTau>(o, d, 0ull);
     return tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
   }

@@ -139,7 +139,10 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
       ++scatters;
     }
     ++bounces;
-    if (lane == 0) b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+    if (lane == 0) {
+      b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+      b.sg[p] = tstar < kInf ? sa.gauss : kNoGauss;
+    }
     if (status) break;
   }
   if (lane == 0) {
@@ -183,11 +186,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
       const float4 a = b.alb4[p];
       const bool scattered = a.w < kInf;
       ShadowSet sh;
-      alive = shade_bounce(E, P, s, scattered, a.w, f3(a.x, a.y, a.z), sh);
+      alive = shade_bounce(E, P, s, scattered, a.w, f3(a.x, a.y, a.z), sh, b.sg[p]);
       ns = sh.n;
       for (int k = 0; k < sh.n; ++k) {
         b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, 1.f);
-        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, 0.f);
+        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k]));
         b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
       }
       if (alive) {
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(Scen
     const uint32_t slot = __ldg(b.qs + item);
     const float4 o = b.so4[slot], d = b.sd4[slot];
     const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws,
-                                                 measure);
+                                                 measure, nullptr, __float_as_uint(d.w));
     if (lane == 0) b.so4[slot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
     if (status) break;
   }
@@ -313,7 +316,7 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   WfWorkspace& w = ctx->wf;
   if (w.cap >= paths && w.base) return VP_OK;
   free_wavefront(ctx);
-  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 3 * 48 + 16 + 4 * 5;
+  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 4 + 3 * 48 + 16 + 4 * 5;
   const size_t bytes = paths * per_path + 64 * 256 + 4096;
   cudaError_t e = cudaMalloc(&w.base, bytes);
   if (e != cudaSuccess) {
@@ -335,6 +338,7 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   carve_buf(cur, b.key2, paths);
   carve_buf(cur, b.meta, paths);
   carve_buf(cur, b.alb4, paths);
+  carve_buf(cur, b.sg, paths);
   carve_buf(cur, b.so4, 3 * paths);
   carve_buf(cur, b.sd4, 3 * paths);
   carve_buf(cur, b.sw4, 3 * paths);

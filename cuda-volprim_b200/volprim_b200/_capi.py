@@ -16,6 +16,7 @@ VP_NEE_MIS, VP_NEE_PHASE, VP_NEE_RIS, VP_NEE_NONE = 0, 1, 2, 3
 VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL, VP_ENGINE_WAVEFRONT = 0, 1, 2
 VP_PRECISION_AUTO, VP_PRECISION_FAST, VP_PRECISION_ACCURATE = 0, 1, 2
 VP_MEASURE_COUNTERS, VP_MEASURE_STAGES = 1, 2
+VP_SCHEDULE_FIFO, VP_SCHEDULE_FAIR, VP_SCHEDULE_SRPT = 0, 1, 2
 
 ERROR_NAMES = {
     -1: "VP_ERROR_INVALID_ARGUMENT", -2: "VP_ERROR_CUDA", -3: "VP_ERROR_OUT_OF_MEMORY",
@@ -138,6 +139,17 @@ class vp_gaussian_grads(C.Structure):
     ]
 
 
+class vp_host_gaussians(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint32),
+        ("mean", C.POINTER(C.c_float)),
+        ("log_scale", C.POINTER(C.c_float)),
+        ("quat_wxyz", C.POINTER(C.c_float)),
+        ("density", C.POINTER(C.c_float)),
+        ("albedo", C.POINTER(C.c_float)),
+    ]
+
+
 class vp_server_config(C.Structure):
     _fields_ = [
         ("memory_budget_bytes", C.c_uint64),
@@ -146,7 +158,7 @@ class vp_server_config(C.Structure):
         ("iterations_per_step", C.c_uint32),
         ("precision", C.c_int32),
         ("use_graph", C.c_int32),
-        ("reserved", C.c_int32),
+        ("schedule", C.c_int32),
     ]
 
 
@@ -221,6 +233,12 @@ SIGNATURES = {
     "vp_server_poll": [P, C.POINTER(C.c_uint64), C.c_uint32, C.POINTER(C.c_uint32)],
     "vp_server_get_stats": [P, C.POINTER(vp_server_stats)],
     "vp_server_destroy": [P],
+    "vp_ply_load": [C.c_char_p, P, C.POINTER(vp_host_gaussians)],
+    "vp_ply_save": [C.c_char_p, C.POINTER(vp_host_gaussians)],
+    "vp_host_gaussians_free": [C.POINTER(vp_host_gaussians)],
+    "vp_hdr_load": [C.c_char_p, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+    "vp_host_free": [P],
+    "vp_exr_save": [C.c_char_p, P, C.c_uint32, C.c_uint32, C.c_int32],
 }
 _RESTYPES = {"vp_last_error_string": C.c_char_p}
 

@@ -27,7 +27,7 @@ class Server:
 
     def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 21,
                  max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
-                 use_graph: bool = True):
+                 use_graph: bool = True, schedule: str = "fifo"):
         c = _capi.vp_server_config()
         c.memory_budget_bytes = int(memory_budget_bytes)
         c.path_slots = int(path_slots)
@@ -35,6 +35,7 @@ class Server:
         c.iterations_per_step = int(iterations_per_step)
         c.precision = {"auto": 0, "fast": 1, "accurate": 2}[precision]
         c.use_graph = 1 if use_graph else 0
+        c.schedule = {"fifo": 0, "fair": 1, "srpt": 2}[schedule]
         h = C.c_void_p()
         check(lib.vp_server_create(ctx.handle, C.byref(c), C.byref(h)))
         self.handle, self.ctx = h, ctx

@@ -358,9 +358,9 @@ vp_status vp_render_emission_backward(vp_scene* scene, vp_env* env, const vp_cam
 
 /* A server owns a pool of path slots and the wavefront stage kernels over them.  Each iteration
  * refills the slots freed by finished paths with new (pixel, sample) paths of the admitted
- * requests in admission order, then extends, shades, traces shadow rays and gathers every path
- * in flight -- paths of different requests, scenes, resolutions and sample counts share the same
- * launches.  The iteration is captured once as a CUDA graph.  Requests wait in a FIFO until the
+ * requests that still have unstarted paths (in the order the schedule gives), then extends,
+ * shades, traces shadow rays and gathers every path in flight -- paths of different requests,
+ * scenes, resolutions and sample counts share the same launches.  The iteration is captured once as a CUDA graph.  Requests wait in a FIFO until the
  * request table has a free entry and their image accumulator fits the memory budget.  A finished
  * path adds its sample to its request's per-pixel sum; a request completes when all its
  * width*height*spp paths have finished, and its mean image is written to its output buffer.
@@ -368,15 +368,25 @@ vp_status vp_render_emission_backward(vp_scene* scene, vp_env* env, const vp_cam
  * (the same PCG32 stream per (pixel, sample)); only the order of the per-pixel FP32 sums differs. */
 typedef struct vp_server vp_server;
 
+/* How an iteration's free path slots are shared among the admitted requests that still have
+ * unstarted paths. */
+typedef enum vp_schedule {
+  VP_SCHEDULE_FIFO = 0,  /* admission order: a request's paths all start before the next's; free
+                            slots the oldest request cannot use go to the next (default) */
+  VP_SCHEDULE_FAIR = 1,  /* equal shares (processor sharing); leftovers in table order */
+  VP_SCHEDULE_SRPT = 2   /* fewest unstarted paths first (shortest remaining work) */
+} vp_schedule;
+
 typedef struct vp_server_config {
   uint64_t memory_budget_bytes;  /* device bytes for resident scenes + path slots + request
                                     accumulators (0 = no limit) */
   uint32_t path_slots;           /* paths in flight (0 = 2^21) */
-  uint32_t max_requests;         /* request table entries (0 = 256) */
+  uint32_t max_requests;         /* request table entries (0 = 256; rounded up to a multiple
+                                    of 32, at most 1024) */
   uint32_t iterations_per_step;  /* wavefront iterations per vp_server_step (0 = 4; even) */
   int32_t precision;             /* vp_precision of every request: FAST or ACCURATE (AUTO = FAST) */
   int32_t use_graph;             /* 1: replay the iterations as a captured CUDA graph */
-  int32_t reserved;
+  int32_t schedule;              /* vp_schedule: how free path slots are shared among requests */
 } vp_server_config;
 
 typedef struct vp_request {
@@ -412,6 +422,43 @@ vp_status vp_server_step(vp_server* server, uint32_t* completed);
 vp_status vp_server_poll(vp_server* server, uint64_t* ids, uint32_t cap, uint32_t* n);
 vp_status vp_server_get_stats(vp_server* server, vp_server_stats* out);
 vp_status vp_server_destroy(vp_server* server);
+
+/* ---------------------------------------------------------------------------------------- */
+/* asset IO on the host (replaces src/thesis/host/utils/io/ply.cpp, hdr.cpp, exr.cpp)          */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Gaussians in library-allocated host arrays (release with vp_host_gaussians_free).  The arrays
+ * go straight into vp_gaussians with scale = log_scale and scale_is_log = 1. */
+typedef struct vp_host_gaussians {
+  uint32_t count;
+  float* mean;       /* [3 * count] */
+  float* log_scale;  /* [3 * count] */
+  float* quat_wxyz;  /* [4 * count], as stored (vp_scene_create normalises) */
+  float* density;    /* [count] total mass (sigma_t_0); sigma_multiplier applies at scene build */
+  float* albedo;     /* [3 * count] (clamped at scene build) */
+} vp_host_gaussians;
+
+/* Reads the "vertex" element of a Gaussian PLY: x y z rot_0..3 (w, x, y, z) scale_0..2 (log)
+ * albedo_0..2 sigma_t_0, any numeric property types, ascii or binary of either byte order.
+ * albedo_override (3 floats, or NULL) replaces the file's albedo when all three are >= 0.
+ * Replaces io::loadPrimitivesFromPLY (ply.cpp:35-175); its validation is vp_scene_create's. */
+vp_status vp_ply_load(const char* path, const float* albedo_override, vp_host_gaussians* out);
+/* Writes the same 14 properties as binary little-endian floats (albedo NULL -> 0). */
+vp_status vp_ply_save(const char* path, const vp_host_gaussians* gaussians);
+vp_status vp_host_gaussians_free(vp_host_gaussians* gaussians);
+
+/* Reads a Radiance RGBE picture ("#?RADIANCE"/"#?RGBE", FORMAT=32-bit_rle_rgbe, "-Y H +X W",
+ * new run-length or raw scanlines) into a library-allocated RGB float array (row 0 = the first
+ * scanline; release with vp_host_free), ready for vp_env_create(..., channels = 3, HOST).
+ * Replaces the reference's .hdr loader (hdr.cpp). */
+vp_status vp_hdr_load(const char* path, float** out_rgb, uint32_t* width, uint32_t* height);
+vp_status vp_host_free(void* p);
+
+/* Writes width*height RGBA floats (alpha dropped) as a single-part scanline OpenEXR file with
+ * uncompressed FLOAT channels B, G, R, flipped vertically when flip_vertical != 0.  Replaces
+ * saveExrImage (exr.cpp:36-100). */
+vp_status vp_exr_save(const char* path, const float* rgba, uint32_t width, uint32_t height,
+                      int32_t flip_vertical);
 
 /* Grid-stride copy out[i] = accumulator[i] * normalization_factor over n float4 pixels on the
  * context's stream (or `stream` when non-NULL).  Same contract as the reference's

@@ -132,6 +132,26 @@ def test_graph_and_direct_launches_agree(vp_ctx, world):
         assert np.all(close(a, b))
 
 
+def test_schedules(vp_ctx, world):
+    """Every schedule gives the same images; under FAIR and SRPT a small request submitted after
+    a large one (more paths than the slot pool) completes first."""
+    big = make_trace(15, 1, rate=0.0, n_scenes=1, resolutions=(256,), spps=(8,))[0]
+    small = make_trace(16, 1, rate=0.0, n_scenes=1, resolutions=(32,), spps=(1,))[0]
+    imgs = {}
+    for sched in ("fair", "fifo", "srpt"):
+        srv = new_server(vp_ctx, world, schedule=sched, iterations_per_step=2)
+        ib = srv.submit(big.scene_id, big.camera, big.config)
+        isml = srv.submit(small.scene_id, small.camera, small.config)
+        order = drain(srv)
+        if sched in ("fair", "srpt"):
+            assert order.index(isml) < order.index(ib), sched
+        imgs[sched] = (srv.result(ib), srv.result(isml))
+        srv.close()
+    for sched in ("fifo", "srpt"):
+        for a, b in zip(imgs[sched], imgs["fair"]):
+            assert np.all(close(a, b)), sched
+
+
 def test_admission_respects_the_memory_budget(vp_ctx, world):
     probe = new_server(vp_ctx, world)
     fixed = probe.stats()["bytes_in_use"]
