@@ -114,7 +114,7 @@ __device__ __forceinline__ void flush_stats(Counters* c, const PathStats& ps, co
 
 // Persistent warp-per-path kernel: warps pull pixels from a global counter; each pixel runs
 // samples [spp_offset, spp_offset + spp_count) in order and Welford-updates mean/count.
-template <bool kAcc>
+template <bool kAcc, bool kMeasure>
 __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneView S, EnvView E, CameraView C,
                                                      ParamsView P, float4* __restrict__ mean,
                                                      uint32_t* __restrict__ count,
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
   uint32_t status = 0;
   WarpStats ws;
   PathStats ps;
-  WarpQueries<kAcc> q{S, W, status, ws, P.measure != 0};
+  WarpQueries<kAcc> q{S, W, status, ws, kMeasure && P.measure != 0};
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(work, 1u);
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
     }
     if (status) break;
   }
-  if (lane == 0) flush_stats(ctr, ps, ws, status, P.measure != 0);
+  if (lane == 0) flush_stats(ctr, ps, ws, status, kMeasure && P.measure != 0);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -297,17 +297,12 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
     const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kHitCap);
     if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the warp engine's shared-memory stack");
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
-    if (P.accurate) {
-      if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(k_render_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      const int blocks = ctx->sm_count * occupancy_blocks(k_render_warp<true>, threads, smem);
-      k_render_warp<true><<<blocks, threads, smem, st>>>(s->view, e->view, cam, P, img->mean, img->count,
-                                                        spp_offset, spp_count, ctx->work_counter, ctx->counters);
-    } else {
-      if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(k_render_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      const int blocks = ctx->sm_count * occupancy_blocks(k_render_warp<false>, threads, smem);
-      k_render_warp<false><<<blocks, threads, smem, st>>>(s->view, e->view, cam, P, img->mean, img->count,
-                                                         spp_offset, spp_count, ctx->work_counter, ctx->counters);
-    }
+    auto kern = P.accurate ? (P.measure ? k_render_warp<true, true> : k_render_warp<true, false>)
+                           : (P.measure ? k_render_warp<false, true> : k_render_warp<false, false>);
+    if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = ctx->sm_count * occupancy_blocks(kern, threads, smem);
+    kern<<<blocks, threads, smem, st>>>(s->view, e->view, cam, P, img->mean, img->count, spp_offset, spp_count,
+                                        ctx->work_counter, ctx->counters);
   } else if (engine == VP_ENGINE_MEGAKERNEL) {
     const dim3 grid((P.width + 15) / 16, (P.height + 7) / 8);
     if (P.accurate)

@@ -105,7 +105,9 @@ __global__ void k_wf_generate(CameraView C, ParamsView P, uint32_t spp_offset, u
   b.L4[p] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-template <bool kAcc>
+// kMeasure = false compiles the statistics out (their registers would otherwise stay live
+// through the traversal loop).
+template <bool kAcc, bool kMeasure>
 __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S, ParamsView P, WfBuffers b, const uint32_t* q,
                                                    const uint32_t* count, unsigned int* work, Counters* ctr) {
   extern __shared__ unsigned char smem[];
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
   uint32_t status = 0, max_overlap = 0;
   unsigned long long bounces = 0, scatters = 0;
   WarpStats ws;
-  const bool measure = P.measure != 0;
+  const bool measure = kMeasure && P.measure != 0;
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(work, 1u);
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
   }
 }
 
-template <bool kAcc>
+template <bool kAcc, bool kMeasure>
 __global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(SceneView S, WfBuffers b, const uint32_t* count,
                                                    unsigned int* work, Counters* ctr, int measure_i) {
   extern __shared__ unsigned char smem[];
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(Scen
   const uint32_t n = *count;
   uint32_t status = 0;
   WarpStats ws;
-  const bool measure = measure_i != 0;
+  const bool measure = kMeasure && measure_i != 0;
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(work, 1u);
@@ -376,8 +378,10 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kExtendHitCap);
   const size_t smem_sh = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, 32);
   if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the shared-memory stack");
-  auto ext = P.accurate ? k_wf_extend<true> : k_wf_extend<false>;
-  auto shd = P.accurate ? k_wf_shadow<true> : k_wf_shadow<false>;
+  auto ext = P.accurate ? (P.measure ? k_wf_extend<true, true> : k_wf_extend<true, false>)
+                        : (P.measure ? k_wf_extend<false, true> : k_wf_extend<false, false>);
+  auto shd = P.accurate ? (P.measure ? k_wf_shadow<true, true> : k_wf_shadow<true, false>)
+                        : (P.measure ? k_wf_shadow<false, true> : k_wf_shadow<false, false>);
   if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(ext, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (smem_sh > 48 * 1024)
     VP_CUDA(cudaFuncSetAttribute(shd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_sh));

@@ -218,3 +218,64 @@ def run_trace_plain(scenes: list, envs: list, trace: list) -> dict:
     paths = sum(r.paths for r in trace)
     return {"latency_s": lat, "makespan_s": makespan, "paths": paths, "busy_s": busy,
             "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "mpaths_per_s": paths / makespan / 1e6}
+
+
+def main(argv=None) -> None:
+    """The serving workload end to end: the 4 resident scenes (50k / 100k / 250k / 500k Gaussians),
+    the first --requests of the seeded request stream all at t = 0 (offline throughput), then
+    with Poisson arrivals at --load x that throughput under each schedule, then through one
+    vp_render per request.  One JSON line per run."""
+    import argparse
+    import json
+
+    from . import scenes
+    from .api import Context, Environment, Scene
+
+    ap = argparse.ArgumentParser(prog="python -m volprim_b200.serving")
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--schedules", default="fifo,fair,srpt")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    ctx = Context(a.device)
+    gs, sigma, env_img = scenes.serving_scenes()
+    scs = [Scene(ctx, g, sigma) for g in gs]
+    env = Environment(ctx, rgb=env_img)
+
+    def server(schedule):
+        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule)
+        for sc in scs:
+            s.add_scene(sc, env)
+        return s
+
+    def summary(r):
+        lat = sorted(r["latency_s"])
+        return {"p50_s": r["p50_s"], "p90_s": percentile(lat, 90), "p99_s": r["p99_s"], "max_s": lat[-1],
+                "mpaths_per_s": r["mpaths_per_s"], "makespan_s": r["makespan_s"]}
+
+    burst = make_trace(a.seed, a.requests, rate=0.0, n_scenes=len(scs))
+    srv = server("fifo")
+    off = run_trace(srv, burst)
+    srv.close()
+    rate = a.load * off["mpaths_per_s"] * 1e6 / (off["paths"] / a.requests)
+    print(json.dumps({"run": "offline", "requests": a.requests, "paths": off["paths"],
+                      "mpaths_per_s": off["mpaths_per_s"], "arrival_rate_per_s": rate, "load": a.load}), flush=True)
+    trace = make_trace(a.seed, a.requests, rate=rate, n_scenes=len(scs))
+    for sched in a.schedules.split(","):
+        srv = server(sched)
+        r = run_trace(srv, trace)
+        st = srv.stats()
+        srv.close()
+        print(json.dumps({"run": "served", "schedule": sched, **summary(r), "device_ms": st["device_ms"],
+                          "iterations": st["iterations"]}), flush=True)
+    pl = run_trace_plain(scs, [env] * len(scs), trace)
+    print(json.dumps({"run": "plain per-request", **summary(pl), "busy_s": pl["busy_s"]}), flush=True)
+    for s in scs:
+        s.close()
+    env.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
