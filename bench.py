@@ -372,6 +372,7 @@ def run_ours(args):
     if rank == 0 and not args.no_forms and world == 1:
         line["differentiation"] = differentiation_form(local)
         line["serving"] = serving_form(local, args.serving_requests)
+        line["other_configs"] = other_configs(local)
     if rank == 0 and not args.no_cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
@@ -484,6 +485,43 @@ def differentiation_form(device):
             "backward_kernel_ms": bwd_ms, "scene_build_ms": info["build_ms"],
             "note": "one gradient = scene build from the parameter tensors + 4 forward + 4 adjoint renders "
                     "(autograd Function), host-timed around torch.cuda.synchronize; kernel split from CUDA events"}
+
+
+def other_configs(device):
+    """The other two configurations, one timed pass each (wavefront engine, inputs resident):
+    the 256-Gaussian absorption case (128x128, 16 spp, ACCURATE, the FP64-gated image) and the
+    2M-Gaussian traversal stress case (1024x1024, one 16-spp batch of its 64 spp) with its BVH
+    build time and the overlap / hit counts of the measured batch."""
+    import torch
+    import volprim_b200 as vp
+    from volprim_b200 import scenes
+
+    out = {}
+    ctx = vp.Context(device)
+    for name, w, spp in (("absorption_256", scenes.absorption_256(), 16), ("stress_2m", scenes.stress_2m(), 16)):
+        cfg = w.config
+        cfg.engine = "wavefront"
+        sc = vp.Scene(ctx, w.gaussians, w.sigma_multiplier)
+        env = vp.Environment(ctx, rgb=w.env) if w.env is not None else vp.Environment(ctx, constant=(1.0, 1.0, 1.0))
+        img = vp.ProgressiveImage(ctx, cfg.image_width, cfg.image_height)
+        img.accumulate(sc, env, w.camera, cfg, 0, min(spp, cfg.num_samples_per_pixel))  # warm-up
+        img.clear()
+        torch.cuda.synchronize()
+        st = img.accumulate(sc, env, w.camera, cfg, 0, min(spp, cfg.num_samples_per_pixel))
+        mcfg = vp.Config(**{**cfg.__dict__, "measure_caps": True})
+        img.clear()
+        ms = img.accumulate(sc, env, w.camera, mcfg, 0, min(spp, cfg.num_samples_per_pixel))
+        info = sc.info()
+        out[name] = {"mpaths_per_s": st["paths"] / (st["ms_kernels"] / 1e3) / 1e6, "paths": st["paths"],
+                     "ms": st["ms_kernels"], "gaussians": info["count"], "bvh_build_ms": info["build_ms"],
+                     "bvh32_nodes": info["wide_nodes"], "precision": cfg.precision,
+                     "max_point_overlap": ms["max_point_overlap"], "max_hits_per_ray": ms["max_hits_per_ray"],
+                     "crossings": ms["crossings"]}
+        img.close()
+        env.close()
+        sc.close()
+    ctx.close()
+    return out
 
 
 def serving_form(device, n_requests):
