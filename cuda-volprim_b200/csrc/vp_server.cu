@@ -150,7 +150,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 //   VP_SCHEDULE_FIFO  in admission order, each request taking all it still has;
 //   VP_SCHEDULE_FAIR  an equal quota ceil(free / k) to each of the k requests (capped at what each
 //                     still has), then what is left over in table order;
-//   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order).
+//   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order), with half of the
+//                     free slots kept for the oldest request that still has unstarted paths.
 // Writes the per-entry offsets of this iteration's new paths (alloc_off, size R + 1) and their
 // first pixel-major path index (alloc_start).
 __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, unsigned long long* __restrict__ started,
@@ -160,6 +161,8 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
   __shared__ uint32_t s_free, s_surv;
   __shared__ unsigned long long s_key[kMaxRequests], s_seq[kMaxRequests];
   __shared__ uint32_t s_by_rank[kMaxRequests];
+  __shared__ unsigned long long s_oldest;
+  __shared__ uint32_t s_reserve;
   const uint32_t e = threadIdx.x, R = blockDim.x;
   if (e == 0) {
     s_free = c->free_count;
@@ -190,13 +193,32 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
     const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? rem64 : seq);
     s_key[e] = key;
     s_seq[e] = seq;
+    // SRPT: half of the free slots stay with the oldest request that has unstarted paths, so a
+    // large request keeps progressing while smaller ones overtake it
+    uint32_t reserve = 0, Fs = F;
+    if (schedule == VP_SCHEDULE_SRPT) {
+      if (e == 0) {
+        s_oldest = ~0ull;
+        s_reserve = 0u;
+      }
+      __syncthreads();
+      if (rem) atomicMin(&s_oldest, seq);
+      __syncthreads();
+      if (rem && seq == s_oldest) {
+        reserve = min(rem, F / 2u);
+        s_reserve = reserve;
+      }
+      __syncthreads();
+      Fs = F - s_reserve;
+    }
     __syncthreads();
     uint32_t rank = 0;
     for (uint32_t j = 0; j < R; ++j) {
       const unsigned long long kj = s_key[j], sj = s_seq[j];
       rank += (kj < key || (kj == key && (sj < seq || (sj == seq && j < e)))) ? 1u : 0u;
     }
-    s_by_rank[rank] = rem;
+    const uint32_t rest = rem - reserve;
+    s_by_rank[rank] = rest;
     __syncthreads();
     uint32_t tot = 0;
     const uint32_t before = block_exclusive_scan(s_by_rank[e], warp_tot, tot);  // thread e = rank e here
@@ -204,7 +226,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
     s_by_rank[e] = before;  // offset of rank e
     __syncthreads();
     const uint32_t off = s_by_rank[rank];
-    a = off >= F ? 0u : min(rem, F - off);
+    a = reserve + (off >= Fs ? 0u : min(rest, Fs - off));
   }
   uint32_t m = 0;
   const uint32_t off = block_exclusive_scan(a, warp_tot, m);
@@ -651,7 +673,7 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   s->ctx = ctx;
   if (config) s->cfg = *config;
   vp_server_config& c = s->cfg;
-  if (c.path_slots == 0) c.path_slots = 1u << 21;
+  if (c.path_slots == 0) c.path_slots = 1u << 18;
   if (c.max_requests == 0) c.max_requests = 256;
   c.max_requests = (c.max_requests + 31u) & ~31u;  // the share computation runs one block of warps
   if (c.max_requests > kMaxRequests) {

@@ -25,7 +25,7 @@ from .api import Camera, Config, Context, Environment, Scene, _alive, _is_cuda_t
 class Server:
     """vp_server_create / add_scene / submit / step / poll."""
 
-    def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 21,
+    def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 18,
                  max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
                  use_graph: bool = True, schedule: str = "fifo"):
         c = _capi.vp_server_config()
@@ -237,14 +237,15 @@ def main(argv=None) -> None:
     ap.add_argument("--schedules", default="fifo,fair,srpt")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--slots", default=str(1 << 18), help="path-slot pool sizes to compare (comma separated)")
     a = ap.parse_args(argv)
     ctx = Context(a.device)
     gs, sigma, env_img = scenes.serving_scenes()
     scs = [Scene(ctx, g, sigma) for g in gs]
     env = Environment(ctx, rgb=env_img)
 
-    def server(schedule):
-        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule)
+    def server(schedule, slots=1 << 18):
+        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule, path_slots=slots)
         for sc in scs:
             s.add_scene(sc, env)
         return s
@@ -262,13 +263,14 @@ def main(argv=None) -> None:
     print(json.dumps({"run": "offline", "requests": a.requests, "paths": off["paths"],
                       "mpaths_per_s": off["mpaths_per_s"], "arrival_rate_per_s": rate, "load": a.load}), flush=True)
     trace = make_trace(a.seed, a.requests, rate=rate, n_scenes=len(scs))
-    for sched in a.schedules.split(","):
-        srv = server(sched)
-        r = run_trace(srv, trace)
-        st = srv.stats()
-        srv.close()
-        print(json.dumps({"run": "served", "schedule": sched, **summary(r), "device_ms": st["device_ms"],
-                          "iterations": st["iterations"]}), flush=True)
+    for slots in (int(x) for x in a.slots.split(",")):
+        for sched in a.schedules.split(","):
+            srv = server(sched, slots)
+            r = run_trace(srv, trace)
+            st = srv.stats()
+            srv.close()
+            print(json.dumps({"run": "served", "schedule": sched, "path_slots": slots, **summary(r),
+                              "device_ms": st["device_ms"], "iterations": st["iterations"]}), flush=True)
     pl = run_trace_plain(scs, [env] * len(scs), trace)
     print(json.dumps({"run": "plain per-request", **summary(pl), "busy_s": pl["busy_s"]}), flush=True)
     for s in scs:

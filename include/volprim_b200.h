@@ -374,13 +374,15 @@ typedef enum vp_schedule {
   VP_SCHEDULE_FIFO = 0,  /* admission order: a request's paths all start before the next's; free
                             slots the oldest request cannot use go to the next (default) */
   VP_SCHEDULE_FAIR = 1,  /* equal shares (processor sharing); leftovers in table order */
-  VP_SCHEDULE_SRPT = 2   /* fewest unstarted paths first (shortest remaining work) */
+  VP_SCHEDULE_SRPT = 2   /* fewest unstarted paths first (shortest remaining work), with half of
+                            the free slots kept for the oldest request so large ones progress */
 } vp_schedule;
 
 typedef struct vp_server_config {
   uint64_t memory_budget_bytes;  /* device bytes for resident scenes + path slots + request
                                     accumulators (0 = no limit) */
-  uint32_t path_slots;           /* paths in flight (0 = 2^21) */
+  uint32_t path_slots;           /* paths in flight (0 = 2^18); fewer slots shorten each iteration,
+                                    so a request's last paths finish sooner */
   uint32_t max_requests;         /* request table entries (0 = 256; rounded up to a multiple
                                     of 32, at most 1024) */
   uint32_t iterations_per_step;  /* wavefront iterations per vp_server_step (0 = 4; even) */
