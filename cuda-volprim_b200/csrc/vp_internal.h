@@ -56,12 +56,15 @@ struct WfBuffers {
                                   // seed Gaussian's bits in .w), weight
   float4* L4;                     // finished sample radiance
   uint32_t *qa, *qb, *qs;         // path queues (current / next) and shadow-query queue
+  uint32_t *qt, *sk_a, *sk_b;     // sorting: a spare queue and the Morton keys of path origins
   uint32_t* ctr;                  // [0] paths now, [1] paths next, [2] shadow queries, [3..4] work heads
 };
 struct WfWorkspace {
   size_t cap = 0;  // paths
   WfBuffers b{};
   void* base = nullptr;
+  void* sort_tmp = nullptr;  // CUB radix-sort scratch for `cap` keys
+  size_t sort_tmp_bytes = 0;
   uint32_t* host_count = nullptr;  // pinned, for polling the active-path count
 };
 }  // namespace vp

@@ -22,6 +22,8 @@
 // same order of radiance accumulation.
 #include <algorithm>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "vp_internal.h"
 #include "vp_path.cuh"
 #include "vp_traverse.cuh"
@@ -44,6 +46,11 @@ constexpr uint32_t kAliveBit = 1u << 18;
 #define VP_WF_EXTEND_HIT_CAP 64
 #endif
 constexpr int kExtendHitCap = VP_WF_EXTEND_HIT_CAP;
+// Queues shorter than this are not re-sorted (the sort would cost more than it saves).
+#ifndef VP_WF_SORT_MIN
+#define VP_WF_SORT_MIN 65536
+#endif
+constexpr uint32_t kSortMinPaths = VP_WF_SORT_MIN;
 
 __device__ __forceinline__ uint32_t meta_bounce(uint32_t m) { return m & 0xFFFFu; }
 __device__ __forceinline__ uint32_t meta_nshadow(uint32_t m) { return (m >> 16) & 3u; }
@@ -301,6 +308,27 @@ __global__ void k_wf_welford(WfBuffers b, uint32_t batch, uint32_t n_pix, float4
   count[pix] = prev + batch;
 }
 
+// Morton key (10 bits per axis) of each queued path's origin over the scene bounds: sorting the
+// queue by it makes neighbouring warps traverse the same BVH32 region (L1 reuse).
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_wf_sort_keys(uint32_t n, const uint32_t* __restrict__ q, const float4* __restrict__ o4,
+                               float3 lo, float3 inv_ext, uint32_t* __restrict__ keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 o = o4[q[i]];
+  auto quant = [](float x) { return (uint32_t)fminf(fmaxf(x, 0.0f), 1023.0f); };
+  const uint32_t x = quant((o.x - lo.x) * inv_ext.x), y = quant((o.y - lo.y) * inv_ext.y),
+                 z = quant((o.z - lo.z) * inv_ext.z);
+  keys[i] = (expand10(z) << 2) | (expand10(y) << 1) | expand10(x);
+}
+
 template <class K>
 int resident_blocks(K kernel, int threads, size_t smem) {
   int b = 0;
@@ -318,7 +346,7 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   WfWorkspace& w = ctx->wf;
   if (w.cap >= paths && w.base) return VP_OK;
   free_wavefront(ctx);
-  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 4 + 3 * 48 + 16 + 4 * 5;
+  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 4 + 3 * 48 + 16 + 4 * 5 + 3 * 4;
   const size_t bytes = paths * per_path + 64 * 256 + 4096;
   cudaError_t e = cudaMalloc(&w.base, bytes);
   if (e != cudaSuccess) {
@@ -348,8 +376,20 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   carve_buf(cur, b.qa, paths);
   carve_buf(cur, b.qb, paths);
   carve_buf(cur, b.qs, 3 * paths);
+  carve_buf(cur, b.qt, paths);
+  carve_buf(cur, b.sk_a, paths);
+  carve_buf(cur, b.sk_b, paths);
   carve_buf(cur, b.ctr, 64);
   w.cap = paths;
+  size_t tmp = 0;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, tmp, b.sk_a, b.sk_b, b.qa, b.qt, (int)paths, 0, 30);
+  if (e == cudaSuccess) e = cudaMalloc(&w.sort_tmp, tmp);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    free_wavefront(ctx);
+    return fail(VP_ERROR_OUT_OF_MEMORY, "wavefront sort scratch");
+  }
+  w.sort_tmp_bytes = tmp;
   return VP_OK;
 }
 
@@ -358,7 +398,10 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
 void free_wavefront(vp_context* ctx) {
   WfWorkspace& w = ctx->wf;
   if (w.base) cudaFree(w.base);
+  if (w.sort_tmp) cudaFree(w.sort_tmp);
   w.base = nullptr;
+  w.sort_tmp = nullptr;
+  w.sort_tmp_bytes = 0;
   w.cap = 0;
 }
 
@@ -412,7 +455,25 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   ctx->launches += 1;
   uint32_t* qcur = b.qa;
   uint32_t* qnext = b.qb;
+  // Path origins' Morton order: the queue is re-sorted after every poll (the count is known on
+  // the host then); compaction keeps most of the order in between.
+  const vp_scene_info& si = s->info;
+  const float3 blo = make_float3((float)si.bounds_min[0], (float)si.bounds_min[1], (float)si.bounds_min[2]);
+  auto inv_ext1 = [](double a, double b) { return (float)(1024.0 / std::max(b - a, 1e-30)); };
+  const float3 binv = make_float3(inv_ext1(si.bounds_min[0], si.bounds_max[0]),
+                                  inv_ext1(si.bounds_min[1], si.bounds_max[1]),
+                                  inv_ext1(si.bounds_min[2], si.bounds_max[2]));
+  uint32_t polled = paths;
   for (uint32_t it = 0; it < P.max_bounces; ++it) {
+    if (it != 0u && (it & 3u) == 0u && polled >= kSortMinPaths) {  // (camera rays share one origin)
+      k_wf_sort_keys<<<(polled + 255) / 256, 256, 0, st>>>(polled, qcur, b.o4, blo, binv, b.sk_a);
+      size_t tmp = ctx->wf.sort_tmp_bytes;
+      VP_CUDA(cub::DeviceRadixSort::SortPairs(ctx->wf.sort_tmp, tmp, b.sk_a, b.sk_b, qcur, b.qt, (int)polled, 0, 30,
+                                              st));
+      VP_CUDA(cudaGetLastError());
+      ctx->launches += 1;
+      std::swap(qcur, b.qt);
+    }
     cudaEvent_t* e4 = ev + 4 * (it & 3u);
     if (timed) VP_CUDA(cudaEventRecord(e4[0], st));
     ext<<<ext_blocks, threads, smem, st>>>(s->view, P, b, qcur, b.ctr + 0, b.ctr + 3, ctx->counters);
@@ -433,7 +494,8 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
       VP_CUDA(cudaMemcpyAsync(ctx->wf.host_count, b.ctr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
       VP_CUDA(cudaStreamSynchronize(st));
       VP_CUDA(harvest());
-      if (*ctx->wf.host_count == 0u) break;
+      polled = *ctx->wf.host_count;
+      if (polled == 0u) break;
     }
   }
   k_wf_welford<<<(n_pix + 255) / 256, 256, 0, st>>>(b, spp_count, n_pix, img->mean, img->count);
