@@ -17,6 +17,8 @@ CSRC = HERE / "csrc"
 OBJ = HERE / "build"
 LIBDIR = HERE / "volprim_b200" / "_lib"
 LIB = LIBDIR / "libvolprim_b200.so"
+APP = HERE / "app" / "vp_render.cpp"
+APP_BIN = LIBDIR / "vp_render"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -76,7 +78,23 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_app(force=force)
     return LIB
+
+
+def build_app(force: bool = False) -> Path:
+    """Compiles the vp_render command-line program (app/vp_render.cpp) against the C ABI only;
+    it finds libvolprim_b200.so beside itself through an $ORIGIN run path."""
+    if force or _stale(APP_BIN, [APP, INCLUDE / "volprim_b200.h", LIB]):
+        cxx = shutil.which("g++") or shutil.which("c++")
+        if cxx is None:
+            raise RuntimeError("a C++ compiler (g++) is required to build vp_render")
+        cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), str(APP), "-L", str(LIBDIR),
+               "-lvolprim_b200", "-Wl,-rpath,$ORIGIN", "-o", str(APP_BIN)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"vp_render build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return APP_BIN
 
 
 if __name__ == "__main__":
