@@ -1,5 +1,8 @@
 // Scene build on the device: per-Gaussian precompute, 3-sigma ellipsoid bounds, 63-bit Morton
-// codes, radix sort, Karras binary radix tree, bottom-up refit, collapse to a 32-wide BVH.
+// codes, radix sort, then two binary trees over the sorted boxes -- a Karras radix tree with a
+// bottom-up refit (the thread-per-ray megakernel's tree) and a PLOC agglomerative clustering
+// (the warp engines' tree) -- and the collapse of the latter to a 32-wide BVH, whose depth-first
+// leaf order becomes the scene order of the Gaussians.
 //
 // Replaces the reference's host Morton sort + OptiX unit-sphere GAS / instance IAS build
 // (src/thesis/host/app/renderer.cpp:85-173, include/thesis/host/utils/math.h:103-131,
@@ -7,6 +10,7 @@
 // (include/thesis/device/params/primitive.h:70-87) plus PLY-load validation
 // (src/thesis/host/utils/io/ply.cpp:124-172).
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -28,6 +32,13 @@ uint32_t leaf_max_setting() {
   if (!e) return kLeafMaxDefault;
   const long v = std::strtol(e, nullptr, 10);
   return (v >= 1 && v <= 32) ? static_cast<uint32_t>(v) : kLeafMaxDefault;
+}
+
+// Binary tree the BVH32 is collapsed from: PLOC clustering (default) or, with VP_WIDE_BUILDER=lbvh
+// in the environment, the Karras radix tree.
+bool wide_builder_is_ploc() {
+  const char* e = std::getenv("VP_WIDE_BUILDER");
+  return !(e && std::strcmp(e, "lbvh") == 0);
 }
 
 struct ErrorWords {
@@ -184,18 +195,27 @@ __global__ void k_morton(uint32_t n, const float* __restrict__ mean, const unsig
   idx[i] = i;
 }
 
+// Records and 3-sigma boxes in scene order (order[i] = caller index of scene position i).
 __global__ void k_gather(uint32_t n, const uint32_t* __restrict__ order, const float4* __restrict__ rec_in,
                          const float4* __restrict__ lo_in, const float4* __restrict__ hi_in,
-                         float4* __restrict__ rec_out, float4* __restrict__ lo_out,
-                         float4* __restrict__ hi_out, float4* __restrict__ pbox) {
+                         float4* __restrict__ rec_out, float4* __restrict__ pbox) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t s = order[i];
   for (int k = 0; k < 4; ++k) rec_out[4 * i + k] = rec_in[4 * s + k];
-  lo_out[i] = lo_in[s];
-  hi_out[i] = hi_in[s];
   pbox[2 * i] = lo_in[s];
   pbox[2 * i + 1] = hi_in[s];
+}
+
+// 3-sigma boxes in Morton order: the input of both tree builders.
+__global__ void k_gather_boxes(uint32_t n, const uint32_t* __restrict__ order, const float4* __restrict__ lo_in,
+                               const float4* __restrict__ hi_in, float4* __restrict__ lo_out,
+                               float4* __restrict__ hi_out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = order[i];
+  lo_out[i] = make_float4(lo_in[s].x, lo_in[s].y, lo_in[s].z, 0.f);
+  hi_out[i] = make_float4(hi_in[s].x, hi_in[s].y, hi_in[s].z, 0.f);
 }
 
 __global__ void k_gather_raw(uint32_t n, const uint32_t* __restrict__ order, const float* __restrict__ scale,
@@ -260,16 +280,19 @@ __global__ void k_karras(int n, const uint64_t* __restrict__ codes, uint32_t* __
   last[i] = hi_i;
 }
 
-__device__ __forceinline__ void child_box(uint32_t ref, const float4* plo, const float4* phi,
-                                          const float4* nlo, const float4* nhi, float4& l, float4& h) {
+// Box of a binary-tree child and the number of Gaussians under it (internal nodes keep the count
+// in hi.w).
+__device__ __forceinline__ uint32_t child_box(uint32_t ref, const float4* plo, const float4* phi,
+                                              const float4* nlo, const float4* nhi, float4& l, float4& h) {
   if (ref_is_leaf(ref)) {
     const uint32_t p = ref & ~kLeafBit;
     l = plo[p];
     h = phi[p];
-  } else {
-    l = __ldcg(nlo + ref);
-    h = __ldcg(nhi + ref);
+    return 1u;
   }
+  l = __ldcg(nlo + ref);
+  h = __ldcg(nhi + ref);
+  return __float_as_uint(h.w);
 }
 
 // Bottom-up refit: the second thread to reach an internal node unions its children.
@@ -285,37 +308,158 @@ __global__ void k_refit(int n, const uint32_t* __restrict__ left, const uint32_t
     if (atomicAdd(&flags[node], 1u) == 0u) return;
     __threadfence();
     float4 al, ah, bl, bh;
-    child_box(left[node], plo, phi, nlo, nhi, al, ah);
-    child_box(right[node], plo, phi, nlo, nhi, bl, bh);
+    const uint32_t ca = child_box(left[node], plo, phi, nlo, nhi, al, ah);
+    const uint32_t cb = child_box(right[node], plo, phi, nlo, nhi, bl, bh);
     __stcg(nlo + node, make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f));
-    __stcg(nhi + node, make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f));
+    __stcg(nhi + node, make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), __uint_as_float(ca + cb)));
     if (node == 0u) return;
     node = parent_int[node];
   }
 }
 
 // Binary-LBVH node records for the thread-per-ray megakernel: (l_lo, l_hi, r_lo, r_hi), child
-// refs in l_lo.w / r_lo.w (leaf bit | Morton-order Gaussian index).
+// refs in l_lo.w / r_lo.w (leaf bit | scene-order Gaussian index: pos maps Morton order to it).
 __global__ void k_binary_nodes(int n, const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                                const float4* __restrict__ plo, const float4* __restrict__ phi,
                                const float4* __restrict__ nlo, const float4* __restrict__ nhi,
-                               float4* __restrict__ out) {
+                               const uint32_t* __restrict__ pos, float4* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  auto scene_ref = [&](uint32_t r) { return ref_is_leaf(r) ? (kLeafBit | pos[r & ~kLeafBit]) : r; };
   float4 al, ah, bl, bh;
   child_box(left[i], plo, phi, nlo, nhi, al, ah);
   child_box(right[i], plo, phi, nlo, nhi, bl, bh);
-  al.w = __uint_as_float(left[i]);
-  bl.w = __uint_as_float(right[i]);
+  al.w = __uint_as_float(scene_ref(left[i]));
+  bl.w = __uint_as_float(scene_ref(right[i]));
+  ah.w = 0.f;
+  bh.w = 0.f;
   out[4 * i + 0] = al;
   out[4 * i + 1] = ah;
   out[4 * i + 2] = bl;
   out[4 * i + 3] = bh;
 }
 
+// ------------------------------------------------------------------------------------------
+// PLOC: Meister & Bittner, "Parallel Locally-Ordered Clustering for Bounding Volume Hierarchy
+// Construction" (IEEE TVCG 2018).  Clusters start as the Morton-sorted Gaussian boxes; every pass,
+// each cluster finds the neighbour within kPlocRadius positions whose union box has the smallest
+// surface area, mutual nearest neighbours merge into a new binary node (at the lower position),
+// and the cluster array is compacted in order.  Node ids are handed out in merge order, so the
+// root is node n - 2.
+// ------------------------------------------------------------------------------------------
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock = 256;
+
+// A cluster is (lo.xyz, ref bits in lo.w) and (hi.xyz, Gaussian count bits in hi.w); refs are
+// binary node ids or kLeafBit | Morton position.
+__global__ void k_ploc_init(uint32_t n, const float4* __restrict__ plo, const float4* __restrict__ phi,
+                            float4* __restrict__ cl, float4* __restrict__ ch) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 l = plo[i], h = phi[i];
+  l.w = __uint_as_float(kLeafBit | i);
+  h.w = __uint_as_float(1u);
+  cl[i] = l;
+  ch[i] = h;
+}
+
+// Surface area of the union of two boxes; the same value whichever box comes first, and NaN
+// (from non-finite extents) ordered as +inf, so the pair order below is a total order and the
+// globally smallest pair is always mutual (every pass merges at least once).
+__device__ __forceinline__ float union_area(float4 al, float4 ah, float4 bl, float4 bh) {
+  const float dx = fmaxf(ah.x, bh.x) - fminf(al.x, bl.x);
+  const float dy = fmaxf(ah.y, bh.y) - fminf(al.y, bl.y);
+  const float dz = fmaxf(ah.z, bh.z) - fminf(al.z, bl.z);
+  const float a = 2.f * (dx * dy + dy * dz + dz * dx);
+  return a == a ? a : INFINITY;
+}
+
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(uint32_t m, const float4* __restrict__ cl,
+                                                        const float4* __restrict__ ch, uint32_t* __restrict__ nn) {
+  __shared__ float4 sl[kPlocBlock + 2 * kPlocRadius], sh[kPlocBlock + 2 * kPlocRadius];
+  const int b0 = (int)(blockIdx.x * kPlocBlock);
+  for (int k = threadIdx.x; k < kPlocBlock + 2 * kPlocRadius; k += blockDim.x) {
+    const int g = b0 - kPlocRadius + k;
+    if (g >= 0 && g < (int)m) {
+      sl[k] = cl[g];
+      sh[k] = ch[g];
+    }
+  }
+  __syncthreads();
+  const int i = b0 + (int)threadIdx.x;
+  if (i >= (int)m) return;
+  const int c = (int)threadIdx.x + kPlocRadius;
+  const float4 al = sl[c], ah = sh[c];
+  float best = INFINITY;
+  int bj = -1;
+  for (int k = -kPlocRadius; k <= kPlocRadius; ++k) {
+    const int j = i + k;
+    if (k == 0 || j < 0 || j >= (int)m) continue;
+    const float a = union_area(al, ah, sl[c + k], sh[c + k]);
+    // pair order: area, then the pair's lower position, then its upper position
+    bool take = bj < 0 || a < best;
+    if (!take && a == best) {
+      const int lo_new = min(i, j), lo_old = min(i, bj);
+      take = lo_new < lo_old || (lo_new == lo_old && max(i, j) < max(i, bj));
+    }
+    if (take) {
+      best = a;
+      bj = j;
+    }
+  }
+  nn[i] = (uint32_t)bj;
+}
+
+// f[i] = merge << 32 | keep: the lower cluster of a mutual pair creates the node (merge) and keeps
+// its position; the upper one is absorbed (keep = 0).
+__global__ void k_ploc_flags(uint32_t m, const uint32_t* __restrict__ nn, unsigned long long* __restrict__ f) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t j = nn[i];
+  const bool mutual = nn[j] == i;
+  const unsigned long long merge = (mutual && i < j) ? 1ull : 0ull;
+  const unsigned long long keep = (mutual && i > j) ? 0ull : 1ull;
+  f[i] = (merge << 32) | keep;
+}
+
+// Writes the merged nodes and the compacted clusters; totals = (merges, clusters left).
+__global__ void k_ploc_write(uint32_t m, uint32_t node_base, const uint32_t* __restrict__ nn,
+                             const unsigned long long* __restrict__ f, const unsigned long long* __restrict__ x,
+                             const float4* __restrict__ cl, const float4* __restrict__ ch,
+                             float4* __restrict__ ol, float4* __restrict__ oh, uint32_t* __restrict__ left,
+                             uint32_t* __restrict__ right, float4* __restrict__ nlo, float4* __restrict__ nhi,
+                             uint32_t* __restrict__ totals) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const unsigned long long fi = f[i], xi = x[i];
+  if (i == m - 1u) {
+    totals[0] = (uint32_t)((xi >> 32) + (fi >> 32));
+    totals[1] = (uint32_t)(xi & 0xFFFFFFFFull) + (uint32_t)(fi & 1ull);
+  }
+  if (!(fi & 1ull)) return;
+  float4 l = cl[i], h = ch[i];
+  if (fi >> 32) {
+    const uint32_t j = nn[i];
+    const float4 bl = cl[j], bh = ch[j];
+    const uint32_t node = node_base + (uint32_t)(xi >> 32);
+    left[node] = __float_as_uint(l.w);
+    right[node] = __float_as_uint(bl.w);
+    l = make_float4(fminf(l.x, bl.x), fminf(l.y, bl.y), fminf(l.z, bl.z), __uint_as_float(node));
+    h = make_float4(fmaxf(h.x, bh.x), fmaxf(h.y, bh.y), fmaxf(h.z, bh.z),
+                    __uint_as_float(__float_as_uint(h.w) + __float_as_uint(bh.w)));
+    nlo[node] = l;
+    nhi[node] = h;
+  }
+  const uint32_t p = (uint32_t)(xi & 0xFFFFFFFFull);
+  ol[p] = l;
+  oh[p] = h;
+}
+
 struct CollapseItem {
-  uint32_t bin;   // binary internal node to expand
-  uint32_t slot;  // BVH32 node slot it becomes
+  uint32_t bin;     // binary internal node to expand
+  uint32_t slot;    // BVH32 node slot it becomes
+  uint32_t offset;  // scene position of its first Gaussian (depth-first leaf order)
+  uint32_t pad;
 };
 
 __device__ __forceinline__ float box_area(float4 l, float4 h) {
@@ -323,31 +467,39 @@ __device__ __forceinline__ float box_area(float4 l, float4 h) {
   return 2.f * (dx * dy + dy * dz + dz * dx);
 }
 
-// Greedy collapse of the binary tree into 32-wide nodes: starting from a binary node's two
-// children, repeatedly replace the largest-area child holding more than 32 Gaussians by its
-// two children until 32 slots are used.  Children with <= 32 Gaussians become leaves (one
-// contiguous Morton range, one lane per Gaussian); larger ones become the next level's nodes.
+__device__ __forceinline__ uint32_t ref_count(uint32_t r, const float4* __restrict__ nhi) {
+  return ref_is_leaf(r) ? 1u : __float_as_uint(nhi[r].w);
+}
+
+// Greedy collapse of a binary tree (Gaussian counts in nhi.w) into 32-wide nodes: starting from a
+// binary node's two children, repeatedly replace the largest-area child holding more than kLeafMax
+// Gaussians by its two children until 32 slots are used.  Children with <= kLeafMax Gaussians
+// become leaves; larger ones become the next level's nodes.  Every child carries the scene
+// position of its first Gaussian in depth-first leaf order (left subtree first), so a leaf is one
+// contiguous range of the scene order; pos[Morton position] receives each Gaussian's scene position.
 __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in,
                            CollapseItem* __restrict__ out, unsigned int* __restrict__ out_count,
                            unsigned int* __restrict__ slot_counter, const uint32_t* __restrict__ left,
-                           const uint32_t* __restrict__ right, const uint32_t* __restrict__ first,
-                           const uint32_t* __restrict__ last, const float4* __restrict__ plo,
+                           const uint32_t* __restrict__ right, const float4* __restrict__ plo,
                            const float4* __restrict__ phi, const float4* __restrict__ nlo,
-                           const float4* __restrict__ nhi, float4* __restrict__ wide, uint32_t kLeafMax) {
+                           const float4* __restrict__ nhi, float4* __restrict__ wide, uint32_t kLeafMax,
+                           uint32_t* __restrict__ pos) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_items) return;
   const CollapseItem it = in[t];
-  uint32_t refs[32];
+  uint32_t refs[32], offs[32];
   int cnt = 2;
   refs[0] = left[it.bin];
   refs[1] = right[it.bin];
+  offs[0] = it.offset;
+  offs[1] = it.offset + ref_count(refs[0], nhi);
   while (cnt < 32) {
     int best = -1;
     float best_a = -1.f;
     for (int c = 0; c < cnt; ++c) {
       const uint32_t r = refs[c];
       if (ref_is_leaf(r)) continue;
-      if (last[r] - first[r] + 1u <= kLeafMax) continue;
+      if (ref_count(r, nhi) <= kLeafMax) continue;
       const float a = box_area(nlo[r], nhi[r]);
       if (a > best_a) {
         best_a = a;
@@ -357,7 +509,9 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
     if (best < 0) break;
     const uint32_t r = refs[best];
     refs[best] = left[r];
-    refs[cnt++] = right[r];
+    refs[cnt] = right[r];
+    offs[cnt] = offs[best] + ref_count(left[r], nhi);
+    ++cnt;
   }
   float4* node = wide + (size_t)it.slot * 64u;
   for (int c = 0; c < 32; ++c) {
@@ -375,17 +529,32 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
       const uint32_t p = r & ~kLeafBit;
       l = plo[p];
       h = phi[p];
-      wref = wide_leaf_ref(p, 1u);
+      pos[p] = offs[c];
+      wref = wide_leaf_ref(offs[c], 1u);
     } else {
       l = nlo[r];
       h = nhi[r];
-      const uint32_t count = last[r] - first[r] + 1u;
+      const uint32_t count = ref_count(r, nhi);
       if (count <= kLeafMax) {
-        wref = wide_leaf_ref(first[r], count);
+        wref = wide_leaf_ref(offs[c], count);
+        // depth-first walk of the leaf's subtree (<= 32 Gaussians, so <= 32 stacked refs)
+        uint32_t st[32];
+        int sp = 0;
+        uint32_t k = offs[c];
+        st[sp++] = r;
+        while (sp > 0) {
+          const uint32_t v = st[--sp];
+          if (ref_is_leaf(v)) {
+            pos[v & ~kLeafBit] = k++;
+          } else {
+            st[sp++] = right[v];
+            st[sp++] = left[v];
+          }
+        }
       } else {
         const uint32_t slot = atomicAdd(slot_counter, 1u);
-        const uint32_t pos = atomicAdd(out_count, 1u);
-        out[pos] = CollapseItem{r, slot};
+        const uint32_t q = atomicAdd(out_count, 1u);
+        out[q] = CollapseItem{r, slot, offs[c], 0u};
         wref = slot;
       }
     }
@@ -394,6 +563,19 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
     node[c] = l;
     node[32 + c] = h;
   }
+}
+
+// Scene order from the collapse's positions: order[pos[m]] = Morton order's caller index.
+__global__ void k_compose(uint32_t n, const uint32_t* __restrict__ morton_order, const uint32_t* __restrict__ pos,
+                          uint32_t* __restrict__ order) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  order[pos[i]] = morton_order[i];
+}
+
+__global__ void k_iota(uint32_t n, uint32_t* __restrict__ v) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
 }
 
 // Root of a scene with <= 32 Gaussians: one node holding one leaf.
@@ -521,41 +703,30 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
 
   // Morton codes + radix sort (stable: ties keep the caller's order).
   Scratch<uint64_t> codes(st), codes_sorted(st);
-  Scratch<uint32_t> idx(st);
+  Scratch<uint32_t> idx(st), morton(st), pos(st);
   Scratch<unsigned char> cub_tmp(st);
-  uint32_t* perm = nullptr;
   if ((s = dev_alloc(&codes.p, n, st))) return s;
   if ((s = dev_alloc(&codes_sorted.p, n, st))) return s;
   if ((s = dev_alloc(&idx.p, n, st))) return s;
-  if ((s = dev_alloc(&perm, n, st))) return s;
-  sc->perm = perm;
+  if ((s = dev_alloc(&morton.p, n, st))) return s;
+  if ((s = dev_alloc(&pos.p, n, st))) return s;
   k_morton<<<nb, TB, 0, st>>>(n, mean, bounds.p, codes.p, idx.p);
   VP_CUDA(cudaGetLastError());
-  size_t tmp_bytes = 0;
-  VP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, codes.p, codes_sorted.p, idx.p, perm,
+  size_t sort_bytes = 0, scan_bytes = 0;
+  VP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, codes.p, codes_sorted.p, idx.p, morton.p,
                                           (int)n, 0, 63, st));
+  VP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long*)nullptr,
+                                        (unsigned long long*)nullptr, (int)n, st));
+  const size_t tmp_bytes = std::max(sort_bytes, scan_bytes);
   if ((s = dev_alloc(&cub_tmp.p, tmp_bytes, st))) return s;
-  VP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp_bytes, codes.p, codes_sorted.p, idx.p, perm,
+  VP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, sort_bytes, codes.p, codes_sorted.p, idx.p, morton.p,
                                           (int)n, 0, 63, st));
-  float4* prims = nullptr;
-  if ((s = dev_alloc(&prims, 4ull * n, st))) return s;
-  sc->prims = prims;
   if ((s = dev_alloc(&plo.p, n, st))) return s;
   if ((s = dev_alloc(&phi.p, n, st))) return s;
-  float4* pbox = nullptr;
-  if ((s = dev_alloc(&pbox, 2ull * n, st))) return s;
-  sc->pbox = pbox;
-  k_gather<<<nb, TB, 0, st>>>(n, perm, rec0.p, lo0.p, hi0.p, prims, plo.p, phi.p, pbox);
-  VP_CUDA(cudaGetLastError());
-  float4* raw = nullptr;
-  if ((s = dev_alloc(&raw, 2ull * n, st))) return s;
-  sc->raw = raw;
-  sc->scale_is_log = g->scale_is_log ? 1 : 0;
-  sc->sigma_multiplier = sigma_multiplier;
-  k_gather_raw<<<nb, TB, 0, st>>>(n, perm, scale, quat, dens, raw);
+  k_gather_boxes<<<nb, TB, 0, st>>>(n, morton.p, lo0.p, hi0.p, plo.p, phi.p);
   VP_CUDA(cudaGetLastError());
 
-  // Binary radix tree + refit.
+  // Karras radix tree + refit over the Morton order (the megakernel's binary tree).
   const uint32_t ni = n > 1 ? n - 1 : 1;
   Scratch<uint32_t> left(st), right(st), first(st), last(st), par_i(st), par_l(st);
   Scratch<float4> nlo(st), nhi(st);
@@ -569,9 +740,6 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   if ((s = dev_alloc(&nlo.p, ni, st))) return s;
   if ((s = dev_alloc(&nhi.p, ni, st))) return s;
   if ((s = dev_alloc(&flags.p, ni, st))) return s;
-  float4* bin = nullptr;
-  if ((s = dev_alloc(&bin, 4ull * ni, st))) return s;
-  sc->bin = bin;
   if (n > 1) {
     VP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned int) * ni, st));
     k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted.p, left.p, right.p, first.p, last.p,
@@ -579,18 +747,63 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     VP_CUDA(cudaGetLastError());
     k_refit<<<nb, TB, 0, st>>>((int)n, left.p, right.p, par_i.p, par_l.p, plo.p, phi.p, nlo.p, nhi.p, flags.p);
     VP_CUDA(cudaGetLastError());
-    k_binary_nodes<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, left.p, right.p, plo.p, phi.p, nlo.p, nhi.p, bin);
-    VP_CUDA(cudaGetLastError());
-  } else {
-    k_single_binary_root<<<1, 1, 0, st>>>(plo.p, phi.p, bin);
-    VP_CUDA(cudaGetLastError());
   }
 
-  // Collapse to BVH32.
+  // The warp engines' binary tree: PLOC clustering (or, with VP_WIDE_BUILDER=lbvh, the Karras tree).
+  const uint32_t kLeafMax = leaf_max_setting();
+  const bool use_ploc = n > kLeafMax && wide_builder_is_ploc();
+  Scratch<uint32_t> pleft(st), pright(st), nn(st), totals(st);
+  Scratch<float4> pnlo(st), pnhi(st), ca(st), cb(st), oa(st), ob(st);
+  Scratch<unsigned long long> fl(st), sc_x(st);
+  uint32_t wroot = 0u;
+  if (use_ploc) {
+    if ((s = dev_alloc(&pleft.p, ni, st))) return s;
+    if ((s = dev_alloc(&pright.p, ni, st))) return s;
+    if ((s = dev_alloc(&pnlo.p, ni, st))) return s;
+    if ((s = dev_alloc(&pnhi.p, ni, st))) return s;
+    if ((s = dev_alloc(&nn.p, n, st))) return s;
+    if ((s = dev_alloc(&totals.p, 2, st))) return s;
+    if ((s = dev_alloc(&ca.p, n, st))) return s;
+    if ((s = dev_alloc(&cb.p, n, st))) return s;
+    if ((s = dev_alloc(&oa.p, n, st))) return s;
+    if ((s = dev_alloc(&ob.p, n, st))) return s;
+    if ((s = dev_alloc(&fl.p, n, st))) return s;
+    if ((s = dev_alloc(&sc_x.p, n, st))) return s;
+    k_ploc_init<<<nb, TB, 0, st>>>(n, plo.p, phi.p, ca.p, cb.p);
+    VP_CUDA(cudaGetLastError());
+    uint32_t m = n, node_base = 0;
+    while (m > 1) {
+      const unsigned mb = (m + kPlocBlock - 1) / kPlocBlock;
+      k_ploc_nn<<<mb, kPlocBlock, 0, st>>>(m, ca.p, cb.p, nn.p);
+      VP_CUDA(cudaGetLastError());
+      k_ploc_flags<<<(m + TB - 1) / TB, TB, 0, st>>>(m, nn.p, fl.p);
+      VP_CUDA(cudaGetLastError());
+      size_t sb = scan_bytes;
+      VP_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, sb, fl.p, sc_x.p, (int)m, st));
+      k_ploc_write<<<(m + TB - 1) / TB, TB, 0, st>>>(m, node_base, nn.p, fl.p, sc_x.p, ca.p, cb.p, oa.p, ob.p,
+                                                     pleft.p, pright.p, pnlo.p, pnhi.p, totals.p);
+      VP_CUDA(cudaGetLastError());
+      uint32_t th[2];
+      VP_CUDA(cudaMemcpyAsync(th, totals.p, sizeof(th), cudaMemcpyDeviceToHost, st));
+      VP_CUDA(cudaStreamSynchronize(st));
+      if (th[0] == 0u || th[1] != m - th[0] || node_base + th[0] > ni)
+        return fail(VP_ERROR_INTERNAL, "PLOC clustering made no progress");
+      node_base += th[0];
+      m = th[1];
+      std::swap(ca.p, oa.p);
+      std::swap(cb.p, ob.p);
+    }
+    wroot = node_base - 1u;  // the last merge made the root (node n - 2)
+  }
+  const uint32_t* wl = use_ploc ? pleft.p : left.p;
+  const uint32_t* wr = use_ploc ? pright.p : right.p;
+  const float4* wlo = use_ploc ? pnlo.p : nlo.p;
+  const float4* whi = use_ploc ? pnhi.p : nhi.p;
+
+  // Collapse to BVH32; its depth-first leaf order defines the scene order (pos).
   // Upper bound on BVH32 nodes: childless nodes hold > L disjoint Gaussians (<= n/(L+1)), nodes
   // with one node child hold 31 leaves of their own (<= n/31), branching nodes are fewer than
   // childless ones (<= n/(L+1)).
-  const uint32_t kLeafMax = leaf_max_setting();
   const uint32_t max_wide = n / 31u + 2u * (n / (kLeafMax + 1u)) + 4u;
   float4* wide = nullptr;
   if ((s = dev_alloc(&wide, 64ull * max_wide, st))) return s;
@@ -599,13 +812,15 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   if (n <= kLeafMax) {
     k_single_leaf_root<<<1, 32, 0, st>>>(n, plo.p, phi.p, wide);
     VP_CUDA(cudaGetLastError());
+    k_iota<<<nb, TB, 0, st>>>(n, pos.p);
+    VP_CUDA(cudaGetLastError());
   } else {
     Scratch<CollapseItem> qa(st), qb(st);
     Scratch<unsigned int> ctr(st);
     if ((s = dev_alloc(&qa.p, max_wide, st))) return s;
     if ((s = dev_alloc(&qb.p, max_wide, st))) return s;
     if ((s = dev_alloc(&ctr.p, 2, st))) return s;
-    CollapseItem root{0u, 0u};
+    CollapseItem root{wroot, 0u, 0u, 0u};
     VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
     unsigned int c0[2] = {1u, 0u};  // [0] = next free slot, [1] = next-level queue length
     VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
@@ -614,8 +829,8 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     while (n_items > 0) {
       ++depth;
       VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
-      k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, left.p, right.p,
-                                                        first.p, last.p, plo.p, phi.p, nlo.p, nhi.p, wide, kLeafMax);
+      k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p,
+                                                        wlo, whi, wide, kLeafMax, pos.p);
       VP_CUDA(cudaGetLastError());
       unsigned int ch[2];
       VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
@@ -626,6 +841,38 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
       if (wide_nodes > max_wide) return fail(VP_ERROR_INTERNAL, "BVH32 node budget exceeded");
     }
   }
+
+  // Scene order, then the records, boxes and adjoint inputs gathered into it.
+  uint32_t* perm = nullptr;
+  if ((s = dev_alloc(&perm, n, st))) return s;
+  sc->perm = perm;
+  k_compose<<<nb, TB, 0, st>>>(n, morton.p, pos.p, perm);
+  VP_CUDA(cudaGetLastError());
+  float4* prims = nullptr;
+  if ((s = dev_alloc(&prims, 4ull * n, st))) return s;
+  sc->prims = prims;
+  float4* pbox = nullptr;
+  if ((s = dev_alloc(&pbox, 2ull * n, st))) return s;
+  sc->pbox = pbox;
+  k_gather<<<nb, TB, 0, st>>>(n, perm, rec0.p, lo0.p, hi0.p, prims, pbox);
+  VP_CUDA(cudaGetLastError());
+  float4* raw = nullptr;
+  if ((s = dev_alloc(&raw, 2ull * n, st))) return s;
+  sc->raw = raw;
+  sc->scale_is_log = g->scale_is_log ? 1 : 0;
+  sc->sigma_multiplier = sigma_multiplier;
+  k_gather_raw<<<nb, TB, 0, st>>>(n, perm, scale, quat, dens, raw);
+  VP_CUDA(cudaGetLastError());
+  float4* bin = nullptr;
+  if ((s = dev_alloc(&bin, 4ull * ni, st))) return s;
+  sc->bin = bin;
+  if (n > 1) {
+    k_binary_nodes<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, left.p, right.p, plo.p, phi.p, nlo.p, nhi.p, pos.p,
+                                                      bin);
+  } else {
+    k_single_binary_root<<<1, 1, 0, st>>>(plo.p, phi.p, bin);
+  }
+  VP_CUDA(cudaGetLastError());
   if (wide_nodes < max_wide) {  // keep only the nodes in use
     float4* tight = nullptr;
     if ((s = dev_alloc(&tight, 64ull * wide_nodes, st))) return s;

@@ -40,8 +40,9 @@ constexpr float kExpMinus4p5 = 0.011108996538242306f;    // exp(-9/2): the integ
 // Warp-cooperative visit of every Gaussian whose 3-sigma chord overlaps [0, inf) of the ray.  The
 // warp walks the BVH32 with the first hit child of each inner node kept in registers and the
 // others on the warp's shared-memory stack (no ordering: the image model is order-independent).
-// At a leaf, lane j takes the leaf's j-th Gaussian: box pre-test, chord set-up, then f(pi, g, ch)
-// on that lane alone.
+// At a leaf (packed with the leaves next on the stack while they fit in 32 lanes), lane j takes the
+// j-th Gaussian of the ranges laid end to end: box pre-test, chord set-up, then f(pi, g, ch) on
+// that lane alone.
 template <bool kAcc, class F>
 __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3 d, uint32_t& status, F&& f) {
   const int lane = threadIdx.x & 31;
@@ -58,8 +59,19 @@ __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3
     }
     have = false;
     if (ref_is_leaf(ref)) {
-      const int total = (int)wide_leaf_count(ref);
-      const uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
+      // leaves next on the stack join this step while their Gaussians fit in the 32 lanes
+      int total = (int)wide_leaf_count(ref);
+      uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
+      while (VP_LEAF_PACK && sp > 0) {
+        const uint32_t r2 = stack[sp - 1];
+        if (!ref_is_leaf(r2)) break;
+        const int c2 = (int)wide_leaf_count(r2);
+        if (total + c2 > 32) break;
+        --sp;
+        if (lane >= total && lane < total + c2) pi = wide_leaf_first(r2) + (uint32_t)(lane - total);
+        total += c2;
+      }
+      __syncwarp();
       if (lane < total) {
         float tb;
         if (slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, kInf, tb)) {

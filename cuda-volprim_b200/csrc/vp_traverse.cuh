@@ -14,6 +14,12 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kHitCap = VP_HIT_CAP;  // hit-buffer entries per warp (retained chords + one step's new ones)
 constexpr int kBinStack = 128; // thread-private stack of the binary traversal
 
+// Leaf packing in the warp traversals (1 = on): a leaf step also takes the leaves next on the
+// stack while their Gaussians fit in the 32 lanes.
+#ifndef VP_LEAF_PACK
+#define VP_LEAF_PACK 1
+#endif
+
 // Resident 256-thread blocks per SM the warp engine's register budget is sized for.
 #ifndef VP_WARP_MIN_BLOCKS
 #define VP_WARP_MIN_BLOCKS 4
@@ -174,16 +180,32 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     have = false;
     if (tn > t_hi) continue;
     if (ref_is_leaf(ref)) {
-      const int total = (int)wide_leaf_count(ref);
+      // Leaf packing: the leaves next on the stack join this step while their Gaussians fit in
+      // the warp's 32 lanes (lane -> Gaussian: the ranges laid end to end).
+      int total = (int)wide_leaf_count(ref);
+      uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
+      int packed = 1;
+      while (VP_LEAF_PACK && sp > 0) {
+        const uint32_t r2 = W.st_ref[sp - 1];
+        if (!ref_is_leaf(r2)) break;
+        const int c2 = (int)wide_leaf_count(r2);
+        if (total + c2 > 32) break;
+        const float t2 = W.st_t[sp - 1];
+        --sp;
+        if (t2 > t_hi) continue;  // culled, as it would be when popped
+        if (lane >= total && lane < total + c2) pi = wide_leaf_first(r2) + (uint32_t)(lane - total);
+        total += c2;
+        ++packed;
+      }
+      __syncwarp();
       if (measure) {
-        ws.leaves++;
-        ws.kind_leaves[kKind]++;
+        ws.leaves += packed;
+        ws.kind_leaves[kKind] += packed;
         ws.kind_prims[kKind] += total;
       }
       bool hit = false;
       Chord ch;
       float icf = 0.f;
-      const uint32_t pi = wide_leaf_first(ref) + (uint32_t)lane;
       bool boxed = false;
       if (lane < total && pi != seed) {  // the Gaussian's own 3-sigma box first (32 B), then its record
         float tb;
