@@ -23,9 +23,10 @@
 namespace vp {
 namespace {
 
-// Gaussians per BVH32 leaf (at most one per lane).  Smaller leaves have tighter bounds; the warp
-// traversal tests several small leaves in one step.  VP_LEAF_MAX in the environment overrides it.
-constexpr uint32_t kLeafMaxDefault = 32;
+// Largest BVH32 leaf (at most one Gaussian per lane).  Smaller leaves have tighter bounds, and the
+// warp traversal packs several small leaves into one step.  VP_LEAF_MAX in the environment
+// overrides it.
+constexpr uint32_t kLeafMaxDefault = 24;
 
 uint32_t leaf_max_setting() {
   const char* e = std::getenv("VP_LEAF_MAX");
@@ -347,7 +348,7 @@ __global__ void k_binary_nodes(int n, const uint32_t* __restrict__ left, const u
 // and the cluster array is compacted in order.  Node ids are handed out in merge order, so the
 // root is node n - 2.
 // ------------------------------------------------------------------------------------------
-constexpr int kPlocRadius = 16;
+constexpr int kPlocRadius = 32;
 constexpr int kPlocBlock = 256;
 
 // A cluster is (lo.xyz, ref bits in lo.w) and (hi.xyz, Gaussian count bits in hi.w); refs are
@@ -374,10 +375,16 @@ __device__ __forceinline__ float union_area(float4 al, float4 ah, float4 bl, flo
   return a == a ? a : INFINITY;
 }
 
-__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(uint32_t m, const float4* __restrict__ cl,
+// The pass kernels take the live cluster count from ctr_in = (clusters, nodes made so far), written
+// by the previous pass, so a run of passes needs no host round trip; grids cover an upper bound.
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const uint32_t* __restrict__ ctr_in,
+                                                        const float4* __restrict__ cl,
                                                         const float4* __restrict__ ch, uint32_t* __restrict__ nn) {
   __shared__ float4 sl[kPlocBlock + 2 * kPlocRadius], sh[kPlocBlock + 2 * kPlocRadius];
+  const uint32_t m = ctr_in[0];
+  if (m < 2u) return;
   const int b0 = (int)(blockIdx.x * kPlocBlock);
+  if (b0 >= (int)m) return;
   for (int k = threadIdx.x; k < kPlocBlock + 2 * kPlocRadius; k += blockDim.x) {
     const int g = b0 - kPlocRadius + k;
     if (g >= 0 && g < (int)m) {
@@ -412,9 +419,17 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(uint32_t m, const float4
 
 // f[i] = merge << 32 | keep: the lower cluster of a mutual pair creates the node (merge) and keeps
 // its position; the upper one is absorbed (keep = 0).
-__global__ void k_ploc_flags(uint32_t m, const uint32_t* __restrict__ nn, unsigned long long* __restrict__ f) {
+// Entries in [m, bound) are 0 so that the scan may run over the grid's upper bound; a lone
+// cluster (m == 1) just keeps its place.
+__global__ void k_ploc_flags(uint32_t bound, const uint32_t* __restrict__ ctr_in, const uint32_t* __restrict__ nn,
+                             unsigned long long* __restrict__ f) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+  if (i >= bound) return;
+  const uint32_t m = ctr_in[0];
+  if (i >= m || m < 2u) {
+    f[i] = (i == 0u && m == 1u) ? 1ull : 0ull;
+    return;
+  }
   const uint32_t j = nn[i];
   const bool mutual = nn[j] == i;
   const unsigned long long merge = (mutual && i < j) ? 1ull : 0ull;
@@ -422,19 +437,20 @@ __global__ void k_ploc_flags(uint32_t m, const uint32_t* __restrict__ nn, unsign
   f[i] = (merge << 32) | keep;
 }
 
-// Writes the merged nodes and the compacted clusters; totals = (merges, clusters left).
-__global__ void k_ploc_write(uint32_t m, uint32_t node_base, const uint32_t* __restrict__ nn,
-                             const unsigned long long* __restrict__ f, const unsigned long long* __restrict__ x,
-                             const float4* __restrict__ cl, const float4* __restrict__ ch,
-                             float4* __restrict__ ol, float4* __restrict__ oh, uint32_t* __restrict__ left,
-                             uint32_t* __restrict__ right, float4* __restrict__ nlo, float4* __restrict__ nhi,
-                             uint32_t* __restrict__ totals) {
+// Writes the merged nodes and the compacted clusters; ctr_out = (clusters left, nodes made).
+__global__ void k_ploc_write(const uint32_t* __restrict__ ctr_in, uint32_t* __restrict__ ctr_out,
+                             const uint32_t* __restrict__ nn, const unsigned long long* __restrict__ f,
+                             const unsigned long long* __restrict__ x, const float4* __restrict__ cl,
+                             const float4* __restrict__ ch, float4* __restrict__ ol, float4* __restrict__ oh,
+                             uint32_t* __restrict__ left, uint32_t* __restrict__ right, float4* __restrict__ nlo,
+                             float4* __restrict__ nhi) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t m = ctr_in[0], node_base = ctr_in[1];
   if (i >= m) return;
   const unsigned long long fi = f[i], xi = x[i];
   if (i == m - 1u) {
-    totals[0] = (uint32_t)((xi >> 32) + (fi >> 32));
-    totals[1] = (uint32_t)(xi & 0xFFFFFFFFull) + (uint32_t)(fi & 1ull);
+    ctr_out[0] = (uint32_t)(xi & 0xFFFFFFFFull) + (uint32_t)(fi & 1ull);
+    ctr_out[1] = node_base + (uint32_t)((xi >> 32) + (fi >> 32));
   }
   if (!(fi & 1ull)) return;
   float4 l = cl[i], h = ch[i];
@@ -762,7 +778,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     if ((s = dev_alloc(&pnlo.p, ni, st))) return s;
     if ((s = dev_alloc(&pnhi.p, ni, st))) return s;
     if ((s = dev_alloc(&nn.p, n, st))) return s;
-    if ((s = dev_alloc(&totals.p, 2, st))) return s;
+    if ((s = dev_alloc(&totals.p, 4, st))) return s;
     if ((s = dev_alloc(&ca.p, n, st))) return s;
     if ((s = dev_alloc(&cb.p, n, st))) return s;
     if ((s = dev_alloc(&oa.p, n, st))) return s;
@@ -771,28 +787,40 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     if ((s = dev_alloc(&sc_x.p, n, st))) return s;
     k_ploc_init<<<nb, TB, 0, st>>>(n, plo.p, phi.p, ca.p, cb.p);
     VP_CUDA(cudaGetLastError());
-    uint32_t m = n, node_base = 0;
-    while (m > 1) {
-      const unsigned mb = (m + kPlocBlock - 1) / kPlocBlock;
-      k_ploc_nn<<<mb, kPlocBlock, 0, st>>>(m, ca.p, cb.p, nn.p);
-      VP_CUDA(cudaGetLastError());
-      k_ploc_flags<<<(m + TB - 1) / TB, TB, 0, st>>>(m, nn.p, fl.p);
-      VP_CUDA(cudaGetLastError());
-      size_t sb = scan_bytes;
-      VP_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, sb, fl.p, sc_x.p, (int)m, st));
-      k_ploc_write<<<(m + TB - 1) / TB, TB, 0, st>>>(m, node_base, nn.p, fl.p, sc_x.p, ca.p, cb.p, oa.p, ob.p,
-                                                     pleft.p, pright.p, pnlo.p, pnhi.p, totals.p);
-      VP_CUDA(cudaGetLastError());
-      uint32_t th[2];
-      VP_CUDA(cudaMemcpyAsync(th, totals.p, sizeof(th), cudaMemcpyDeviceToHost, st));
-      VP_CUDA(cudaStreamSynchronize(st));
-      if (th[0] == 0u || th[1] != m - th[0] || node_base + th[0] > ni)
-        return fail(VP_ERROR_INTERNAL, "PLOC clustering made no progress");
-      node_base += th[0];
-      m = th[1];
-      std::swap(ca.p, oa.p);
-      std::swap(cb.p, ob.p);
+    {
+      const uint32_t c0[4] = {n, 0u, n, 0u};
+      VP_CUDA(cudaMemcpyAsync(totals.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
     }
+    // Passes run in chunks between host reads of the count; the count only falls, so the last
+    // value read bounds the grids of the next chunk.
+    constexpr int kChunk = 8;
+    uint32_t m = n, made = 0u;
+    int pass = 0;
+    while (m > 1u) {
+      for (int k = 0; k < kChunk; ++k, ++pass) {
+        const uint32_t* cin = totals.p + 2 * (pass & 1);
+        uint32_t* cout = totals.p + 2 * ((pass + 1) & 1);
+        k_ploc_nn<<<(m + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(cin, ca.p, cb.p, nn.p);
+        VP_CUDA(cudaGetLastError());
+        k_ploc_flags<<<(m + TB - 1) / TB, TB, 0, st>>>(m, cin, nn.p, fl.p);
+        VP_CUDA(cudaGetLastError());
+        size_t sb = scan_bytes;
+        VP_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, sb, fl.p, sc_x.p, (int)m, st));
+        k_ploc_write<<<(m + TB - 1) / TB, TB, 0, st>>>(cin, cout, nn.p, fl.p, sc_x.p, ca.p, cb.p, oa.p, ob.p,
+                                                       pleft.p, pright.p, pnlo.p, pnhi.p);
+        VP_CUDA(cudaGetLastError());
+        std::swap(ca.p, oa.p);
+        std::swap(cb.p, ob.p);
+      }
+      uint32_t th[2];
+      VP_CUDA(cudaMemcpyAsync(th, totals.p + 2 * (pass & 1), sizeof(th), cudaMemcpyDeviceToHost, st));
+      VP_CUDA(cudaStreamSynchronize(st));
+      if (th[0] >= m && m > 1u) return fail(VP_ERROR_INTERNAL, "PLOC clustering made no progress");
+      if (th[0] + th[1] != n || th[1] > ni) return fail(VP_ERROR_INTERNAL, "PLOC clustering lost a cluster");
+      m = th[0];
+      made = th[1];
+    }
+    const uint32_t node_base = made;
     wroot = node_base - 1u;  // the last merge made the root (node n - 2)
   }
   const uint32_t* wl = use_ploc ? pleft.p : left.p;
