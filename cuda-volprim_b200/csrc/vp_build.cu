@@ -23,25 +23,6 @@
 namespace vp {
 namespace {
 
-// Largest BVH32 leaf (at most one Gaussian per lane).  Smaller leaves have tighter bounds, and the
-// warp traversal packs several small leaves into one step.  VP_LEAF_MAX in the environment
-// overrides it.
-constexpr uint32_t kLeafMaxDefault = 24;
-
-uint32_t leaf_max_setting() {
-  const char* e = std::getenv("VP_LEAF_MAX");
-  if (!e) return kLeafMaxDefault;
-  const long v = std::strtol(e, nullptr, 10);
-  return (v >= 1 && v <= 32) ? static_cast<uint32_t>(v) : kLeafMaxDefault;
-}
-
-// Binary tree the BVH32 is collapsed from: PLOC clustering (default) or, with VP_WIDE_BUILDER=lbvh
-// in the environment, the Karras radix tree.
-bool wide_builder_is_ploc() {
-  const char* e = std::getenv("VP_WIDE_BUILDER");
-  return !(e && std::strcmp(e, "lbvh") == 0);
-}
-
 struct ErrorWords {
   int bad_scale, bad_density, bad_center;  // lowest failing index (INT_MAX = none)
   unsigned int any_albedo;                 // 1 if some albedo component > 0
@@ -437,7 +418,8 @@ __global__ void k_ploc_flags(uint32_t bound, const uint32_t* __restrict__ ctr_in
   f[i] = (merge << 32) | keep;
 }
 
-// Writes the merged nodes and the compacted clusters; ctr_out = (clusters left, nodes made).
+// Writes the merged nodes (Gaussian count in nhi.w, height in nlo.w) and the compacted clusters;
+// ctr_out = (clusters left, nodes made).
 __global__ void k_ploc_write(const uint32_t* __restrict__ ctr_in, uint32_t* __restrict__ ctr_out,
                              const uint32_t* __restrict__ nn, const unsigned long long* __restrict__ f,
                              const unsigned long long* __restrict__ x, const float4* __restrict__ cl,
@@ -458,12 +440,16 @@ __global__ void k_ploc_write(const uint32_t* __restrict__ ctr_in, uint32_t* __re
     const uint32_t j = nn[i];
     const float4 bl = cl[j], bh = ch[j];
     const uint32_t node = node_base + (uint32_t)(xi >> 32);
-    left[node] = __float_as_uint(l.w);
-    right[node] = __float_as_uint(bl.w);
+    const uint32_t lref = __float_as_uint(l.w), rref = __float_as_uint(bl.w);
+    left[node] = lref;
+    right[node] = rref;
+    // node height (leaf refs 0) in nlo.w: the children were made in earlier passes
+    const uint32_t hl = ref_is_leaf(lref) ? 0u : __float_as_uint(nlo[lref].w);
+    const uint32_t hr = ref_is_leaf(rref) ? 0u : __float_as_uint(nlo[rref].w);
     l = make_float4(fminf(l.x, bl.x), fminf(l.y, bl.y), fminf(l.z, bl.z), __uint_as_float(node));
     h = make_float4(fmaxf(h.x, bh.x), fmaxf(h.y, bh.y), fmaxf(h.z, bh.z),
                     __uint_as_float(__float_as_uint(h.w) + __float_as_uint(bh.w)));
-    nlo[node] = l;
+    nlo[node] = make_float4(l.x, l.y, l.z, __uint_as_float(1u + max(hl, hr)));
     nhi[node] = h;
   }
   const uint32_t p = (uint32_t)(xi & 0xFFFFFFFFull);
@@ -499,7 +485,7 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
                            const uint32_t* __restrict__ right, const float4* __restrict__ plo,
                            const float4* __restrict__ phi, const float4* __restrict__ nlo,
                            const float4* __restrict__ nhi, float4* __restrict__ wide, uint32_t kLeafMax,
-                           uint32_t* __restrict__ pos) {
+                           uint32_t* __restrict__ pos, unsigned int* __restrict__ leaf_counter) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_items) return;
   const CollapseItem it = in[t];
@@ -547,12 +533,14 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
       h = phi[p];
       pos[p] = offs[c];
       wref = wide_leaf_ref(offs[c], 1u);
+      atomicAdd(leaf_counter, 1u);
     } else {
       l = nlo[r];
       h = nhi[r];
       const uint32_t count = ref_count(r, nhi);
       if (count <= kLeafMax) {
         wref = wide_leaf_ref(offs[c], count);
+        atomicAdd(leaf_counter, 1u);
         // depth-first walk of the leaf's subtree (<= 32 Gaussians, so <= 32 stacked refs)
         uint32_t st[32];
         int sp = 0;
@@ -636,7 +624,8 @@ struct Scratch {  // stream-ordered temporary, freed on scope exit
 
 }  // namespace
 
-vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene* sc) {
+vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, const vp_scene_options& opt,
+                      vp_scene* sc) {
   cudaStream_t st = ctx->stream;
   const uint32_t n = g->count;
   if (n == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "scene has no Gaussians");
@@ -742,36 +731,16 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   k_gather_boxes<<<nb, TB, 0, st>>>(n, morton.p, lo0.p, hi0.p, plo.p, phi.p);
   VP_CUDA(cudaGetLastError());
 
-  // Karras radix tree + refit over the Morton order (the megakernel's binary tree).
+  // PLOC clustering: the binary tree of the BVH32 and of the megakernel unless the options ask for
+  // the Karras tree for both (a BVH32 that is a single leaf needs no tree).
   const uint32_t ni = n > 1 ? n - 1 : 1;
-  Scratch<uint32_t> left(st), right(st), first(st), last(st), par_i(st), par_l(st);
-  Scratch<float4> nlo(st), nhi(st);
-  Scratch<unsigned int> flags(st);
-  if ((s = dev_alloc(&left.p, ni, st))) return s;
-  if ((s = dev_alloc(&right.p, ni, st))) return s;
-  if ((s = dev_alloc(&first.p, ni, st))) return s;
-  if ((s = dev_alloc(&last.p, ni, st))) return s;
-  if ((s = dev_alloc(&par_i.p, ni, st))) return s;
-  if ((s = dev_alloc(&par_l.p, n, st))) return s;
-  if ((s = dev_alloc(&nlo.p, ni, st))) return s;
-  if ((s = dev_alloc(&nhi.p, ni, st))) return s;
-  if ((s = dev_alloc(&flags.p, ni, st))) return s;
-  if (n > 1) {
-    VP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned int) * ni, st));
-    k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted.p, left.p, right.p, first.p, last.p,
-                                                par_i.p, par_l.p);
-    VP_CUDA(cudaGetLastError());
-    k_refit<<<nb, TB, 0, st>>>((int)n, left.p, right.p, par_i.p, par_l.p, plo.p, phi.p, nlo.p, nhi.p, flags.p);
-    VP_CUDA(cudaGetLastError());
-  }
-
-  // The warp engines' binary tree: PLOC clustering (or, with VP_WIDE_BUILDER=lbvh, the Karras tree).
-  const uint32_t kLeafMax = leaf_max_setting();
-  const bool use_ploc = n > kLeafMax && wide_builder_is_ploc();
+  const uint32_t kLeafMax = opt.leaf_max;
+  const bool wide_ploc = n > kLeafMax && opt.wide_builder == VP_TREE_PLOC;
+  const bool use_ploc = n > 1u && (wide_ploc || opt.binary_builder == VP_TREE_PLOC);
   Scratch<uint32_t> pleft(st), pright(st), nn(st), totals(st);
   Scratch<float4> pnlo(st), pnhi(st), ca(st), cb(st), oa(st), ob(st);
   Scratch<unsigned long long> fl(st), sc_x(st);
-  uint32_t wroot = 0u;
+  uint32_t wroot = 0u, ploc_height = 0u;
   if (use_ploc) {
     if ((s = dev_alloc(&pleft.p, ni, st))) return s;
     if ((s = dev_alloc(&pright.p, ni, st))) return s;
@@ -822,11 +791,44 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     }
     const uint32_t node_base = made;
     wroot = node_base - 1u;  // the last merge made the root (node n - 2)
+    float4 root_lo;
+    VP_CUDA(cudaMemcpyAsync(&root_lo, pnlo.p + wroot, sizeof(root_lo), cudaMemcpyDeviceToHost, st));
+    VP_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(&ploc_height, &root_lo.w, sizeof(ploc_height));
   }
-  const uint32_t* wl = use_ploc ? pleft.p : left.p;
-  const uint32_t* wr = use_ploc ? pright.p : right.p;
-  const float4* wlo = use_ploc ? pnlo.p : nlo.p;
-  const float4* whi = use_ploc ? pnhi.p : nhi.p;
+  // Karras radix tree + refit over the Morton order: the BVH32's source when the options ask for it,
+  // and the megakernel's binary tree when they ask for it or the PLOC tree is deeper than the
+  // megakernel's thread-private stack.
+  Scratch<uint32_t> left(st), right(st), first(st), last(st), par_i(st), par_l(st);
+  Scratch<float4> nlo(st), nhi(st);
+  Scratch<unsigned int> flags(st);
+  const bool bin_from_ploc = use_ploc && opt.binary_builder == VP_TREE_PLOC && ploc_height + 1u < (uint32_t)kBinStack;
+  const bool need_karras = !wide_ploc || !bin_from_ploc;
+  if (need_karras) {
+    if ((s = dev_alloc(&left.p, ni, st))) return s;
+    if ((s = dev_alloc(&right.p, ni, st))) return s;
+    if ((s = dev_alloc(&first.p, ni, st))) return s;
+    if ((s = dev_alloc(&last.p, ni, st))) return s;
+    if ((s = dev_alloc(&par_i.p, ni, st))) return s;
+    if ((s = dev_alloc(&par_l.p, n, st))) return s;
+    if ((s = dev_alloc(&nlo.p, ni, st))) return s;
+    if ((s = dev_alloc(&nhi.p, ni, st))) return s;
+    if ((s = dev_alloc(&flags.p, ni, st))) return s;
+    if (n > 1) {
+      VP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned int) * ni, st));
+      k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted.p, left.p, right.p, first.p, last.p,
+                                                  par_i.p, par_l.p);
+      VP_CUDA(cudaGetLastError());
+      k_refit<<<nb, TB, 0, st>>>((int)n, left.p, right.p, par_i.p, par_l.p, plo.p, phi.p, nlo.p, nhi.p, flags.p);
+      VP_CUDA(cudaGetLastError());
+    }
+  }
+
+  const uint32_t wide_root = wide_ploc ? wroot : 0u;
+  const uint32_t* wl = wide_ploc ? pleft.p : left.p;
+  const uint32_t* wr = wide_ploc ? pright.p : right.p;
+  const float4* wlo = wide_ploc ? pnlo.p : nlo.p;
+  const float4* whi = wide_ploc ? pnhi.p : nhi.p;
 
   // Collapse to BVH32; its depth-first leaf order defines the scene order (pos).
   // Upper bound on BVH32 nodes: childless nodes hold > L disjoint Gaussians (<= n/(L+1)), nodes
@@ -836,7 +838,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   float4* wide = nullptr;
   if ((s = dev_alloc(&wide, 64ull * max_wide, st))) return s;
   sc->wide = wide;
-  uint32_t depth = 1, wide_nodes = 1;
+  uint32_t depth = 1, wide_nodes = 1, leaves = 1;
   if (n <= kLeafMax) {
     k_single_leaf_root<<<1, 32, 0, st>>>(n, plo.p, phi.p, wide);
     VP_CUDA(cudaGetLastError());
@@ -847,10 +849,10 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     Scratch<unsigned int> ctr(st);
     if ((s = dev_alloc(&qa.p, max_wide, st))) return s;
     if ((s = dev_alloc(&qb.p, max_wide, st))) return s;
-    if ((s = dev_alloc(&ctr.p, 2, st))) return s;
-    CollapseItem root{wroot, 0u, 0u, 0u};
+    if ((s = dev_alloc(&ctr.p, 3, st))) return s;
+    CollapseItem root{wide_root, 0u, 0u, 0u};
     VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
-    unsigned int c0[2] = {1u, 0u};  // [0] = next free slot, [1] = next-level queue length
+    unsigned int c0[3] = {1u, 0u, 0u};  // next free slot, next-level queue length, leaves
     VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
     uint32_t n_items = 1;
     depth = 0;
@@ -858,13 +860,14 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
       ++depth;
       VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
       k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p,
-                                                        wlo, whi, wide, kLeafMax, pos.p);
+                                                        wlo, whi, wide, kLeafMax, pos.p, ctr.p + 2);
       VP_CUDA(cudaGetLastError());
-      unsigned int ch[2];
+      unsigned int ch[3];
       VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
       VP_CUDA(cudaStreamSynchronize(st));
       n_items = ch[1];
       wide_nodes = ch[0];
+      leaves = ch[2];
       std::swap(qa.p, qb.p);
       if (wide_nodes > max_wide) return fail(VP_ERROR_INTERNAL, "BVH32 node budget exceeded");
     }
@@ -894,7 +897,12 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   float4* bin = nullptr;
   if ((s = dev_alloc(&bin, 4ull * ni, st))) return s;
   sc->bin = bin;
-  if (n > 1) {
+  uint32_t bin_root = 0u;
+  if (bin_from_ploc) {
+    k_binary_nodes<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, pleft.p, pright.p, plo.p, phi.p, pnlo.p, pnhi.p, pos.p,
+                                                      bin);
+    bin_root = wroot;
+  } else if (n > 1) {
     k_binary_nodes<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, left.p, right.p, plo.p, phi.p, nlo.p, nhi.p, pos.p,
                                                       bin);
   } else {
@@ -923,7 +931,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   v.pbox = pbox;
   v.count = n;
   v.wide_root = 0u;
-  v.bin_root = 0u;
+  v.bin_root = bin_root;
   v.stack_cap = 31u * depth + 2u;
   v.albedo_all_zero = eh.any_albedo ? 0 : 1;
   vp_scene_info& info = sc->info;
@@ -931,7 +939,11 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   info.wide_nodes = wide_nodes;
   info.wide_depth = depth;
   info.binary_nodes = n > 1 ? n - 1 : 1;
-  info.leaves = 0;
+  info.leaves = leaves;
+  info.wide_builder = n <= kLeafMax ? opt.wide_builder : (wide_ploc ? VP_TREE_PLOC : VP_TREE_LBVH);
+  info.binary_builder = bin_from_ploc ? VP_TREE_PLOC : VP_TREE_LBVH;
+  info.binary_height = ploc_height;
+  info.leaf_max = kLeafMax;
   info.albedo_all_zero = v.albedo_all_zero;
   info.build_ms = ms;
   for (int k = 0; k < 3; ++k) {

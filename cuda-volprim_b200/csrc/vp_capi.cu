@@ -240,14 +240,29 @@ vp_status vp_context_sm_count(vp_context* c, int32_t* out) {
   return VP_OK;
 }
 
-vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene** out) {
+vp_status vp_scene_options_default(vp_scene_options* out) {
+  if (!out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  *out = vp_scene_options{VP_TREE_PLOC, VP_TREE_PLOC, 24u, 0u};
+  return VP_OK;
+}
+
+vp_status vp_scene_create_ex(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier,
+                             const vp_scene_options* options, vp_scene** out) {
   if (!ctx || !g || !out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
   *out = nullptr;
+  vp_scene_options opt;
+  vp_scene_options_default(&opt);
+  if (options) opt = *options;
+  auto builder_ok = [](int32_t b) { return b == VP_TREE_PLOC || b == VP_TREE_LBVH; };
+  if (!builder_ok(opt.wide_builder) || !builder_ok(opt.binary_builder))
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options: builders must be VP_TREE_PLOC or VP_TREE_LBVH");
+  if (opt.leaf_max < 1u || opt.leaf_max > 32u)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.leaf_max must be in [1, 32]");
   VP_CUDA(cudaSetDevice(ctx->device));
   auto* s = new (std::nothrow) vp_scene();
   if (!s) return fail(VP_ERROR_OUT_OF_MEMORY, "host allocation failed");
   s->ctx = ctx;
-  const vp_status st = build_scene(ctx, g, sigma_multiplier, s);
+  const vp_status st = build_scene(ctx, g, sigma_multiplier, opt, s);
   if (st != VP_OK) {
     const std::string msg = g_last_error;
     vp_scene_destroy(s);
@@ -256,6 +271,10 @@ vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* g, float sigma_mu
   }
   *out = s;
   return VP_OK;
+}
+
+vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene** out) {
+  return vp_scene_create_ex(ctx, g, sigma_multiplier, nullptr, out);
 }
 
 vp_status vp_scene_info_get(vp_scene* s, vp_scene_info* out) {

@@ -43,6 +43,9 @@ constexpr float kInvSqrt2 = 1.0f / 1.41421356237309504880f;
 constexpr uint32_t kEmptyRef = 0xFFFFFFFFu;
 constexpr uint32_t kNoGauss = 0xFFFFFFFFu;  // no Gaussian (scene order)
 constexpr uint32_t kLeafBit = 0x80000000u;
+// Thread-private stack of the binary-tree traversal (megakernel); the scene build keeps the
+// binary tree's height below it.
+constexpr int kBinStack = 128;
 __host__ __device__ inline bool ref_is_leaf(uint32_t r) { return (r & kLeafBit) != 0u; }
 // BVH32 leaf: bit31 | (count-1) << 26 | first
 __host__ __device__ inline uint32_t wide_leaf_ref(uint32_t first, uint32_t count) {

@@ -121,7 +121,8 @@ struct vp_image {
 };
 
 namespace vp {
-vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, vp_scene* s);
+vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, const vp_scene_options& opt,
+                      vp_scene* s);
 vp_status build_env(vp_context* ctx, const float* rgb, uint32_t w, uint32_t h, uint32_t channels,
                     int32_t memory, vp_env* env);
 // Host restatement of host::params::Camera::build (camera.h:106-177).

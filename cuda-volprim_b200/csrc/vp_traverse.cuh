@@ -12,7 +12,6 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 #define VP_HIT_CAP 128
 #endif
 constexpr int kHitCap = VP_HIT_CAP;  // hit-buffer entries per warp (retained chords + one step's new ones)
-constexpr int kBinStack = 128; // thread-private stack of the binary traversal
 
 // Leaf packing in the warp traversals (1 = on): a leaf step also takes the leaves next on the
 // stack while their Gaussians fit in the 32 lanes.

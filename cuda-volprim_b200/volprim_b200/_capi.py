@@ -17,6 +17,7 @@ VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL, VP_ENGINE_WAVEFRONT = 0, 1, 2
 VP_PRECISION_AUTO, VP_PRECISION_FAST, VP_PRECISION_ACCURATE = 0, 1, 2
 VP_MEASURE_COUNTERS, VP_MEASURE_STAGES = 1, 2
 VP_SCHEDULE_FIFO, VP_SCHEDULE_FAIR, VP_SCHEDULE_SRPT = 0, 1, 2
+VP_TREE_PLOC, VP_TREE_LBVH = 0, 1
 
 ERROR_NAMES = {
     -1: "VP_ERROR_INVALID_ARGUMENT", -2: "VP_ERROR_CUDA", -3: "VP_ERROR_OUT_OF_MEMORY",
@@ -58,6 +59,19 @@ class vp_scene_info(C.Structure):
         ("bounds_min", C.c_double * 3),
         ("bounds_max", C.c_double * 3),
         ("device_bytes", C.c_uint64),
+        ("wide_builder", C.c_int32),
+        ("binary_builder", C.c_int32),
+        ("binary_height", C.c_uint32),
+        ("leaf_max", C.c_uint32),
+    ]
+
+
+class vp_scene_options(C.Structure):
+    _fields_ = [
+        ("wide_builder", C.c_int32),
+        ("binary_builder", C.c_int32),
+        ("leaf_max", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -200,6 +214,8 @@ SIGNATURES = {
     "vp_context_synchronize": [P],
     "vp_context_sm_count": [P, C.POINTER(C.c_int32)],
     "vp_scene_create": [P, C.POINTER(vp_gaussians), C.c_float, PP],
+    "vp_scene_options_default": [C.POINTER(vp_scene_options)],
+    "vp_scene_create_ex": [P, C.POINTER(vp_gaussians), C.c_float, C.POINTER(vp_scene_options), PP],
     "vp_scene_info_get": [P, C.POINTER(vp_scene_info)],
     "vp_scene_destroy": [P],
     "vp_env_create": [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, PP],

@@ -114,11 +114,25 @@ class Gaussians:
         return int(self.density.shape[0]) if hasattr(self.density, "shape") else len(self.density)
 
 
-class Scene:
-    """Gaussians + acceleration structure on the device (vp_scene_create)."""
+_BUILDERS = {"ploc": _capi.VP_TREE_PLOC, "lbvh": _capi.VP_TREE_LBVH}
 
-    def __init__(self, ctx: Context, g: Gaussians, sigma_multiplier: float = 1.0):
+
+class Scene:
+    """Gaussians + acceleration structure on the device (vp_scene_create_ex).
+
+    wide_builder / binary_builder pick the binary tree of the BVH32 (warp and wavefront engines)
+    and of the megakernel: "ploc" (clustering, the default) or "lbvh" (Karras radix tree);
+    leaf_max is the largest BVH32 leaf (1..32)."""
+
+    def __init__(self, ctx: Context, g: Gaussians, sigma_multiplier: float = 1.0, wide_builder: str = "ploc",
+                 binary_builder: str = "ploc", leaf_max: int = 24):
         n = g.count
+        if wide_builder not in _BUILDERS or binary_builder not in _BUILDERS:
+            raise ValueError("builders are 'ploc' or 'lbvh'")
+        opt = _capi.vp_scene_options()
+        check(lib.vp_scene_options_default(C.byref(opt)))
+        opt.wide_builder, opt.binary_builder = _BUILDERS[wide_builder], _BUILDERS[binary_builder]
+        opt.leaf_max = int(leaf_max)
         self.ctx = ctx
         self._keep = []
         s = _capi.vp_gaussians()
@@ -148,7 +162,7 @@ class Scene:
             s.mean, s.scale, s.quat_wxyz, s.density = (a.ctypes.data for a in arrs)
             s.albedo = alb.ctypes.data if alb is not None else None
         h = C.c_void_p()
-        check(lib.vp_scene_create(ctx.handle, C.byref(s), C.c_float(sigma_multiplier), C.byref(h)))
+        check(lib.vp_scene_create_ex(ctx.handle, C.byref(s), C.c_float(sigma_multiplier), C.byref(opt), C.byref(h)))
         self.handle = h
         self._keep = []
 
@@ -159,7 +173,10 @@ class Scene:
             "count": i.count, "wide_nodes": i.wide_nodes, "wide_depth": i.wide_depth,
             "binary_nodes": i.binary_nodes, "albedo_all_zero": bool(i.albedo_all_zero),
             "build_ms": i.build_ms, "bounds_min": list(i.bounds_min), "bounds_max": list(i.bounds_max),
-            "device_bytes": i.device_bytes,
+            "device_bytes": i.device_bytes, "leaves": i.leaves,
+            "wide_builder": "ploc" if i.wide_builder == _capi.VP_TREE_PLOC else "lbvh",
+            "binary_builder": "ploc" if i.binary_builder == _capi.VP_TREE_PLOC else "lbvh",
+            "binary_height": i.binary_height, "leaf_max": i.leaf_max,
         }
 
     def transmittance(self, origins, dirs, precision: int = _capi.VP_PRECISION_AUTO,

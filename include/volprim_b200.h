@@ -60,7 +60,7 @@ typedef enum vp_nee_mode {
 /* Which GPU engine runs the path loop. */
 typedef enum vp_engine {
   VP_ENGINE_WARP = 0,       /* persistent kernel, one path per warp, warp-cooperative BVH32 traversal */
-  VP_ENGINE_MEGAKERNEL = 1, /* plain per-pixel megakernel, thread-per-ray binary-LBVH traversal */
+  VP_ENGINE_MEGAKERNEL = 1, /* plain per-pixel megakernel, thread-per-ray binary-tree traversal */
   VP_ENGINE_WAVEFRONT = 2   /* wavefront of persistent stage kernels over compacted path queues,
                                warp-cooperative BVH32 traversal; same results as VP_ENGINE_WARP */
 } vp_engine;
@@ -131,24 +131,50 @@ typedef struct vp_scene_info {
   uint32_t count;           /* primitives */
   uint32_t wide_nodes;      /* BVH32 nodes */
   uint32_t wide_depth;      /* BVH32 depth (root = 1) */
-  uint32_t binary_nodes;    /* binary LBVH internal nodes */
+  uint32_t binary_nodes;    /* internal nodes of the megakernel's binary tree */
   uint32_t leaves;          /* BVH32 leaf ranges */
   int32_t albedo_all_zero;  /* 1 when every albedo is 0 (absorption-only scene) */
   double build_ms;          /* device time of the whole build (precompute, Morton, sort,
-                               hierarchy, refit, collapse), CUDA events */
+                               clustering / hierarchy, collapse, gathers), CUDA events */
   double bounds_min[3];
   double bounds_max[3];
   uint64_t device_bytes;    /* device memory held by the scene */
+  int32_t wide_builder;     /* vp_tree_builder the BVH32 was collapsed from */
+  int32_t binary_builder;   /* vp_tree_builder of the megakernel's binary tree */
+  uint32_t binary_height;   /* height of the PLOC tree (0 when no PLOC tree was built) */
+  uint32_t leaf_max;        /* largest BVH32 leaf the build allowed */
 } vp_scene_info;
 
 /* Validates the primitives (positive finite scales, positive finite density, finite centres;
  * ply.cpp:146-172), precomputes the per-primitive whitening record (primitive.h:70-87), builds
- * the LBVH over 3-sigma ellipsoid bounds on the device (Morton codes, radix sort, Karras
- * hierarchy, bottom-up refit, collapse to a 32-wide BVH).  Replaces Renderer::initPrimsAndGAS
+ * the BVH over 3-sigma ellipsoid bounds on the device (Morton codes, radix sort, PLOC clustering
+ * or Karras hierarchy + refit, collapse to a 32-wide BVH).  Replaces Renderer::initPrimsAndGAS
  * (renderer.cpp:85-173: host Morton sort + OptiX GAS/IAS build).  No primitive-count cap below
  * 2^26 (the reference caps at 65,535, renderer.cpp:54-59). */
 vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* prims, float sigma_multiplier,
                           vp_scene** out);
+
+/* Binary tree a scene's traversal structures come from. */
+typedef enum vp_tree_builder {
+  VP_TREE_PLOC = 0, /* agglomerative clustering of the Morton-sorted 3-sigma boxes (Meister & Bittner
+                       2018: nearest neighbour by union surface area in a +-32 window) */
+  VP_TREE_LBVH = 1  /* Karras radix tree over the 63-bit Morton codes, refitted */
+} vp_tree_builder;
+
+/* Build choices of vp_scene_create_ex; vp_scene_create uses vp_scene_options_default. */
+typedef struct vp_scene_options {
+  int32_t wide_builder;   /* vp_tree_builder collapsed into the BVH32 of the warp and wavefront
+                             engines (default VP_TREE_PLOC) */
+  int32_t binary_builder; /* vp_tree_builder of the megakernel's binary tree (default VP_TREE_PLOC;
+                             a PLOC tree deeper than the megakernel's 128-entry stack falls back
+                             to VP_TREE_LBVH) */
+  uint32_t leaf_max;      /* largest BVH32 leaf in Gaussians, 1..32 (default 24) */
+  uint32_t reserved;      /* 0 */
+} vp_scene_options;
+
+vp_status vp_scene_options_default(vp_scene_options* out);
+vp_status vp_scene_create_ex(vp_context* ctx, const vp_gaussians* prims, float sigma_multiplier,
+                             const vp_scene_options* options, vp_scene** out);
 vp_status vp_scene_info_get(vp_scene* scene, vp_scene_info* out);
 vp_status vp_scene_destroy(vp_scene* scene);
 

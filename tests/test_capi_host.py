@@ -57,6 +57,14 @@ def test_version_and_defaults():
     assert p.engine == _capi.VP_ENGINE_WAVEFRONT
 
 
+def test_scene_option_defaults():
+    o = _capi.vp_scene_options()
+    _capi.check(_capi.lib.vp_scene_options_default(C.byref(o)))
+    assert (o.wide_builder, o.binary_builder, o.leaf_max, o.reserved) == (_capi.VP_TREE_PLOC, _capi.VP_TREE_PLOC, 24, 0)
+    assert _capi.lib.vp_scene_options_default(None) == -1
+    assert _capi.lib.vp_scene_create_ex(None, None, C.c_float(1.0), None, None) == -1
+
+
 def test_null_arguments_are_errors_not_crashes():
     assert _capi.lib.vp_context_create(0, None) == -1
     assert b"NULL" in _capi.lib.vp_last_error_string() or _capi.lib.vp_last_error_string()
@@ -84,7 +92,7 @@ def test_struct_layouts_match_header(tmp_path):
                "vp_camera": _capi.vp_camera, "vp_render_params": _capi.vp_render_params,
                "vp_render_stats": _capi.vp_render_stats, "vp_gaussian_grads": _capi.vp_gaussian_grads,
                "vp_server_config": _capi.vp_server_config, "vp_request": _capi.vp_request,
-               "vp_server_stats": _capi.vp_server_stats}
+               "vp_server_stats": _capi.vp_server_stats, "vp_scene_options": _capi.vp_scene_options}
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
