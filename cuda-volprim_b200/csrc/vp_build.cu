@@ -384,11 +384,15 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const uint32_t* __restri
     const int j = i + k;
     if (k == 0 || j < 0 || j >= (int)m) continue;
     const float a = union_area(al, ah, sl[c + k], sh[c + k]);
-    // pair order: area, then the pair's lower position, then its upper position
+    // pair order: area, then buddy pairs (2k, 2k + 1) first -- so equal boxes pair up in halves
+    // instead of chaining -- then the pair's lower position, then its upper position
     bool take = bj < 0 || a < best;
     if (!take && a == best) {
       const int lo_new = min(i, j), lo_old = min(i, bj);
-      take = lo_new < lo_old || (lo_new == lo_old && max(i, j) < max(i, bj));
+      const bool bud_new = !(lo_new & 1) && max(i, j) == lo_new + 1;
+      const bool bud_old = !(lo_old & 1) && max(i, bj) == lo_old + 1;
+      take = (bud_new != bud_old) ? bud_new
+                                  : (lo_new < lo_old || (lo_new == lo_old && max(i, j) < max(i, bj)));
     }
     if (take) {
       best = a;
@@ -735,8 +739,8 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   // the Karras tree for both (a BVH32 that is a single leaf needs no tree).
   const uint32_t ni = n > 1 ? n - 1 : 1;
   const uint32_t kLeafMax = opt.leaf_max;
-  const bool wide_ploc = n > kLeafMax && opt.wide_builder == VP_TREE_PLOC;
-  const bool use_ploc = n > 1u && (wide_ploc || opt.binary_builder == VP_TREE_PLOC);
+  bool wide_ploc = n > kLeafMax && opt.wide_builder == VP_TREE_PLOC;
+  bool use_ploc = n > 1u && (wide_ploc || opt.binary_builder == VP_TREE_PLOC);
   Scratch<uint32_t> pleft(st), pright(st), nn(st), totals(st);
   Scratch<float4> pnlo(st), pnhi(st), ca(st), cb(st), oa(st), ob(st);
   Scratch<unsigned long long> fl(st), sc_x(st);
@@ -762,10 +766,13 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     }
     // Passes run in chunks between host reads of the count; the count only falls, so the last
     // value read bounds the grids of the next chunk.
+    // A chain of nested boxes (concentric Gaussians of growing size) merges about one pair per
+    // pass; past kMaxPasses the build drops the clustering and uses the Karras tree instead.
     constexpr int kChunk = 8;
+    constexpr int kMaxPasses = 1024;
     uint32_t m = n, made = 0u;
     int pass = 0;
-    while (m > 1u) {
+    while (m > 1u && pass < kMaxPasses) {
       for (int k = 0; k < kChunk; ++k, ++pass) {
         const uint32_t* cin = totals.p + 2 * (pass & 1);
         uint32_t* cout = totals.p + 2 * ((pass + 1) & 1);
@@ -789,12 +796,16 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
       m = th[0];
       made = th[1];
     }
-    const uint32_t node_base = made;
-    wroot = node_base - 1u;  // the last merge made the root (node n - 2)
-    float4 root_lo;
-    VP_CUDA(cudaMemcpyAsync(&root_lo, pnlo.p + wroot, sizeof(root_lo), cudaMemcpyDeviceToHost, st));
-    VP_CUDA(cudaStreamSynchronize(st));
-    std::memcpy(&ploc_height, &root_lo.w, sizeof(ploc_height));
+    if (m > 1u) {
+      use_ploc = false;
+      wide_ploc = false;
+    } else {
+      wroot = made - 1u;  // the last merge made the root (node n - 2)
+      float4 root_lo;
+      VP_CUDA(cudaMemcpyAsync(&root_lo, pnlo.p + wroot, sizeof(root_lo), cudaMemcpyDeviceToHost, st));
+      VP_CUDA(cudaStreamSynchronize(st));
+      std::memcpy(&ploc_height, &root_lo.w, sizeof(ploc_height));
+    }
   }
   // Karras radix tree + refit over the Morton order: the BVH32's source when the options ask for it,
   // and the megakernel's binary tree when they ask for it or the PLOC tree is deeper than the

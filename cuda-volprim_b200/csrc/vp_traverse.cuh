@@ -3,6 +3,8 @@
 // wavefront engine.
 #pragma once
 
+#include <type_traits>
+
 #include "vp_internal.h"
 
 namespace vp {
@@ -107,6 +109,9 @@ struct ScatterAlbedo {
 // chord starts before t* <= t), so the set is complete; if the retained chords outgrow the
 // buffer, sa->valid stays false and the caller runs the point query instead.
 //
+// The optical depth accumulates in FP64 under kAcc (thousands of overlapping chords keep the
+// 1e-5 transmittance bound) and in FP32 otherwise.
+//
 // A kTau query whose origin lies inside a known Gaussian (`seed`, the one whose free flight put
 // the path there) evaluates that chord first: in a dense medium it alone usually reaches
 // MAX_OPTICAL_DEPTH and the traversal is skipped; otherwise the traversal skips it at its leaf.
@@ -118,7 +123,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   const unsigned lt_mask = (1u << lane) - 1u;
   const float3 inv = safe_inv(d);
   float t_hi = kInf;
-  float acc = 0.0f;
+  using TauSum = std::conditional_t<kAcc, double, float>;
+  TauSum acc = 0;
   uint32_t arg = kNoGauss;  // kArgmin: the Gaussian of the current minimum
   if (kKind == kTau && seed != kNoGauss) {
     float v = 0.0f;
@@ -130,7 +136,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     }
     acc = __shfl_sync(kFull, v, 0);
     if (measure) ws.crossings += 1;
-    if (acc >= kMaxOpticalDepth) return acc;
+    if (acc >= kMaxOpticalDepth) return (float)acc;
   }
   int sp = 0, hb = 0, kept = 0;  // retained chords [0, kept); hb == kept between leaves
   bool keep = (kKind == kArgmin) && sa != nullptr;
@@ -226,7 +232,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           const float v = hit ? chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f),
                                                 ch.t_out, icf)
                               : 0.0f;
-          acc += warp_sum(v);
+          acc += warp_sum((TauSum)v);
           hits_seen += __popc(m);
           if (measure) ws.crossings += (unsigned)__popc(m);
           if (acc >= kMaxOpticalDepth) break;
@@ -353,7 +359,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     }
   }
   __syncwarp();
-  return (kKind == kArgmin) ? t_hi : acc;
+  return (kKind == kArgmin) ? t_hi : (float)acc;
 }
 
 // Albedo at a point: sigma_t * pdf weighted mean over the ellipsoids containing it
@@ -452,7 +458,8 @@ struct ThreadQueries {
     const float3 inv = safe_inv(d);
     uint32_t stack[kBinStack];
     int sp = 0;
-    float t_hi = kInf, acc = 0.f;
+    float t_hi = kInf;
+    std::conditional_t<kAcc, double, float> acc = 0;  // FP64 optical-depth sum under kAcc
     uint32_t node = S.bin_root;
     unsigned int hits = 0;
     while (true) {
@@ -512,7 +519,7 @@ struct ThreadQueries {
       node = stack[--sp];
     }
     if (measure) ws.max_hits = max(ws.max_hits, hits);
-    return (kKind == kArgmin) ? t_hi : acc;
+    return (kKind == kArgmin) ? t_hi : (float)acc;
   }
   __device__ float argmin(float3 o, float3 d, uint64_t key, ScatterAlbedo* sa) {
     sa->valid = false;  // the plain megakernel evaluates the albedo with its own point query

@@ -95,3 +95,50 @@ def test_invalid_scene_options(vp_ctx):
     h = C.c_void_p()
     assert _capi.lib.vp_scene_create_ex(vp_ctx.handle, C.byref(s), C.c_float(1.0), C.byref(opt), C.byref(h)) == -1
     assert b"builders" in _capi.lib.vp_last_error_string()
+
+
+def nested(n, seed):
+    """n concentric spherical Gaussians of strictly growing scale: PLOC merges about one pair per
+    pass here, so its tree is a chain of height ~n."""
+    rng = np.random.default_rng(seed)
+    scale = np.repeat((0.01 * 1.003 ** np.arange(n))[:, None], 3, 1).astype(np.float32)
+    mean = np.zeros((n, 3), np.float32)
+    return vp.Gaussians(mean, scale, scenes.uniform_quaternions(rng, n), np.full(n, 2.0 / n, np.float32),
+                        np.full((n, 3), 0.5, np.float32))
+
+
+def identical(n):
+    q = np.tile(np.array([1.0, 0, 0, 0], np.float32), (n, 1))
+    return vp.Gaussians(np.full((n, 3), 0.1, np.float32), np.full((n, 3), 0.2, np.float32), q,
+                        np.full(n, 3.0 / n, np.float32), np.full((n, 3), 0.7, np.float32))
+
+
+@pytest.mark.parametrize("case, wide, binary, max_height", [
+    ("identical_1000", "ploc", "ploc", 16),   # buddy pairs: about log2(n) passes, a balanced tree
+    ("nested_300", "ploc", "lbvh", None),     # chain of height ~300: the megakernel takes the LBVH
+    ("nested_2000", "lbvh", "lbvh", 0),       # > 1024 passes: the build drops the clustering
+])
+def test_degenerate_layouts(vp_ctx, case, wide, binary, max_height):
+    g = identical(1000) if case.startswith("identical") else nested(int(case.split("_")[1]), 5)
+    sc = vp.Scene(vp_ctx, g, 1.0)
+    info = sc.info()
+    assert (info["wide_builder"], info["binary_builder"]) == (wide, binary), info
+    if max_height is not None:
+        assert info["binary_height"] <= max_height, info
+    else:
+        assert info["binary_height"] >= 127, info
+    osc = O.OracleScene.from_gaussians(g)
+    rng = np.random.default_rng(8)
+    o, d = random_rays(rng, 3000, radius=3.0, inside_frac=0.3)
+    o[:500] = rng.normal(0, 0.05, (500, 3))
+    T64, tau64 = osc.transmittance_fp64(o, d)
+    sel = tau64 < 80
+    for eng in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+        T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=eng).astype(np.float64)
+        assert np.all(np.abs(T - T64)[sel] <= 2e-5 * T64[sel] + 1e-9), (eng, np.max(np.abs(T - T64)[sel]))
+        pts = rng.normal(0, 0.3, (2000, 3)).astype(np.float32)
+        _, cnt = sc.albedo_at(pts, engine=eng)
+        _, ocnt = osc.albedo_at(pts)
+        diff = np.abs(cnt.astype(np.int64) - ocnt.astype(np.int64))
+        assert diff.max() <= 1 and np.mean(diff > 0) < 1e-3, (eng, diff.max())
+    sc.close()
