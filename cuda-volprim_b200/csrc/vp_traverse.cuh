@@ -249,7 +249,10 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           v = chord_free_flight<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), ch.t_in, ch.t_out, icf,
                                       free_flight_tau<kAcc>(key, orig));
         }
-        const float mn = warp_min(v);
+        // free flights are >= 0 (+ 0 turns -0 into +0), so their bits order as their values and
+        // one redux.sync takes the warp minimum
+        v += 0.0f;
+        const float mn = __uint_as_float(__reduce_min_sync(kFull, __float_as_uint(v)));
         if (mn < t_hi) {
           const unsigned wm = __ballot_sync(kFull, v == mn);
           arg = __shfl_sync(kFull, pi, __ffs(wm) - 1);
