@@ -238,7 +238,16 @@ __device__ __forceinline__ bool chord_fast(const PrimGeo& g, float3 o, float3 d,
   const float3 q = whiten(g, dh);
   const float a2 = dot3(w, w);
   const float ra = __frcp_rn(a2);
-  const float tc = -dot3(q, w) * ra;
+  const float qw = dot3(q, w);
+  // Early miss: the closest-approach distance is also |q|^2 - (q.w)^2 / |w|^2.  Its FP32 error is
+  // a few ulps of |q|^2 (cancellation), so a lane above 9 + 1e-5 |q|^2 + 1e-4 is a miss for the
+  // exact test below as well (inf and NaN never reject); the rest go through the compensated
+  // closest-approach frame, so the chords are the same with or without this test.
+  {
+    const float qq = dot3(q, q);
+    if (fmaf(-qw * qw, ra, qq) > fmaf(1e-5f, qq, kExtent2 + 1e-4f)) return false;
+  }
+  const float tc = -qw * ra;
   const float3 r = add(fma3(tc, d, dh), dl);
   const float3 pp = whiten(g, r);
   const float d2 = dot3(pp, pp);
