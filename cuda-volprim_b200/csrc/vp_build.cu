@@ -477,47 +477,187 @@ __device__ __forceinline__ uint32_t ref_count(uint32_t r, const float4* __restri
   return ref_is_leaf(r) ? 1u : __float_as_uint(nhi[r].w);
 }
 
-// Greedy collapse of a binary tree (Gaussian counts in nhi.w) into 32-wide nodes: starting from a
-// binary node's two children, repeatedly replace the largest-area child holding more than kLeafMax
-// Gaussians by its two children until 32 slots are used.  Children with <= kLeafMax Gaussians
-// become leaves; larger ones become the next level's nodes.  Every child carries the scene
-// position of its first Gaussian in depth-first leaf order (left subtree first), so a leaf is one
-// contiguous range of the scene order; pos[Morton position] receives each Gaussian's scene position.
+// ------------------------------------------------------------------------------------------
+// SAH-optimal collapse (the dynamic programme of Ylitie, Karras & Laine, "Efficient Incoherent Ray
+// Traversal on GPUs Through Compressed Wide BVHs", HPG 2017, with 32 slots per node).  For each
+// binary node v and slot budget i, C(v, i) is the least expected traversal cost of representing
+// v's subtree with at most i child slots of the enclosing BVH32 node:
+//   C(v, 1) = min(leaf: A(v) (c_leaf + c_box n(v)) if n(v) <= leaf_max,  node: A(v) c_node + D(v, 32))
+//   D(v, i) = min over 2 <= k <= i, 1 <= j < k of C(left, j) + C(right, k - j)
+//   C(v, i) = min(C(v, 1), D(v, i))
+// with A the surface area.  A Gaussian is a leaf of cost A (c_leaf + c_box).  The costs weigh an
+// inner-node step against a leaf range (leaf packing shares warp steps between ranges) and a box
+// test: c_node = 1, c_leaf = 0.5, c_box = 0.02.
+// ------------------------------------------------------------------------------------------
+constexpr float kDpNode = 1.0f, kDpLeaf = 0.5f, kDpBox = 0.02f;
+
+struct DpTables {
+  float* cost;       // [ni * 32]: C(v, i) at v * 32 + i - 1
+  uint8_t* split;    // [ni * 32]: j of the best split into exactly i slots
+  uint8_t* best;     // [ni * 32]: the k <= i of D(v, i)
+  uint32_t* single;  // [ni]: bit i - 1 set when C(v, i) uses one slot
+  uint8_t* leaf;     // [ni]: the one slot of C(v, 1) is a leaf
+};
+
+// Parent links of a binary tree (internal children in parent[], Gaussians in parent_leaf[]).
+__global__ void k_parents(uint32_t ni, const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                          uint32_t* __restrict__ parent, uint32_t* __restrict__ parent_leaf) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= ni) return;
+  const uint32_t c[2] = {left[v], right[v]};
+  for (int k = 0; k < 2; ++k) {
+    if (ref_is_leaf(c[k])) parent_leaf[c[k] & ~kLeafBit] = v;
+    else parent[c[k]] = v;
+  }
+}
+
+__device__ __forceinline__ void dp_child(uint32_t ref, const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                         const float* cost, float (&C)[32]) {
+  if (ref_is_leaf(ref)) {
+    const uint32_t p = ref & ~kLeafBit;
+    const float c = box_area(plo[p], phi[p]) * (kDpLeaf + kDpBox);
+    for (int i = 0; i < 32; ++i) C[i] = c;
+  } else {
+    for (int i = 0; i < 32; ++i) C[i] = __ldcg(cost + (size_t)ref * 32u + i);
+  }
+}
+
+// Bottom-up: one thread per Gaussian walks to the root; the second arrival at a node computes it.
+__global__ void k_dp_cost(uint32_t n, uint32_t root, const uint32_t* __restrict__ left,
+                          const uint32_t* __restrict__ right, const float4* __restrict__ plo,
+                          const float4* __restrict__ phi, const float4* __restrict__ nlo,
+                          const float4* __restrict__ nhi, const uint32_t* __restrict__ parent,
+                          const uint32_t* __restrict__ parent_leaf, unsigned int* flags, DpTables T,
+                          uint32_t leaf_max) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t v = parent_leaf[k];
+  while (true) {
+    __threadfence();
+    if (atomicAdd(&flags[v], 1u) == 0u) return;
+    __threadfence();
+    float Cl[32], Cr[32], D[33];
+    dp_child(left[v], plo, phi, T.cost, Cl);
+    dp_child(right[v], plo, phi, T.cost, Cr);
+    float dprev = INFINITY;
+    uint32_t kprev = 2;
+    for (int i = 2; i <= 32; ++i) {
+      float b = INFINITY;
+      int bj = 1;
+      for (int j = 1; j < i; ++j) {
+        const float c = Cl[j - 1] + Cr[i - j - 1];
+        if (c < b) {
+          b = c;
+          bj = j;
+        }
+      }
+      T.split[(size_t)v * 32u + i - 1] = (uint8_t)bj;
+      if (i == 2 || b < dprev) {
+        dprev = b;
+        kprev = (uint32_t)i;
+      }
+      D[i] = dprev;
+      T.best[(size_t)v * 32u + i - 1] = (uint8_t)kprev;
+    }
+    const float4 l = nlo[v], h = nhi[v];
+    const float A = box_area(l, h);
+    const uint32_t count = __float_as_uint(h.w);
+    const float c_node = fmaf(A, kDpNode, D[32]);
+    const float c_leaf = count <= leaf_max ? A * fmaf(kDpBox, (float)count, kDpLeaf) : INFINITY;
+    const bool is_leaf = count <= leaf_max && c_leaf <= c_node;  // a leaf fits in one warp step
+    const float c1 = fminf(c_leaf, c_node);
+    uint32_t mask = 1u;
+    __stcg(T.cost + (size_t)v * 32u, c1);
+    for (int i = 2; i <= 32; ++i) {
+      const bool one = c1 <= D[i];
+      if (one) mask |= 1u << (i - 1);
+      __stcg(T.cost + (size_t)v * 32u + i - 1, one ? c1 : D[i]);
+    }
+    T.single[v] = mask;
+    T.leaf[v] = is_leaf ? 1 : 0;
+    if (v == root) return;
+    v = parent[v];
+  }
+}
+
+// Collapse of a binary tree (Gaussian counts in nhi.w) into 32-wide nodes, level by level:
+//  - greedy (kDp false): starting from the binary node's two children, repeatedly replace the
+//    largest-area child holding more than kLeafMax Gaussians by its two children until 32 slots
+//    are used; children with <= kLeafMax Gaussians become leaves, larger ones the next level's
+//    nodes;
+//  - SAH-optimal (kDp true): replay the choices of k_dp_cost for a budget of 32 slots.
+// Every child carries the scene position of its first Gaussian in depth-first leaf order (left
+// subtree first), so a leaf is one contiguous range of the scene order; pos[Morton position]
+// receives each Gaussian's scene position.  Nodes beyond max_nodes are not written: the build
+// then sees *overflow set and falls back to the greedy collapse.
+template <bool kDp>
 __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in,
                            CollapseItem* __restrict__ out, unsigned int* __restrict__ out_count,
                            unsigned int* __restrict__ slot_counter, const uint32_t* __restrict__ left,
                            const uint32_t* __restrict__ right, const float4* __restrict__ plo,
                            const float4* __restrict__ phi, const float4* __restrict__ nlo,
                            const float4* __restrict__ nhi, float4* __restrict__ wide, uint32_t kLeafMax,
-                           uint32_t* __restrict__ pos, unsigned int* __restrict__ leaf_counter) {
+                           uint32_t* __restrict__ pos, unsigned int* __restrict__ leaf_counter, DpTables T,
+                           uint32_t max_nodes, unsigned int* __restrict__ overflow) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_items) return;
   const CollapseItem it = in[t];
   uint32_t refs[32], offs[32];
-  int cnt = 2;
-  refs[0] = left[it.bin];
-  refs[1] = right[it.bin];
-  offs[0] = it.offset;
-  offs[1] = it.offset + ref_count(refs[0], nhi);
-  while (cnt < 32) {
-    int best = -1;
-    float best_a = -1.f;
-    for (int c = 0; c < cnt; ++c) {
-      const uint32_t r = refs[c];
-      if (ref_is_leaf(r)) continue;
-      if (ref_count(r, nhi) <= kLeafMax) continue;
-      const float a = box_area(nlo[r], nhi[r]);
-      if (a > best_a) {
-        best_a = a;
-        best = c;
-      }
+  uint32_t leafmask = 0;  // kDp: internal refs that are leaves
+  int cnt = 0;
+  if constexpr (kDp) {
+    // expansion stack of (ref, slot budget, offset); the budgets on it sum to <= 32
+    uint32_t sv[32], so[32];
+    uint8_t si[32];
+    int sp = 0;
+    {
+      const uint32_t v = it.bin;
+      const uint32_t kk = T.best[(size_t)v * 32u + 31u], j = T.split[(size_t)v * 32u + kk - 1u];
+      sv[sp] = right[v], si[sp] = (uint8_t)(kk - j), so[sp] = it.offset + ref_count(left[v], nhi), ++sp;
+      sv[sp] = left[v], si[sp] = (uint8_t)j, so[sp] = it.offset, ++sp;
     }
-    if (best < 0) break;
-    const uint32_t r = refs[best];
-    refs[best] = left[r];
-    refs[cnt] = right[r];
-    offs[cnt] = offs[best] + ref_count(left[r], nhi);
-    ++cnt;
+    while (sp > 0 && cnt < 32) {
+      --sp;
+      const uint32_t v = sv[sp], i = si[sp], off = so[sp];
+      if (ref_is_leaf(v) || i == 1u || ((T.single[v] >> (i - 1u)) & 1u)) {
+        if (!ref_is_leaf(v) && T.leaf[v]) leafmask |= 1u << cnt;
+        refs[cnt] = v;
+        offs[cnt] = off;
+        ++cnt;
+        continue;
+      }
+      const uint32_t kk = T.best[(size_t)v * 32u + i - 1u], j = T.split[(size_t)v * 32u + kk - 1u];
+      sv[sp] = right[v], si[sp] = (uint8_t)(kk - j), so[sp] = off + ref_count(left[v], nhi), ++sp;
+      sv[sp] = left[v], si[sp] = (uint8_t)j, so[sp] = off, ++sp;
+    }
+  } else {
+    cnt = 2;
+    refs[0] = left[it.bin];
+    refs[1] = right[it.bin];
+    offs[0] = it.offset;
+    offs[1] = it.offset + ref_count(refs[0], nhi);
+    while (cnt < 32) {
+      int best = -1;
+      float best_a = -1.f;
+      for (int c = 0; c < cnt; ++c) {
+        const uint32_t r = refs[c];
+        if (ref_is_leaf(r)) continue;
+        if (ref_count(r, nhi) <= kLeafMax) continue;
+        const float a = box_area(nlo[r], nhi[r]);
+        if (a > best_a) {
+          best_a = a;
+          best = c;
+        }
+      }
+      if (best < 0) break;
+      const uint32_t r = refs[best];
+      refs[best] = left[r];
+      refs[cnt] = right[r];
+      offs[cnt] = offs[best] + ref_count(left[r], nhi);
+      ++cnt;
+    }
+    for (int c = 0; c < cnt; ++c)
+      if (!ref_is_leaf(refs[c]) && ref_count(refs[c], nhi) <= kLeafMax) leafmask |= 1u << c;
   }
   float4* node = wide + (size_t)it.slot * 64u;
   for (int c = 0; c < 32; ++c) {
@@ -542,7 +682,7 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
       l = nlo[r];
       h = nhi[r];
       const uint32_t count = ref_count(r, nhi);
-      if (count <= kLeafMax) {
+      if ((leafmask >> c) & 1u) {
         wref = wide_leaf_ref(offs[c], count);
         atomicAdd(leaf_counter, 1u);
         // depth-first walk of the leaf's subtree (<= 32 Gaussians, so <= 32 stacked refs)
@@ -561,9 +701,14 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
         }
       } else {
         const uint32_t slot = atomicAdd(slot_counter, 1u);
-        const uint32_t q = atomicAdd(out_count, 1u);
-        out[q] = CollapseItem{r, slot, offs[c], 0u};
-        wref = slot;
+        if (slot >= max_nodes) {  // over the node budget: no write; the build falls back
+          atomicOr(overflow, 1u);
+          wref = kEmptyRef;
+        } else {
+          const uint32_t q = atomicAdd(out_count, 1u);
+          out[q] = CollapseItem{r, slot, offs[c], 0u};
+          wref = slot;
+        }
       }
     }
     l.w = __uint_as_float(wref);
@@ -850,40 +995,80 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   if ((s = dev_alloc(&wide, 64ull * max_wide, st))) return s;
   sc->wide = wide;
   uint32_t depth = 1, wide_nodes = 1, leaves = 1;
+  bool dp_used = false;
   if (n <= kLeafMax) {
     k_single_leaf_root<<<1, 32, 0, st>>>(n, plo.p, phi.p, wide);
     VP_CUDA(cudaGetLastError());
     k_iota<<<nb, TB, 0, st>>>(n, pos.p);
     VP_CUDA(cudaGetLastError());
   } else {
+    // SAH-optimal slot tables (k_dp_cost) when asked for and the scene is at most 2^24 Gaussians.
+    const uint32_t nint = n - 1u;
+    Scratch<float> dp_cost(st);
+    Scratch<uint8_t> dp_split(st), dp_best(st), dp_leaf(st);
+    Scratch<uint32_t> dp_single(st), par(st), par_leaf(st);
+    Scratch<unsigned int> dp_flags(st);
+    DpTables T{nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool dp = opt.wide_collapse == VP_COLLAPSE_SAH && n <= (1u << 24);
+    if (dp) {
+      if ((s = dev_alloc(&dp_cost.p, 32ull * nint, st))) return s;
+      if ((s = dev_alloc(&dp_split.p, 32ull * nint, st))) return s;
+      if ((s = dev_alloc(&dp_best.p, 32ull * nint, st))) return s;
+      if ((s = dev_alloc(&dp_leaf.p, nint, st))) return s;
+      if ((s = dev_alloc(&dp_single.p, nint, st))) return s;
+      if ((s = dev_alloc(&par.p, nint, st))) return s;
+      if ((s = dev_alloc(&par_leaf.p, n, st))) return s;
+      if ((s = dev_alloc(&dp_flags.p, nint, st))) return s;
+      VP_CUDA(cudaMemsetAsync(dp_flags.p, 0, sizeof(unsigned int) * nint, st));
+      k_parents<<<(nint + TB - 1) / TB, TB, 0, st>>>(nint, wl, wr, par.p, par_leaf.p);
+      VP_CUDA(cudaGetLastError());
+      T = DpTables{dp_cost.p, dp_split.p, dp_best.p, dp_single.p, dp_leaf.p};
+      k_dp_cost<<<nb, TB, 0, st>>>(n, wide_root, wl, wr, plo.p, phi.p, wlo, whi, par.p, par_leaf.p, dp_flags.p, T,
+                                   kLeafMax);
+      VP_CUDA(cudaGetLastError());
+    }
     Scratch<CollapseItem> qa(st), qb(st);
     Scratch<unsigned int> ctr(st);
     if ((s = dev_alloc(&qa.p, max_wide, st))) return s;
     if ((s = dev_alloc(&qb.p, max_wide, st))) return s;
-    if ((s = dev_alloc(&ctr.p, 3, st))) return s;
-    CollapseItem root{wide_root, 0u, 0u, 0u};
-    VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
-    unsigned int c0[3] = {1u, 0u, 0u};  // next free slot, next-level queue length, leaves
-    VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
-    uint32_t n_items = 1;
-    depth = 0;
-    while (n_items > 0) {
-      ++depth;
-      VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
-      k_collapse<<<(n_items + 127) / 128, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p,
-                                                        wlo, whi, wide, kLeafMax, pos.p, ctr.p + 2);
-      VP_CUDA(cudaGetLastError());
-      unsigned int ch[3];
-      VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
-      VP_CUDA(cudaStreamSynchronize(st));
-      n_items = ch[1];
-      wide_nodes = ch[0];
-      leaves = ch[2];
-      std::swap(qa.p, qb.p);
-      if (wide_nodes > max_wide) return fail(VP_ERROR_INTERNAL, "BVH32 node budget exceeded");
+    if ((s = dev_alloc(&ctr.p, 4, st))) return s;
+    // A level-by-level collapse; an SAH cut that needs more nodes than the greedy bound is redone
+    // greedily.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      CollapseItem root{wide_root, 0u, 0u, 0u};
+      VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+      unsigned int c0[4] = {1u, 0u, 0u, 0u};  // next free slot, next-level queue length, leaves, overflow
+      VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
+      uint32_t n_items = 1;
+      depth = 0;
+      unsigned int ch[4] = {0u, 0u, 0u, 0u};
+      while (n_items > 0) {
+        ++depth;
+        VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
+        const unsigned grid = (n_items + 127) / 128;
+        if (dp)
+          k_collapse<true><<<grid, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p, wlo,
+                                                 whi, wide, kLeafMax, pos.p, ctr.p + 2, T, max_wide, ctr.p + 3);
+        else
+          k_collapse<false><<<grid, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p, wlo,
+                                                  whi, wide, kLeafMax, pos.p, ctr.p + 2, T, max_wide, ctr.p + 3);
+        VP_CUDA(cudaGetLastError());
+        VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
+        VP_CUDA(cudaStreamSynchronize(st));
+        n_items = ch[1];
+        wide_nodes = ch[0];
+        leaves = ch[2];
+        std::swap(qa.p, qb.p);
+        if (ch[3] != 0u) break;
+      }
+      if (ch[3] == 0u) {
+        dp_used = dp;
+        break;
+      }
+      if (!dp) return fail(VP_ERROR_INTERNAL, "BVH32 node budget exceeded");
+      dp = false;
     }
   }
-
   // Scene order, then the records, boxes and adjoint inputs gathered into it.
   uint32_t* perm = nullptr;
   if ((s = dev_alloc(&perm, n, st))) return s;
@@ -955,6 +1140,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   info.binary_builder = bin_from_ploc ? VP_TREE_PLOC : VP_TREE_LBVH;
   info.binary_height = ploc_height;
   info.leaf_max = kLeafMax;
+  info.wide_collapse = dp_used ? VP_COLLAPSE_SAH : VP_COLLAPSE_GREEDY;
   info.albedo_all_zero = v.albedo_all_zero;
   info.build_ms = ms;
   for (int k = 0; k < 3; ++k) {

@@ -240,9 +240,14 @@ vp_status vp_context_sm_count(vp_context* c, int32_t* out) {
   return VP_OK;
 }
 
+// Default BVH32 collapse of vp_scene_options_default.
+#ifndef VP_DEFAULT_COLLAPSE
+#define VP_DEFAULT_COLLAPSE VP_COLLAPSE_SAH
+#endif
+
 vp_status vp_scene_options_default(vp_scene_options* out) {
   if (!out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
-  *out = vp_scene_options{VP_TREE_PLOC, VP_TREE_PLOC, 24u, 0u};
+  *out = vp_scene_options{VP_TREE_PLOC, VP_TREE_PLOC, 24u, VP_DEFAULT_COLLAPSE};
   return VP_OK;
 }
 
@@ -256,6 +261,8 @@ vp_status vp_scene_create_ex(vp_context* ctx, const vp_gaussians* g, float sigma
   auto builder_ok = [](int32_t b) { return b == VP_TREE_PLOC || b == VP_TREE_LBVH; };
   if (!builder_ok(opt.wide_builder) || !builder_ok(opt.binary_builder))
     return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options: builders must be VP_TREE_PLOC or VP_TREE_LBVH");
+  if (opt.wide_collapse != VP_COLLAPSE_GREEDY && opt.wide_collapse != VP_COLLAPSE_SAH)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.wide_collapse must be VP_COLLAPSE_GREEDY or VP_COLLAPSE_SAH");
   if (opt.leaf_max < 1u || opt.leaf_max > 32u)
     return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.leaf_max must be in [1, 32]");
   VP_CUDA(cudaSetDevice(ctx->device));

@@ -18,6 +18,7 @@ VP_PRECISION_AUTO, VP_PRECISION_FAST, VP_PRECISION_ACCURATE = 0, 1, 2
 VP_MEASURE_COUNTERS, VP_MEASURE_STAGES = 1, 2
 VP_SCHEDULE_FIFO, VP_SCHEDULE_FAIR, VP_SCHEDULE_SRPT = 0, 1, 2
 VP_TREE_PLOC, VP_TREE_LBVH = 0, 1
+VP_COLLAPSE_GREEDY, VP_COLLAPSE_SAH = 0, 1
 
 ERROR_NAMES = {
     -1: "VP_ERROR_INVALID_ARGUMENT", -2: "VP_ERROR_CUDA", -3: "VP_ERROR_OUT_OF_MEMORY",
@@ -63,6 +64,8 @@ class vp_scene_info(C.Structure):
         ("binary_builder", C.c_int32),
         ("binary_height", C.c_uint32),
         ("leaf_max", C.c_uint32),
+        ("wide_collapse", C.c_int32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -71,7 +74,7 @@ class vp_scene_options(C.Structure):
         ("wide_builder", C.c_int32),
         ("binary_builder", C.c_int32),
         ("leaf_max", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("wide_collapse", C.c_int32),
     ]
 
 

@@ -143,6 +143,8 @@ typedef struct vp_scene_info {
   int32_t binary_builder;   /* vp_tree_builder of the megakernel's binary tree */
   uint32_t binary_height;   /* height of the PLOC tree (0 when no PLOC tree was built) */
   uint32_t leaf_max;        /* largest BVH32 leaf the build allowed */
+  int32_t wide_collapse;    /* vp_collapse the BVH32 was cut with */
+  uint32_t reserved;
 } vp_scene_info;
 
 /* Validates the primitives (positive finite scales, positive finite density, finite centres;
@@ -161,6 +163,16 @@ typedef enum vp_tree_builder {
   VP_TREE_LBVH = 1  /* Karras radix tree over the 63-bit Morton codes, refitted */
 } vp_tree_builder;
 
+/* How the BVH32 is cut from its binary tree. */
+typedef enum vp_collapse {
+  VP_COLLAPSE_GREEDY = 0, /* open the largest-area child until 32 slots are used; subtrees of at
+                             most leaf_max Gaussians become leaves */
+  VP_COLLAPSE_SAH = 1     /* SAH-optimal slot assignment by dynamic programming over the binary
+                             tree (Ylitie, Karras & Laine, HPG 2017, with 32 slots); scenes above
+                             2^24 Gaussians, or whose optimal cut needs more BVH32 nodes than the
+                             greedy bound, use the greedy collapse */
+} vp_collapse;
+
 /* Build choices of vp_scene_create_ex; vp_scene_create uses vp_scene_options_default. */
 typedef struct vp_scene_options {
   int32_t wide_builder;   /* vp_tree_builder collapsed into the BVH32 of the warp and wavefront
@@ -169,7 +181,8 @@ typedef struct vp_scene_options {
                              a PLOC tree deeper than the megakernel's 128-entry stack falls back
                              to VP_TREE_LBVH) */
   uint32_t leaf_max;      /* largest BVH32 leaf in Gaussians, 1..32 (default 24) */
-  uint32_t reserved;      /* 0 */
+  int32_t wide_collapse;  /* vp_collapse: how the binary tree becomes 32-wide nodes (default
+                             VP_COLLAPSE_SAH) */
 } vp_scene_options;
 
 vp_status vp_scene_options_default(vp_scene_options* out);

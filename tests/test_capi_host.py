@@ -60,7 +60,8 @@ def test_version_and_defaults():
 def test_scene_option_defaults():
     o = _capi.vp_scene_options()
     _capi.check(_capi.lib.vp_scene_options_default(C.byref(o)))
-    assert (o.wide_builder, o.binary_builder, o.leaf_max, o.reserved) == (_capi.VP_TREE_PLOC, _capi.VP_TREE_PLOC, 24, 0)
+    assert (o.wide_builder, o.binary_builder, o.leaf_max, o.wide_collapse) == (
+        _capi.VP_TREE_PLOC, _capi.VP_TREE_PLOC, 24, _capi.VP_COLLAPSE_SAH)
     assert _capi.lib.vp_scene_options_default(None) == -1
     assert _capi.lib.vp_scene_create_ex(None, None, C.c_float(1.0), None, None) == -1
 

@@ -1,5 +1,6 @@
 """GPU: the scene build's tree choices (vp_scene_options): PLOC clustering or the Karras LBVH for
-the BVH32 and for the megakernel's binary tree, and the BVH32 leaf size.
+the BVH32 and for the megakernel's binary tree, the BVH32 leaf size, and the SAH-optimal or greedy
+collapse to BVH32.
 
 Every choice must give the oracle's answers: transmittance within the FP64 gate of the parity
 tests (2e-5 relative), ellipsoid overlap counts at points exactly.  Renders from different trees
@@ -21,8 +22,9 @@ from test_gpu_parity import random_rays, small_scatter_workload
 
 pytestmark = pytest.mark.gpu
 
-COMBOS = [("ploc", "ploc", 24), ("lbvh", "lbvh", 24), ("ploc", "lbvh", 32), ("lbvh", "ploc", 8),
-          ("ploc", "ploc", 1)]
+COMBOS = [("ploc", "ploc", 24, "sah"), ("ploc", "ploc", 24, "greedy"), ("lbvh", "lbvh", 24, "sah"),
+          ("lbvh", "lbvh", 24, "greedy"), ("ploc", "lbvh", 32, "sah"), ("lbvh", "ploc", 8, "greedy"),
+          ("ploc", "ploc", 1, "sah")]
 
 
 def clustered(n, seed):
@@ -38,13 +40,14 @@ def clustered(n, seed):
                         np.exp(rng.normal(-1.0, 0.5, n)).astype(np.float32), alb)
 
 
-@pytest.mark.parametrize("wide, binary, leaf", COMBOS)
-def test_tree_choices_match_the_oracle(vp_ctx, wide, binary, leaf):
+@pytest.mark.parametrize("wide, binary, leaf, collapse", COMBOS)
+def test_tree_choices_match_the_oracle(vp_ctx, wide, binary, leaf, collapse):
     n = 5000
     g = clustered(n, 11)
-    sc = vp.Scene(vp_ctx, g, 2.0, wide_builder=wide, binary_builder=binary, leaf_max=leaf)
+    sc = vp.Scene(vp_ctx, g, 2.0, wide_builder=wide, binary_builder=binary, leaf_max=leaf, collapse=collapse)
     info = sc.info()
     assert (info["wide_builder"], info["binary_builder"], info["leaf_max"]) == (wide, binary, leaf)
+    assert info["wide_collapse"] == collapse
     assert info["leaves"] >= math.ceil(n / leaf)
     assert (info["binary_height"] > 0) == ("ploc" in (wide, binary))
     osc = O.OracleScene.from_gaussians(g, sigma_multiplier=2.0)
@@ -72,13 +75,15 @@ def test_renders_agree_across_trees(vp_ctx, engine):
     cfg.engine = engine
     cam = scenes.negz_camera(3.0, 40.0)
     imgs = {}
-    for wide, binary in (("ploc", "ploc"), ("lbvh", "lbvh")):
-        sc = vp.Scene(vp_ctx, g, 2.0, wide_builder=wide, binary_builder=binary)
-        imgs[wide] = vp.Renderer(cfg, sc, cam, env=env, ctx=vp_ctx).render()[..., :3]
+    for key, wide, binary, collapse in (("ploc", "ploc", "ploc", "sah"), ("lbvh", "lbvh", "lbvh", "sah"),
+                                        ("greedy", "ploc", "ploc", "greedy")):
+        sc = vp.Scene(vp_ctx, g, 2.0, wide_builder=wide, binary_builder=binary, collapse=collapse)
+        imgs[key] = vp.Renderer(cfg, sc, cam, env=env, ctx=vp_ctx).render()[..., :3]
         sc.close()
     scale = float(imgs["ploc"].mean())
     assert scale > 0.01
     assert np.abs(imgs["ploc"] - imgs["lbvh"]).mean() / scale < 1e-4
+    assert np.abs(imgs["ploc"] - imgs["greedy"]).mean() / scale < 1e-4
 
 
 def test_invalid_scene_options(vp_ctx):
@@ -86,6 +91,8 @@ def test_invalid_scene_options(vp_ctx):
     for bad in ({"leaf_max": 0}, {"leaf_max": 33}):
         with pytest.raises(vp.VpError, match="leaf_max"):
             vp.Scene(vp_ctx, g, 1.0, **bad)
+    with pytest.raises(ValueError):
+        vp.Scene(vp_ctx, g, 1.0, collapse="optimal")
     with pytest.raises(ValueError):
         vp.Scene(vp_ctx, g, 1.0, wide_builder="sah")
     opt = _capi.vp_scene_options()
