@@ -109,8 +109,9 @@ struct ScatterAlbedo {
 // chord starts before t* <= t), so the set is complete; if the retained chords outgrow the
 // buffer, sa->valid stays false and the caller runs the point query instead.
 //
-// The optical depth accumulates in FP64 under kAcc (thousands of overlapping chords keep the
-// 1e-5 transmittance bound) and in FP32 otherwise.
+// The optical depth is summed over the warp in FP32 after every leaf step (for the stop at
+// MAX_OPTICAL_DEPTH); under kAcc each lane also keeps an FP64 sum of its own chords, reduced once
+// at the end, so thousands of overlapping chords keep the 1e-5 transmittance bound.
 //
 // A kTau query whose origin lies inside a known Gaussian (`seed`, the one whose free flight put
 // the path there) evaluates that chord first: in a dense medium it alone usually reaches
@@ -123,8 +124,12 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   const unsigned lt_mask = (1u << lane) - 1u;
   const float3 inv = safe_inv(d);
   float t_hi = kInf;
-  using TauSum = std::conditional_t<kAcc, double, float>;
-  TauSum acc = 0;
+  float acc = 0.0f;
+  double lane_tau = 0.0;  // kAcc: this lane's chords in FP64
+  auto tau_total = [&]() -> float {
+    if constexpr (kAcc) return (float)warp_sum(lane_tau);
+    else return acc;
+  };
   uint32_t arg = kNoGauss;  // kArgmin: the Gaussian of the current minimum
   if (kKind == kTau && seed != kNoGauss) {
     float v = 0.0f;
@@ -135,8 +140,9 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
         v = chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, g.icf);
     }
     acc = __shfl_sync(kFull, v, 0);
+    if (kAcc) lane_tau = v;  // v is 0 on lanes other than 0
     if (measure) ws.crossings += 1;
-    if (acc >= kMaxOpticalDepth) return (float)acc;
+    if (acc >= kMaxOpticalDepth) return tau_total();
   }
   int sp = 0, hb = 0, kept = 0;  // retained chords [0, kept); hb == kept between leaves
   bool keep = (kKind == kArgmin) && sa != nullptr;
@@ -232,7 +238,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           const float v = hit ? chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f),
                                                 ch.t_out, icf)
                               : 0.0f;
-          acc += warp_sum((TauSum)v);
+          acc += warp_sum(v);
+          if (kAcc) lane_tau += v;
           hits_seen += __popc(m);
           if (measure) ws.crossings += (unsigned)__popc(m);
           if (acc >= kMaxOpticalDepth) break;
@@ -362,7 +369,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     }
   }
   __syncwarp();
-  return (kKind == kArgmin) ? t_hi : (float)acc;
+  if constexpr (kKind == kArgmin) return t_hi;
+  else return tau_total();
 }
 
 // Albedo at a point: sigma_t * pdf weighted mean over the ellipsoids containing it

@@ -34,9 +34,10 @@ namespace {
 constexpr uint32_t kAliveBit = 1u << 18;
 
 // Resident 256-thread blocks per SM the extend / shadow kernels' register budgets are sized for:
-// 4 (64 registers) for extend; 5 (48 registers, 52 B of spills) for shadow, whose smaller state
-// gains more from the extra warps than it loses to the spills (-2% shadow time on the showcase;
-// extend at 5 spills 116 B and loses 9%).
+// 4 (64 registers) for extend; 5 (48 registers, 52 B of spills) for the FP32 shadow kernel, whose
+// smaller state gains more from the extra warps than it loses to the spills (-2% shadow time on
+// the showcase; extend at 5 spills 116 B and loses 9%).  The FP64 (ACCURATE) shadow kernel keeps
+// the extend budget.
 #ifndef VP_WF_MIN_BLOCKS
 #define VP_WF_MIN_BLOCKS 4
 #endif
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
 }
 
 template <bool kAcc, bool kMeasure>
-__global__ void __launch_bounds__(256, VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(SceneView S, WfBuffers b, const uint32_t* count,
+__global__ void __launch_bounds__(256, kAcc ? VP_WF_MIN_BLOCKS : VP_WF_SHADOW_MIN_BLOCKS) k_wf_shadow(SceneView S, WfBuffers b, const uint32_t* count,
                                                    unsigned int* work, Counters* ctr, int measure_i) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
