@@ -34,9 +34,6 @@
 namespace vp {
 namespace {
 
-constexpr float kSqrt2OverPi = 0.79788456080286535588f;  // sqrt(2/pi)
-constexpr float kExpMinus4p5 = 0.011108996538242306f;    // exp(-9/2): the integrand at the 3-sigma boundary
-
 // Warp-cooperative visit of every Gaussian whose 3-sigma chord overlaps [0, inf) of the ray.  The
 // warp walks the BVH32 with the first hit child of each inner node kept in registers and the
 // others on the warp's shared-memory stack (no ordering: the image model is order-independent).
