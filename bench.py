@@ -196,6 +196,10 @@ BOX_BYTES, RECORD_BYTES, WIDE_NODE_BYTES, BINARY_NODE_BYTES = 32, 64, 1024, 64
 EXTEND_STATE_BYTES, SHADOW_STATE_BYTES = 64, 40
 
 
+F_CROSS_FLOPS = 111  # FP32 flops of one closed-form chord evaluation (FMA = 2), erf and MUFU excluded
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
 def roofline(args, m, step_stats):
     """Roofline of the dominant kernel, from the counters of one measured batch (m) and the CUDA-event
     stage times of the timed steps (the steps are the same batch size over the same image)."""
@@ -241,6 +245,14 @@ def roofline(args, m, step_stats):
                          "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"]}}
     if args.engine == "wavefront":
         roof["stage_ms_per_step[extend,shadow,other]"] = ms
+    # The FP32 side: closed-form (ray, Gaussian) evaluations of the step's traversal kernels times
+    # the declared 111 FP32 flops of one (FMA = 2; erf and MUFU work not counted), against the
+    # nominal FP32 rate (148 SMs x 128 lanes x 2 flops x 1965 MHz) -- no FP32 peak is measured.
+    trav_ms = (ms[0] + ms[1]) if args.engine == "wavefront" else step_ms
+    fp32_tflops = m["crossings"] * F_CROSS_FLOPS / (trav_ms / 1e3) / 1e12
+    roof["fp32_side"] = {"crossings_per_step": m["crossings"], "flops_per_crossing": F_CROSS_FLOPS,
+                         "achieved_tflops": fp32_tflops, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
+                         "frac": fp32_tflops / FP32_NOMINAL_TFLOPS, "peak_source": "nominal"}
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         try:
