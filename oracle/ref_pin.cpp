@@ -1,5 +1,5 @@
 // ORACLE pin (test infrastructure only): a C-ABI shim over the reference's OWN host-compilable
-// headers, compiled from /root/reference/include by oracle/Makefile into _ref/libref_pin.so.
+// headers, compiled from the reference's include/ tree by oracle/Makefile into _ref/libref_pin.so.
 // It exposes the reference's Primitive constructor and whitening transforms
 // (include/thesis/device/params/primitive.h:70-122), the 3-sigma containment test
 // (include/thesis/common/geometry/intersection.h:56-61), the host camera build
