@@ -183,7 +183,20 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   while (true) {
     if (!have) {
       if (sp == 0) break;
-      --sp;
+      if constexpr (kKind == kArgmin) {
+        // the argmin's bound shrinks: pop the topmost entry within it, skipping culled ones in
+        // one step (lane j looks at the j-th entry from the top)
+        const int e = sp - 1 - lane;
+        const unsigned bm = __ballot_sync(kFull, e >= 0 && W.st_t[max(e, 0)] <= t_hi);
+        if (bm == 0u) {
+          sp = max(sp - 32, 0);
+          __syncwarp();
+          continue;
+        }
+        sp -= __ffs(bm);
+      } else {
+        --sp;
+      }
       ref = W.st_ref[sp];
       tn = W.st_t[sp];
       __syncwarp();
