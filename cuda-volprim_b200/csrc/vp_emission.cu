@@ -158,8 +158,19 @@ __device__ __forceinline__ float3 ray_radiance(const RaySums& rs, float3 env) {
   return f3(fmaf(a, rs.r, T * env.x), fmaf(a, rs.g, T * env.y), fmaf(a, rs.b, T * env.z));
 }
 
+// Resident 256-thread blocks per SM the FP32 emission kernels' register budgets are sized for
+// (64 registers; the FP64 variants keep 2).  On the differentiation workload 4 blocks take the
+// forward from 56.5 to 49.2 ms and the adjoint from 127 to 114 ms against the compiler's own
+// budgets (76 and 80 registers: 3 blocks).
+#ifndef VP_EMIS_FWD_BLOCKS
+#define VP_EMIS_FWD_BLOCKS 4
+#endif
+#ifndef VP_EMIS_BWD_BLOCKS
+#define VP_EMIS_BWD_BLOCKS 4
+#endif
+
 template <bool kAcc>
-__global__ void __launch_bounds__(256) k_emis_forward(SceneView S, EnvView E, CameraView C, ParamsView P,
+__global__ void __launch_bounds__(256, kAcc ? 2 : VP_EMIS_FWD_BLOCKS) k_emis_forward(SceneView S, EnvView E, CameraView C, ParamsView P,
                                                       const float4* __restrict__ emis, float4* __restrict__ out,
                                                       unsigned int* work, Counters* ctr) {
   extern __shared__ uint32_t stacks[];
@@ -259,7 +270,7 @@ __device__ __forceinline__ bool tau_grad(const PrimGeo& g, const Chord& ch, floa
 }
 
 template <bool kAcc>
-__global__ void __launch_bounds__(256) k_emis_backward(SceneView S, EnvView E, CameraView C, ParamsView P,
+__global__ void __launch_bounds__(256, kAcc ? 2 : VP_EMIS_BWD_BLOCKS) k_emis_backward(SceneView S, EnvView E, CameraView C, ParamsView P,
                                                        const float4* __restrict__ emis,
                                                        const float4* __restrict__ dl_dpix, float4* __restrict__ acc,
                                                        unsigned int* work, Counters* ctr) {
