@@ -588,10 +588,11 @@ __global__ void k_dp_cost(uint32_t n, uint32_t root, const uint32_t* __restrict_
 //  - SAH-optimal (kDp true): replay the choices of k_dp_cost for a budget of 32 slots.
 // Every child carries the scene position of its first Gaussian in depth-first leaf order (left
 // subtree first), so a leaf is one contiguous range of the scene order; pos[Morton position]
-// receives each Gaussian's scene position.  Nodes beyond max_nodes are not written: the build
-// then sees *overflow set and falls back to the greedy collapse.
+// receives each Gaussian's scene position.  The level's item count is read on the device
+// (*n_items_dev), so levels run back to back with upper-bound grids.  Nodes beyond max_nodes are
+// not written: the build then sees *overflow set and falls back to the greedy collapse.
 template <bool kDp>
-__global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in,
+__global__ void k_collapse(const unsigned int* __restrict__ n_items_dev, const CollapseItem* __restrict__ in,
                            CollapseItem* __restrict__ out, unsigned int* __restrict__ out_count,
                            unsigned int* __restrict__ slot_counter, const uint32_t* __restrict__ left,
                            const uint32_t* __restrict__ right, const float4* __restrict__ plo,
@@ -600,7 +601,7 @@ __global__ void k_collapse(uint32_t n_items, const CollapseItem* __restrict__ in
                            uint32_t* __restrict__ pos, unsigned int* __restrict__ leaf_counter, DpTables T,
                            uint32_t max_nodes, unsigned int* __restrict__ overflow) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_items) return;
+  if (t >= *n_items_dev) return;
   const CollapseItem it = in[t];
   uint32_t refs[32], offs[32];
   uint32_t leafmask = 0;  // kDp: internal refs that are leaves
@@ -913,7 +914,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     // value read bounds the grids of the next chunk.
     // A chain of nested boxes (concentric Gaussians of growing size) merges about one pair per
     // pass; past kMaxPasses the build drops the clustering and uses the Karras tree instead.
-    constexpr int kChunk = 8;
+    constexpr int kChunk = 16;
     constexpr int kMaxPasses = 1024;
     uint32_t m = n, made = 0u;
     int pass = 0;
@@ -1028,40 +1029,58 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
       VP_CUDA(cudaGetLastError());
     }
     Scratch<CollapseItem> qa(st), qb(st);
-    Scratch<unsigned int> ctr(st);
+    Scratch<unsigned int> ctr(st), lvl(st);
+    constexpr int kMaxLevels = 512;  // BVH32 depth bound (a PLOC chain of 1,024 passes stays far below)
+    constexpr int kLevelChunk = 4;   // levels between host reads
     if ((s = dev_alloc(&qa.p, max_wide, st))) return s;
     if ((s = dev_alloc(&qb.p, max_wide, st))) return s;
-    if ((s = dev_alloc(&ctr.p, 4, st))) return s;
-    // A level-by-level collapse; an SAH cut that needs more nodes than the greedy bound is redone
-    // greedily.
+    if ((s = dev_alloc(&ctr.p, 3, st))) return s;
+    if ((s = dev_alloc(&lvl.p, kMaxLevels + 1, st))) return s;
+    // A level-by-level collapse: lvl[k] = items (BVH32 nodes to fill) at level k, counted on the
+    // device; the host reads the counts every kLevelChunk levels.  An SAH cut that needs more
+    // nodes than the greedy bound is redone greedily.
     for (int attempt = 0; attempt < 2; ++attempt) {
       CollapseItem root{wide_root, 0u, 0u, 0u};
       VP_CUDA(cudaMemcpyAsync(qa.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
-      unsigned int c0[4] = {1u, 0u, 0u, 0u};  // next free slot, next-level queue length, leaves, overflow
+      const unsigned int c0[3] = {1u, 0u, 0u};  // next free slot, leaves, overflow
       VP_CUDA(cudaMemcpyAsync(ctr.p, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
-      uint32_t n_items = 1;
-      depth = 0;
-      unsigned int ch[4] = {0u, 0u, 0u, 0u};
-      while (n_items > 0) {
-        ++depth;
-        VP_CUDA(cudaMemsetAsync(ctr.p + 1, 0, sizeof(unsigned int), st));
-        const unsigned grid = (n_items + 127) / 128;
-        if (dp)
-          k_collapse<true><<<grid, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p, wlo,
-                                                 whi, wide, kLeafMax, pos.p, ctr.p + 2, T, max_wide, ctr.p + 3);
-        else
-          k_collapse<false><<<grid, 128, 0, st>>>(n_items, qa.p, qb.p, ctr.p + 1, ctr.p, wl, wr, plo.p, phi.p, wlo,
-                                                  whi, wide, kLeafMax, pos.p, ctr.p + 2, T, max_wide, ctr.p + 3);
-        VP_CUDA(cudaGetLastError());
+      VP_CUDA(cudaMemsetAsync(lvl.p, 0, sizeof(unsigned int) * (kMaxLevels + 1), st));
+      const unsigned int one = 1u;
+      VP_CUDA(cudaMemcpyAsync(lvl.p, &one, sizeof(one), cudaMemcpyHostToDevice, st));
+      uint64_t bound = 1;  // upper bound of the items at the next level to launch
+      int k = 0;
+      bool done = false, over = false;
+      while (!done) {
+        for (int c = 0; c < kLevelChunk; ++c, ++k) {
+          if (k >= kMaxLevels) return fail(VP_ERROR_INTERNAL, "BVH32 deeper than 512 levels");
+          const unsigned grid = (unsigned)((bound + 127) / 128);
+          CollapseItem* qin = (k & 1) ? qb.p : qa.p;
+          CollapseItem* qout = (k & 1) ? qa.p : qb.p;
+          if (dp)
+            k_collapse<true><<<grid, 128, 0, st>>>(lvl.p + k, qin, qout, lvl.p + k + 1, ctr.p, wl, wr, plo.p, phi.p,
+                                                   wlo, whi, wide, kLeafMax, pos.p, ctr.p + 1, T, max_wide, ctr.p + 2);
+          else
+            k_collapse<false><<<grid, 128, 0, st>>>(lvl.p + k, qin, qout, lvl.p + k + 1, ctr.p, wl, wr, plo.p, phi.p,
+                                                    wlo, whi, wide, kLeafMax, pos.p, ctr.p + 1, T, max_wide, ctr.p + 2);
+          VP_CUDA(cudaGetLastError());
+          bound = std::min<uint64_t>(bound * 32u, max_wide);  // each item makes at most 32 children
+        }
+        unsigned int ch[3], next = 0u;
         VP_CUDA(cudaMemcpyAsync(ch, ctr.p, sizeof(ch), cudaMemcpyDeviceToHost, st));
+        VP_CUDA(cudaMemcpyAsync(&next, lvl.p + k, sizeof(next), cudaMemcpyDeviceToHost, st));
         VP_CUDA(cudaStreamSynchronize(st));
-        n_items = ch[1];
         wide_nodes = ch[0];
-        leaves = ch[2];
-        std::swap(qa.p, qb.p);
-        if (ch[3] != 0u) break;
+        leaves = ch[1];
+        over = ch[2] != 0u;
+        bound = next;
+        done = over || next == 0u;
       }
-      if (ch[3] == 0u) {
+      if (!over) {
+        std::vector<unsigned int> counts(k + 1);
+        VP_CUDA(cudaMemcpyAsync(counts.data(), lvl.p, sizeof(unsigned int) * (k + 1), cudaMemcpyDeviceToHost, st));
+        VP_CUDA(cudaStreamSynchronize(st));
+        depth = 0;
+        while (depth < (uint32_t)k && counts[depth] != 0u) ++depth;
         dp_used = dp;
         break;
       }
