@@ -12,6 +12,9 @@
 //   --phase-g F              Henyey-Greenstein g (default 0.85)
 //   --ris [--ris-candidates N]   product RIS NEE (default: MIS)
 //   --measure-caps           print the device counters (hits per ray, point overlap)
+//   --adaptive-threshold F [--adaptive-min-samples N]   adaptive sampling (the reference's
+//                            compile-time ADAPTIVE_THRESHOLD / ADAPTIVE_MIN_SAMPLES,
+//                            device/core/constants.cuh:196-211; default off, 32)
 //   --ply PATH               Gaussian PLY (x y z rot_0..3 scale_0..2 albedo_0..2 sigma_t_0);
 //                            default: main.cpp's single purple Gaussian at the origin
 //   --sigma-multiplier F     density multiplier (ply.cpp:116; default 1)
@@ -50,7 +53,8 @@ struct Args {
   std::string output = "output.exr", env_map, ply;
   uint32_t width = 1000, height = 750, spp = 1, seed = 42, max_depth = 128, rr_depth = 12, ris_k = 6;
   float rr_max_survival = 0.99f, firefly = 0.f, filter = 0.f, phase_g = 0.85f, sigma = 1.f, vfov = 90.f,
-        ortho_h = 0.f;
+        ortho_h = 0.f, adaptive = 0.f;
+  uint32_t adaptive_min = 32;
   float eye[3] = {0.f, 0.f, -1.f}, lookat[3] = {0.f, 0.f, 0.f}, up[3] = {0.f, 1.f, 0.f};
   float albedo[3] = {-1.f, -1.f, -1.f};
   bool ris = false, measure = false;
@@ -86,6 +90,8 @@ Args parse(int argc, char** argv) {
     else if (o == "--rr-depth") need(i, 1), a.rr_depth = u32(argv[++i]);
     else if (o == "--rr-max-survival") need(i, 1), a.rr_max_survival = f32(argv[++i]);
     else if (o == "--firefly-clamp") need(i, 1), a.firefly = f32(argv[++i]);
+    else if (o == "--adaptive-threshold") need(i, 1), a.adaptive = f32(argv[++i]);
+    else if (o == "--adaptive-min-samples") need(i, 1), a.adaptive_min = u32(argv[++i]);
     else if (o == "--filter-width") need(i, 1), a.filter = f32(argv[++i]);
     else if (o == "--phase-g") need(i, 1), a.phase_g = f32(argv[++i]);
     else if (o == "--raygen" || o == "--miss" || o == "--anyhit" || o == "--launch_params" ||
@@ -126,6 +132,7 @@ Args parse(int argc, char** argv) {
   if (!(a.phase_g >= -0.999f && a.phase_g <= 0.999f)) die("--phase-g must be in [-0.999, 0.999]");
   if (!(a.rr_max_survival >= 0.f && a.rr_max_survival <= 1.f)) die("--rr-max-survival must be in [0, 1]");
   if (!(a.firefly >= 0.f)) die("--firefly-clamp must be non-negative");
+  if (!(a.adaptive >= 0.f)) die("--adaptive-threshold must be non-negative");
   if (!(a.filter >= 0.f)) die("--filter-width must be non-negative");
   if (a.width == 0 || a.height == 0 || a.spp == 0) die("--width, --height and --samples_per_pixel must be positive");
   return a;
@@ -179,6 +186,7 @@ int main(int argc, char** argv) {
   p.ris_candidates = a.ris_k;
   p.engine = a.engine, p.precision = a.precision;
   p.measure = a.measure ? VP_MEASURE_COUNTERS : 0;
+  p.adaptive_threshold = a.adaptive, p.adaptive_min_samples = a.adaptive_min;
 
   std::vector<float> rgba(4ull * a.width * a.height);
   vp_render_stats st{};
@@ -191,6 +199,9 @@ int main(int argc, char** argv) {
   std::printf("rendered %ux%u x %u spp of %u Gaussians in %.3f s (%.3f ms on the device, %.2f Mpaths/s) -> %s\n",
               a.width, a.height, a.spp, info.count, secs, st.ms_kernels,
               (double)st.paths / (st.ms_kernels * 1e-3) / 1e6, a.output.c_str());
+  if (st.paths_skipped)
+    std::printf("adaptive sampling: %llu of %llu paths skipped\n", (unsigned long long)st.paths_skipped,
+                (unsigned long long)(st.paths + st.paths_skipped));
   if (a.measure)
     std::printf("max hits per ray %u, max point overlap %u, crossings %llu, shadow rays %llu\n", st.max_hits_per_ray,
                 st.max_point_overlap, (unsigned long long)st.crossings, (unsigned long long)st.shadow_rays);

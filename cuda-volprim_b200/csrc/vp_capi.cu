@@ -127,6 +127,8 @@ ParamsView make_params(const vp_render_params& p, const vp_scene* s) {
   P.accurate = p.precision == VP_PRECISION_ACCURATE ||
                (p.precision == VP_PRECISION_AUTO && s->view.albedo_all_zero);
   P.measure = p.measure & VP_MEASURE_COUNTERS;
+  P.adaptive_threshold = p.adaptive_threshold;
+  P.adaptive_min_samples = p.adaptive_min_samples;
   return P;
 }
 
@@ -143,6 +145,8 @@ vp_status check_params(const vp_render_params* p) {
   if (p->precision < VP_PRECISION_AUTO || p->precision > VP_PRECISION_ACCURATE)
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown precision");
   if (!(p->hg_g > -1.0f && p->hg_g < 1.0f)) return fail(VP_ERROR_INVALID_ARGUMENT, "hg_g must be in (-1, 1)");
+  if (!(p->adaptive_threshold >= 0.0f && p->adaptive_threshold <= 3.402823466e38f))
+    return fail(VP_ERROR_INVALID_ARGUMENT, "adaptive_threshold must be finite and non-negative");
   return VP_OK;
 }
 
@@ -366,6 +370,8 @@ vp_status vp_render_params_default(vp_render_params* p) {
   p->engine = VP_ENGINE_WAVEFRONT;
   p->precision = VP_PRECISION_AUTO;
   p->measure = 0;
+  p->adaptive_threshold = 0.0f;   // ADAPTIVE_THRESHOLD (constants.cuh:207): off
+  p->adaptive_min_samples = 32;   // ADAPTIVE_MIN_SAMPLES (constants.cuh:202)
   return VP_OK;
 }
 
@@ -398,6 +404,8 @@ vp_status vp_image_clear(vp_image* im) {
   const size_t n = (size_t)im->width * im->height;
   VP_CUDA(cudaMemsetAsync(im->mean, 0, n * sizeof(float4), im->ctx->stream));
   VP_CUDA(cudaMemsetAsync(im->count, 0, n * sizeof(uint32_t), im->ctx->stream));
+  if (im->m2) VP_CUDA(cudaMemsetAsync(im->m2, 0, n * sizeof(float4), im->ctx->stream));
+  im->m2_complete = true;
   return VP_OK;
 }
 
@@ -405,6 +413,7 @@ vp_status vp_image_destroy(vp_image* im) {
   if (!im) return VP_OK;
   cudaStream_t st = im->ctx ? im->ctx->stream : nullptr;
   dev_free(im->mean, st);
+  dev_free(im->m2, st);
   dev_free(im->count, st);
   if (st) cudaStreamSynchronize(st);
   delete im;
@@ -441,6 +450,27 @@ vp_status vp_image_device_buffers(vp_image* im, void** mean, void** count) {
   return VP_OK;
 }
 
+vp_status vp_image_read_welford(vp_image* im, float* out_m2, uint32_t* out_count, int32_t memory) {
+  if (!im) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL image");
+  if (memory != VP_MEMORY_HOST && memory != VP_MEMORY_DEVICE) return fail(VP_ERROR_INVALID_ARGUMENT, "bad memory kind");
+  if (out_m2 && !im->m2_complete)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "M2 is incomplete: a batch since the last clear ran without adaptive sampling");
+  cudaStream_t st = im->ctx->stream;
+  const size_t n = (size_t)im->width * im->height;
+  const cudaMemcpyKind kind = memory == VP_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  VP_CUDA(cudaSetDevice(im->ctx->device));
+  if (out_m2 && im->m2) {
+    VP_CUDA(cudaMemcpyAsync(out_m2, im->m2, n * sizeof(float4), kind, st));
+  } else if (out_m2) {  // no adaptive batch since the image was made: no samples, M2 = 0
+    VP_CUDA(cudaStreamSynchronize(st));
+    if (memory == VP_MEMORY_HOST) std::memset(out_m2, 0, n * sizeof(float4));
+    else VP_CUDA(cudaMemsetAsync(out_m2, 0, n * sizeof(float4), st));
+  }
+  if (out_count) VP_CUDA(cudaMemcpyAsync(out_count, im->count, n * sizeof(uint32_t), kind, st));
+  VP_CUDA(cudaStreamSynchronize(st));
+  return VP_OK;
+}
+
 vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, const vp_render_params* p,
                                vp_image* im, uint32_t spp_offset, uint32_t spp_count, vp_render_stats* stats) {
   if (!s || !e || !cam || !im) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
@@ -451,6 +481,20 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
   if ((uint64_t)spp_offset + spp_count > p->spp) return fail(VP_ERROR_INVALID_ARGUMENT, "sample range exceeds params->spp");
   vp_context* ctx = s->ctx;
   VP_CUDA(cudaSetDevice(ctx->device));
+  // Adaptive sampling reads M2, which only adaptive batches keep (the reference allocates and
+  // updates it only when ENABLE_ADAPTIVE_SAMPLING is compiled in, image.h:43-57).
+  if (spp_count > 0 && p->adaptive_threshold > 0.0f) {
+    if (!im->m2_complete)
+      return fail(VP_ERROR_INVALID_ARGUMENT,
+                  "adaptive sampling needs every batch since the image's last clear to keep M2 (adaptive_threshold > 0)");
+    if (!im->m2) {
+      const size_t n = (size_t)im->width * im->height;
+      if ((st = dev_alloc(&im->m2, n, ctx->stream))) return st;
+      VP_CUDA(cudaMemsetAsync(im->m2, 0, n * sizeof(float4), ctx->stream));
+    }
+  } else if (spp_count > 0) {
+    im->m2_complete = false;
+  }
   CameraView cv;
   build_camera(*cam, p->width, p->height, cv);
   const ParamsView P = make_params(*p, s);
@@ -478,7 +522,8 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
     VP_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     std::memset(stats, 0, sizeof(*stats));
     stats->ms_kernels = ms;
-    stats->paths = (uint64_t)p->width * p->height * spp_count;
+    stats->paths = (uint64_t)p->width * p->height * spp_count - c.skipped;
+    stats->paths_skipped = c.skipped;
     stats->bounces = c.bounces;
     stats->scatters = c.scatters;
     stats->crossings = c.crossings;

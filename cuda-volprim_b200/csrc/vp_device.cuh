@@ -100,6 +100,8 @@ struct ParamsView {
   float hg_g, hg_g_eff, hg_one_plus_g2, hg_one_minus_g2, hg_neg_inv_2g, hg_phase_coeff;
   int32_t accurate;
   int32_t measure;
+  float adaptive_threshold;  // 0: adaptive sampling off
+  uint32_t adaptive_min_samples;
 };
 
 struct Counters {  // device-side statistics (only touched when ParamsView::measure)
@@ -108,6 +110,7 @@ struct Counters {  // device-side statistics (only touched when ParamsView::meas
   // Gaussian records loaded
   unsigned long long kind_nodes[3], kind_leaves[3], kind_prims[3], kind_geo[3];
   unsigned int max_hits, max_overlap, status;
+  unsigned long long skipped;  // paths of converged pixels not traced (adaptive sampling)
 };
 
 // ---- small vector helpers ----------------------------------------------------------------

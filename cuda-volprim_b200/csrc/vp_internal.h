@@ -118,6 +118,10 @@ struct vp_image {
   uint32_t width = 0, height = 0;
   float4* mean = nullptr;
   uint32_t* count = nullptr;
+  // Welford sum of squared deviations per channel (w unused), allocated by the first batch with
+  // adaptive sampling.  m2_complete: every batch since the last clear kept it.
+  float4* m2 = nullptr;
+  bool m2_complete = true;
 };
 
 namespace vp {

@@ -146,4 +146,32 @@ __device__ __forceinline__ float3 finalize_sample(const ParamsView& P, float3 ra
   return rad;
 }
 
+// Adaptive-sampling test on a pixel's Welford state before a batch (raygen.cuh:52-67 with
+// constants.cuh:202-211): converged when every channel's sample standard deviation
+// sqrt(M2 / (n - 1)) is below threshold x max(mean, 1e-6).  The reference's float3 divisions
+// are multiplications by a round-to-nearest reciprocal; they are written out here with the _rn
+// intrinsics so that no contraction changes a rounding.  Its max is `a > b ? a : b`
+// (math.h:218-226), kept for the same answer when a rounding makes M2 a tiny negative number
+// (a NaN error).  n >= 2 keeps n - 1 non-zero when the caller's minimum is 0 or 1.
+constexpr float kAdaptiveMinLuminance = 1e-6f;
+__device__ __forceinline__ bool pixel_converged(const ParamsView& P, uint32_t n, float4 mean, float4 m2) {
+  if (!(P.adaptive_threshold > 0.0f) || n < P.adaptive_min_samples || n < 2u) return false;
+  auto mx = [](float a, float b) { return a > b ? a : b; };
+  const float inv_n1 = __frcp_rn((float)(n - 1u));
+  auto err = [&](float m2c, float mc) {
+    return __fmul_rn(__fsqrt_rn(__fmul_rn(m2c, inv_n1)), __frcp_rn(mx(mc, kAdaptiveMinLuminance)));
+  };
+  return mx(mx(err(m2.x, mean.x), err(m2.y, mean.y)), err(m2.z, mean.z)) < P.adaptive_threshold;
+}
+
+// One Welford step of a pixel's mean (and, with kM2, M2) for its k-th sample (k = 1, 2, ...;
+// raygen.cuh:214-222): delta1 = L - mean, mean += delta1 * rcp(k), M2 += delta1 * (L - mean).
+template <bool kM2>
+__device__ __forceinline__ void welford_step(float3& m, float3& m2, float3 L, uint32_t k) {
+  const float n_inv = __frcp_rn((float)k);
+  const float3 d1 = sub(L, m);
+  m = add(m, mul(d1, n_inv));
+  if constexpr (kM2) m2 = add(m2, mul(d1, sub(L, m)));
+}
+
 }  // namespace vp

@@ -21,6 +21,7 @@
 // starts at t <= 0; the active set at a point is the set of ellipsoids containing it), so no
 // per-ray capacity limit exists.
 #include <algorithm>
+#include <type_traits>
 
 #include "vp_internal.h"
 #include "vp_path.cuh"
@@ -114,10 +115,12 @@ __device__ __forceinline__ void flush_stats(Counters* c, const PathStats& ps, co
 
 // Persistent warp-per-path kernel: warps pull pixels from a global counter; each pixel runs
 // samples [spp_offset, spp_offset + spp_count) in order and Welford-updates mean/count.
-template <bool kAcc, bool kMeasure>
+// kAdaptive also keeps M2 and skips converged pixels (M2 stays out of the registers of the
+// plain variant, whose sample loop has none to spare).
+template <bool kAcc, bool kMeasure, bool kAdaptive>
 __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneView S, EnvView E, CameraView C,
                                                      ParamsView P, float4* __restrict__ mean,
-                                                     uint32_t* __restrict__ count,
+                                                     float4* __restrict__ m2, uint32_t* __restrict__ count,
                                                      uint32_t spp_offset, uint32_t spp_count,
                                                      unsigned int* __restrict__ work,
                                                      Counters* __restrict__ ctr) {
@@ -137,14 +140,22 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
     const uint32_t px = item % P.width, py = item / P.width;
     const uint32_t prev = count[item];
     const float4 m4 = mean[item];
-    float3 m = f3(m4.x, m4.y, m4.z);
+    float3 m = f3(m4.x, m4.y, m4.z), m2c = f3(0.f, 0.f, 0.f);
+    if constexpr (kAdaptive) {
+      const float4 q4 = m2[item];
+      if (pixel_converged(P, prev, m4, q4)) {  // the same state on every lane: a warp-uniform skip
+        if (lane == 0) atomicAdd(&ctr->skipped, (unsigned long long)spp_count);
+        continue;
+      }
+      m2c = f3(q4.x, q4.y, q4.z);
+    }
     for (uint32_t s = 0; s < spp_count; ++s) {
       const float3 L = trace_path(S, E, C, P, q, px, py, (uint64_t)spp_offset + s, ps);
-      const float n_inv = __frcp_rn((float)(prev + s + 1u));
-      m = add(m, mul(sub(L, m), n_inv));  // Welford mean (raygen.cuh:214-219)
+      welford_step<kAdaptive>(m, m2c, L, prev + s + 1u);
     }
     if (lane == 0) {
       mean[item] = make_float4(m.x, m.y, m.z, 0.f);
+      if constexpr (kAdaptive) m2[item] = make_float4(m2c.x, m2c.y, m2c.z, 0.f);
       count[item] = prev + spp_count;
     }
     if (status) break;
@@ -155,9 +166,10 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
 // ------------------------------------------------------------------------------------------
 // megakernel (thread per pixel, binary LBVH)
 // ------------------------------------------------------------------------------------------
-template <bool kAcc>
+template <bool kAcc, bool kAdaptive>
 __global__ void __launch_bounds__(128) k_render_mega(SceneView S, EnvView E, CameraView C, ParamsView P,
-                                                     float4* __restrict__ mean, uint32_t* __restrict__ count,
+                                                     float4* __restrict__ mean, float4* __restrict__ m2,
+                                                     uint32_t* __restrict__ count,
                                                      uint32_t spp_offset, uint32_t spp_count,
                                                      Counters* __restrict__ ctr) {
   const uint32_t px = blockIdx.x * 16 + (threadIdx.x & 15);
@@ -171,14 +183,19 @@ __global__ void __launch_bounds__(128) k_render_mega(SceneView S, EnvView E, Cam
     const uint32_t item = py * P.width + px;
     const uint32_t prev = count[item];
     const float4 m4 = mean[item];
-    float3 m = f3(m4.x, m4.y, m4.z);
-    for (uint32_t s = 0; s < spp_count; ++s) {
-      const float3 L = trace_path(S, E, C, P, q, px, py, (uint64_t)spp_offset + s, ps);
-      const float n_inv = __frcp_rn((float)(prev + s + 1u));
-      m = add(m, mul(sub(L, m), n_inv));
+    const float4 q4 = kAdaptive ? m2[item] : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (kAdaptive && pixel_converged(P, prev, m4, q4)) {
+      atomicAdd(&ctr->skipped, (unsigned long long)spp_count);
+    } else {
+      float3 m = f3(m4.x, m4.y, m4.z), m2c = f3(q4.x, q4.y, q4.z);
+      for (uint32_t s = 0; s < spp_count; ++s) {
+        const float3 L = trace_path(S, E, C, P, q, px, py, (uint64_t)spp_offset + s, ps);
+        welford_step<kAdaptive>(m, m2c, L, prev + s + 1u);
+      }
+      mean[item] = make_float4(m.x, m.y, m.z, 0.f);
+      if constexpr (kAdaptive) m2[item] = make_float4(m2c.x, m2c.y, m2c.z, 0.f);
+      count[item] = prev + spp_count;
     }
-    mean[item] = make_float4(m.x, m.y, m.z, 0.f);
-    count[item] = prev + spp_count;
   }
   if (status) atomicOr(&ctr->status, status);
   if (P.measure && inside) flush_stats(ctr, ps, ws, 0u, true);
@@ -297,20 +314,24 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
     const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kHitCap);
     if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the warp engine's shared-memory stack");
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
-    auto kern = P.accurate ? (P.measure ? k_render_warp<true, true> : k_render_warp<true, false>)
-                           : (P.measure ? k_render_warp<false, true> : k_render_warp<false, false>);
+    const bool adaptive = P.adaptive_threshold > 0.0f;
+    auto pick = [&](auto acc) {
+      constexpr bool kA = decltype(acc)::value;
+      return adaptive ? (P.measure ? k_render_warp<kA, true, true> : k_render_warp<kA, false, true>)
+                      : (P.measure ? k_render_warp<kA, true, false> : k_render_warp<kA, false, false>);
+    };
+    auto kern = P.accurate ? pick(std::true_type{}) : pick(std::false_type{});
     if (smem > 48 * 1024) VP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int blocks = ctx->sm_count * occupancy_blocks(kern, threads, smem);
-    kern<<<blocks, threads, smem, st>>>(s->view, e->view, cam, P, img->mean, img->count, spp_offset, spp_count,
+    kern<<<blocks, threads, smem, st>>>(s->view, e->view, cam, P, img->mean, img->m2, img->count, spp_offset, spp_count,
                                         ctx->work_counter, ctx->counters);
   } else if (engine == VP_ENGINE_MEGAKERNEL) {
     const dim3 grid((P.width + 15) / 16, (P.height + 7) / 8);
-    if (P.accurate)
-      k_render_mega<true><<<grid, 128, 0, st>>>(s->view, e->view, cam, P, img->mean, img->count, spp_offset,
-                                               spp_count, ctx->counters);
-    else
-      k_render_mega<false><<<grid, 128, 0, st>>>(s->view, e->view, cam, P, img->mean, img->count, spp_offset,
-                                                spp_count, ctx->counters);
+    const bool adaptive = P.adaptive_threshold > 0.0f;
+    auto kern = P.accurate ? (adaptive ? k_render_mega<true, true> : k_render_mega<true, false>)
+                           : (adaptive ? k_render_mega<false, true> : k_render_mega<false, false>);
+    kern<<<grid, 128, 0, st>>>(s->view, e->view, cam, P, img->mean, img->m2, img->count, spp_offset, spp_count,
+                               ctx->counters);
   } else {
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown engine");
   }

@@ -782,6 +782,8 @@ vp_status vp_server_submit(vp_server* s, const vp_request* r, uint64_t* request_
   vp_status st;
   if ((st = check_params(&r->params))) return st;
   if (r->params.max_bounces == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "max_bounces must be positive for a served request");
+  if (r->params.adaptive_threshold > 0.0f)  // a request's paths are summed, not kept per pixel per batch
+    return fail(VP_ERROR_INVALID_ARGUMENT, "adaptive sampling is not available for a served request");
   if (s->cfg.memory_budget_bytes && s->bytes_fixed + request_bytes(*r) > s->cfg.memory_budget_bytes)
     return fail(VP_ERROR_LIMIT, "request does not fit the memory budget");
   const uint64_t id = s->next_id++;

@@ -98,21 +98,38 @@ __device__ __forceinline__ uint32_t queue_reserve(uint32_t* counter, uint32_t n)
   return base + incl - n;
 }
 
+// Path p is sample p % batch of pixel p / batch.  Without adaptive sampling every path starts
+// and queue slot p holds path p.  With it, the host has cleared the counters and only the paths
+// of pixels that have not converged join the queue (their order within a warp is kept).
 __global__ void k_wf_generate(CameraView C, ParamsView P, uint32_t spp_offset, uint32_t batch, uint32_t n,
-                              WfBuffers b) {
+                              WfBuffers b, const float4* __restrict__ mean, const float4* __restrict__ m2,
+                              const uint32_t* __restrict__ count, Counters* __restrict__ ctr) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p == 0) {
-    b.ctr[0] = P.max_bounces > 0 ? n : 0u;
-    b.ctr[1] = b.ctr[2] = b.ctr[3] = b.ctr[4] = 0u;
+  const bool adaptive = P.adaptive_threshold > 0.0f;
+  uint32_t slot = p;
+  if (!adaptive) {
+    if (p == 0) {
+      b.ctr[0] = P.max_bounces > 0 ? n : 0u;
+      b.ctr[1] = b.ctr[2] = b.ctr[3] = b.ctr[4] = 0u;
+    }
+    if (p >= n) return;
+  } else {
+    bool live = false;
+    if (p < n) {
+      const uint32_t pixel = p / batch;
+      live = !pixel_converged(P, count[pixel], mean[pixel], m2[pixel]);
+      if (!live && p % batch == 0u) atomicAdd(&ctr->skipped, (unsigned long long)batch);
+    }
+    slot = queue_reserve(b.ctr + 0, live ? 1u : 0u);  // all 32 lanes: blockDim is a multiple of 32
+    if (!live) return;
   }
-  if (p >= n) return;
   const uint32_t pixel = p / batch, s = p % batch;
   PathState st = start_path(C, P, pixel % P.width, pixel / P.width, (uint64_t)spp_offset + s);
   const uint64_t key = draw_bounce_key(st.rng);
   store_path(b, p, st);
   b.key2[p] = make_uint2((uint32_t)key, (uint32_t)(key >> 32));
   b.meta[p] = 0u | kAliveBit;
-  b.qa[p] = p;
+  b.qa[slot] = p;
   b.L4[p] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -296,19 +313,24 @@ __global__ void k_wf_advance(uint32_t* ctr) {
 }
 
 // Welford mean over the batch's samples of each pixel, in sample order (raygen.cuh:214-242).
-__global__ void k_wf_welford(WfBuffers b, uint32_t batch, uint32_t n_pix, float4* __restrict__ mean,
-                             uint32_t* __restrict__ count) {
+// With adaptive sampling it also keeps M2, and a pixel that k_wf_generate found converged (the
+// same test on the same, still unchanged state) keeps its state.
+__global__ void k_wf_welford(ParamsView P, WfBuffers b, uint32_t batch, uint32_t n_pix, float4* __restrict__ mean,
+                             float4* __restrict__ m2, uint32_t* __restrict__ count) {
   const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= n_pix) return;
+  const bool adaptive = P.adaptive_threshold > 0.0f;
   const uint32_t prev = count[pix];
   const float4 m4 = mean[pix];
-  float3 m = f3(m4.x, m4.y, m4.z);
+  const float4 q4 = adaptive ? m2[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (adaptive && pixel_converged(P, prev, m4, q4)) return;
+  float3 m = f3(m4.x, m4.y, m4.z), q = f3(q4.x, q4.y, q4.z);
   for (uint32_t s = 0; s < batch; ++s) {
     const float4 L = b.L4[(size_t)pix * batch + s];
-    const float n_inv = __frcp_rn((float)(prev + s + 1u));
-    m = add(m, mul(sub(f3(L.x, L.y, L.z), m), n_inv));
+    welford_step<true>(m, q, f3(L.x, L.y, L.z), prev + s + 1u);
   }
   mean[pix] = make_float4(m.x, m.y, m.z, 0.f);
+  if (adaptive) m2[pix] = make_float4(q.x, q.y, q.z, 0.f);
   count[pix] = prev + batch;
 }
 
@@ -454,7 +476,9 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
     pending = 0;
     return cudaSuccess;
   };
-  k_wf_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, P, spp_offset, spp_count, paths, b);
+  if (P.adaptive_threshold > 0.0f) VP_CUDA(cudaMemsetAsync(b.ctr, 0, 5 * sizeof(uint32_t), st));
+  k_wf_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, P, spp_offset, spp_count, paths, b, img->mean, img->m2,
+                                                     img->count, ctx->counters);
   VP_CUDA(cudaGetLastError());
   ctx->launches += 1;
   uint32_t* qcur = b.qa;
@@ -502,7 +526,7 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
       if (polled == 0u) break;
     }
   }
-  k_wf_welford<<<(n_pix + 255) / 256, 256, 0, st>>>(b, spp_count, n_pix, img->mean, img->count);
+  k_wf_welford<<<(n_pix + 255) / 256, 256, 0, st>>>(P, b, spp_count, n_pix, img->mean, img->m2, img->count);
   VP_CUDA(cudaGetLastError());
   ctx->launches += 1;
   if (timed && pending) {

@@ -107,6 +107,8 @@ class vp_render_params(C.Structure):
         ("engine", C.c_int32),
         ("precision", C.c_int32),
         ("measure", C.c_int32),
+        ("adaptive_threshold", C.c_float),
+        ("adaptive_min_samples", C.c_uint32),
     ]
 
 
@@ -133,6 +135,7 @@ class vp_render_stats(C.Structure):
         ("ms_stage", C.c_double * 3),
         ("stage_launches", C.c_uint32 * 3),
         ("reserved", C.c_uint32),
+        ("paths_skipped", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -231,6 +234,7 @@ SIGNATURES = {
     "vp_image_destroy": [P],
     "vp_image_read": [P, P, C.c_int32],
     "vp_image_device_buffers": [P, PP, PP],
+    "vp_image_read_welford": [P, P, P, C.c_int32],
     "vp_render_accumulate": [P, P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, C.c_uint32,
                              C.c_uint32, C.POINTER(vp_render_stats)],
     "vp_render": [P, P, C.POINTER(vp_camera), C.POINTER(vp_render_params), P, C.c_int32,

@@ -361,6 +361,11 @@ class Config:
     engine: str = "wavefront"   # "wavefront" | "warp" | "megakernel"
     precision: str = "auto"     # "auto" | "fast" | "accurate"
     batch_spp: int = 16         # BATCH_SIZE (renderer.cpp:32)
+    # adaptive sampling (ADAPTIVE_THRESHOLD / ADAPTIVE_MIN_SAMPLES, constants.cuh:196-211): a pixel
+    # with at least adaptive_min_samples samples whose largest per-channel std-dev / mean is below
+    # adaptive_threshold takes no more batches; 0 = off (the reference's default)
+    adaptive_threshold: float = 0.0
+    adaptive_min_samples: int = 32
 
     def to_c(self) -> _capi.vp_render_params:
         p = _capi.vp_render_params()
@@ -378,6 +383,7 @@ class Config:
         p.precision = {"auto": 0, "fast": 1, "accurate": 2}[self.precision]
         p.measure = ((_capi.VP_MEASURE_COUNTERS if self.measure_caps else 0)
                      | (_capi.VP_MEASURE_STAGES if self.time_stages else 0))
+        p.adaptive_threshold, p.adaptive_min_samples = self.adaptive_threshold, self.adaptive_min_samples
         return p
 
 
@@ -443,6 +449,15 @@ class ProgressiveImage:
         img = np.empty((self.height, self.width, 4), dtype=np.float32)
         check(lib.vp_image_read(self.handle, img.ctypes.data, _capi.VP_MEMORY_HOST))
         return img
+
+    def read_welford(self, m2: bool = True):
+        """(M2 (H, W, 3) float32 or None, sample counts (H, W) uint32).  M2 exists only while every
+        batch since the last clear ran with adaptive sampling on."""
+        q = np.empty((self.height, self.width, 4), dtype=np.float32) if m2 else None
+        n = np.empty((self.height, self.width), dtype=np.uint32)
+        check(lib.vp_image_read_welford(self.handle, q.ctypes.data if m2 else None, n.ctypes.data,
+                                        _capi.VP_MEMORY_HOST))
+        return (q[..., :3] if m2 else None), n
 
     def close(self):
         if getattr(self, "handle", None):

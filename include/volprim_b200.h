@@ -243,6 +243,14 @@ typedef struct vp_render_params {
   int32_t measure;         /* bit set: VP_MEASURE_COUNTERS counts crossings, bounces, shadow rays
                               and maxima (costs atomics); VP_MEASURE_STAGES times the wavefront
                               stages with CUDA events (no device-side cost) */
+  /* Adaptive sampling (ADAPTIVE_THRESHOLD / ADAPTIVE_MIN_SAMPLES, device/core/constants.cuh:
+   * 196-211; the test of device/entry/raygen.cuh:52-67).  Before each batch, a pixel that already
+   * holds n >= max(adaptive_min_samples, 2) samples takes none in this batch when
+   *   max over r, g, b of  sqrt(M2 * rcp(n - 1)) * rcp(max(mean, 1e-6))  <  adaptive_threshold
+   * (M2: the pixel's Welford sum of squared deviations; rcp and sqrt rounded to nearest, as the
+   * reference's math::rcp / math::sqrt).  0 (the default, the reference's value) turns it off. */
+  float adaptive_threshold;
+  uint32_t adaptive_min_samples;   /* default 32 */
 } vp_render_params;
 
 /* Fills the reference's defaults (config.h:119-136, launch_params.h:38-58). */
@@ -250,7 +258,7 @@ vp_status vp_render_params_default(vp_render_params* out);
 
 typedef struct vp_render_stats {
   double ms_kernels;           /* device time of the render launches (CUDA events) */
-  uint64_t paths;              /* width * height * spp */
+  uint64_t paths;              /* paths traced: width * height * spp less paths_skipped */
   uint64_t bounces;            /* scatter-or-escape events        (measure != 0) */
   uint64_t scatters;           /* events that scattered           (measure != 0) */
   uint64_t crossings;          /* closed-form (ray, Gaussian) evaluations (measure != 0) */
@@ -275,15 +283,19 @@ typedef struct vp_render_stats {
                                                                              (measure stages) */
   uint32_t stage_launches[3];  /* launches in each ms_stage bucket            (measure stages) */
   uint32_t reserved;
+  uint64_t paths_skipped;      /* paths not traced because their pixel had converged (adaptive
+                                  sampling); paths counts only the traced ones (always counted) */
 } vp_render_stats;
 
 /* ---------------------------------------------------------------------------------------- */
 /* rendering                                                                                */
 /* ---------------------------------------------------------------------------------------- */
 
-/* Progressive Welford image (float4 mean + uint32 count per pixel).  Replaces
+/* Progressive Welford image (float4 mean, float4 M2 and uint32 count per pixel).  Replaces
  * host::params::Image (include/thesis/host/params/image.h) and device::params::Image
- * (include/thesis/device/params/image.h:15-38). */
+ * (include/thesis/device/params/image.h:15-38).  M2, the running sum of squared deviations,
+ * is kept on every render (the reference allocates it only when adaptive sampling is compiled
+ * in), so adaptive sampling can be switched on for any batch. */
 vp_status vp_image_create(vp_context* ctx, uint32_t width, uint32_t height, vp_image** out);
 vp_status vp_image_clear(vp_image* image);
 vp_status vp_image_destroy(vp_image* image);
@@ -291,9 +303,14 @@ vp_status vp_image_destroy(vp_image* image);
 vp_status vp_image_read(vp_image* image, float* out_rgba, int32_t memory);
 /* Raw device pointers (float4 mean[W*H], uint32 count[W*H]). */
 vp_status vp_image_device_buffers(vp_image* image, void** mean, void** count);
+/* Copies the Welford state: out_m2_rgba (W*H*4 floats: M2 per channel, alpha 0) and out_count
+ * (W*H samples per pixel), both in `memory` (host or device); either may be NULL. */
+vp_status vp_image_read_welford(vp_image* image, float* out_m2_rgba, uint32_t* out_count, int32_t memory);
 
 /* Renders samples [spp_offset, spp_offset + spp_count) of a params->spp-sample render into
- * image (Welford update).  Replaces one Renderer::render batch iteration
+ * image (Welford update).  With params->adaptive_threshold > 0 every batch first skips the pixels
+ * that pass the adaptive test and keeps M2; that needs every batch since the image's last clear
+ * to have kept M2, else VP_ERROR_INVALID_ARGUMENT.  Replaces one Renderer::render batch iteration
  * (renderer.cpp:353-376 -> optixLaunch of __raygen__rg, device/entry/raygen.cuh:21-243). */
 vp_status vp_render_accumulate(vp_scene* scene, vp_env* env, const vp_camera* camera,
                                const vp_render_params* params, vp_image* image,

@@ -67,6 +67,11 @@ def lib() -> C.CDLL:
         L.or_render.restype = C.c_double
         L.or_render.argtypes = [C.c_void_p, C.c_void_p, F, U, F, C.c_uint32, C.c_uint32, C.c_uint32,
                                 C.c_uint32, C.c_int, F]
+        L.or_render_welford.restype = C.c_double
+        L.or_render_welford.argtypes = [C.c_void_p, C.c_void_p, F, U, F, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_float, C.c_uint32, C.c_int, F, F, U]
+        L.or_welford_step.argtypes = [F, C.c_uint32, F]
+        L.or_adaptive_converged.argtypes = [F, F, U, C.c_uint32, C.c_float, C.c_uint32, C.POINTER(C.c_uint8)]
         L.or_albedo_at.argtypes = [C.c_void_p, F, C.c_uint32, F, U]
         L.or_transform.argtypes = [C.c_void_p, C.c_uint32, F, F, F]
         L.or_morton3d.restype = C.c_uint32
@@ -232,6 +237,48 @@ def render_absorption_fp64(scene: OracleScene, env: OracleEnv, cam16, width, hei
 NEE = {"mis": 0, "phase": 1, "ris": 2, "none": 3}
 
 
+def _render_params(config, rng_mode="keyed"):
+    nee = "ris" if config.use_ris else config.nee
+    pu = np.array([config.image_width, config.image_height, config.num_samples_per_pixel, config.seed,
+                   config.max_bounces, config.rr_depth, NEE[nee], config.ris_num_candidates,
+                   1 if rng_mode == "keyed" else 0], np.uint32)
+    pf = np.array([config.rr_max_survival, config.hg_g, config.firefly_clamp_luminance,
+                   config.pixel_filter_stddev], np.float32)
+    return pu, pf
+
+
+def adaptive_converged(mean, m2, count, threshold, min_samples):
+    """The adaptive-sampling test (raygen.cuh:52-67) on Welford states: mean and m2 (..., 3),
+    count (...); returns a bool array of count's shape."""
+    mean = _f(np.asarray(mean).reshape(-1, 3))
+    m2 = _f(np.asarray(m2).reshape(-1, 3))
+    cnt = np.ascontiguousarray(np.asarray(count).reshape(-1), np.uint32)
+    out = np.empty(cnt.size, np.uint8)
+    lib().or_adaptive_converged(_p(mean), _p(m2), _p(cnt, U), cnt.size, threshold, min_samples,
+                                out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return out.reshape(np.shape(count)).astype(bool)
+
+
+def render_welford(scene: OracleScene, env: OracleEnv, cam16, config, state=None, s0=0, s1=None, threads=0):
+    """FP32 restatement of the progressive render with the reference's Welford state and its
+    adaptive-sampling test (raygen.cuh:31-67, :210-242), for samples [s0, s1) in batches of
+    config.batch_spp, with config.adaptive_threshold / adaptive_min_samples.
+
+    state: (mean (H, W, 3) float32, M2 (H, W, 3) float32, count (H, W) uint32), updated in place;
+    None starts from an empty image.  Returns (state, elapsed seconds)."""
+    W, H = config.image_width, config.image_height
+    s1 = config.num_samples_per_pixel if s1 is None else s1
+    if state is None:
+        state = (np.zeros((H, W, 3), np.float32), np.zeros((H, W, 3), np.float32), np.zeros((H, W), np.uint32))
+    mean, m2, cnt = state
+    assert mean.flags.c_contiguous and m2.flags.c_contiguous and cnt.flags.c_contiguous
+    pu, pf = _render_params(config)
+    secs = lib().or_render_welford(scene.h, env.h, _p(_f(cam16)), _p(pu, U), _p(pf), s0, s1, config.batch_spp,
+                                   config.adaptive_threshold, config.adaptive_min_samples, int(threads),
+                                   _p(mean), _p(m2), _p(cnt, U))
+    return state, secs
+
+
 def render(scene: OracleScene, env: OracleEnv, cam16, config, y0=0, y1=None, s0=0, s1=None,
            rng_mode="keyed", threads=0):
     """FP32 restatement of the path tracer over rows [y0, y1) and samples [s0, s1).
@@ -240,11 +287,7 @@ def render(scene: OracleScene, env: OracleEnv, cam16, config, y0=0, y1=None, s0=
     W, H = config.image_width, config.image_height
     y1 = H if y1 is None else y1
     s1 = config.num_samples_per_pixel if s1 is None else s1
-    nee = "ris" if config.use_ris else config.nee
-    pu = np.array([W, H, config.num_samples_per_pixel, config.seed, config.max_bounces, config.rr_depth,
-                   NEE[nee], config.ris_num_candidates, 1 if rng_mode == "keyed" else 0], np.uint32)
-    pf = np.array([config.rr_max_survival, config.hg_g, config.firefly_clamp_luminance,
-                   config.pixel_filter_stddev], np.float32)
+    pu, pf = _render_params(config, rng_mode)
     out = np.empty((y1 - y0) * W * 3, np.float32)
     secs = lib().or_render(scene.h, env.h, _p(_f(cam16)), _p(pu, U), _p(pf), y0, y1, s0, s1, int(threads), _p(out))
     return out.reshape(y1 - y0, W, 3), secs
@@ -272,5 +315,8 @@ def ref_lib():
         L.ref_camera.argtypes = [F, F, F, C.c_float, C.c_float, C.c_int, C.c_uint, C.c_uint, F]
         L.ref_morton3d.restype = C.c_uint
         L.ref_morton3d.argtypes = [F, F, F]
+        L.ref_adaptive_constants.argtypes = [F]
+        L.ref_adaptive_error.argtypes = [F, F, C.c_uint, F]
+        L.ref_welford_step.argtypes = [F, C.c_uint, F]
         _ref = L
     return _ref

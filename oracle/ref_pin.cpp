@@ -5,8 +5,11 @@
 // (include/thesis/common/geometry/intersection.h:56-61), the host camera build
 // (include/thesis/host/params/camera.h:106-216) and the Morton code
 // (include/thesis/host/utils/math.h:103-131), so the oracle's restatement of them can be checked
-// against the reference's code itself.  The device-only parts of the path (OptiX programs,
-// sampling.cuh) need the OptiX SDK and are not built here.
+// against the reference's code itself.  It also exposes the adaptive-sampling constants
+// (device/core/constants.cuh:196-211) and evaluates the raygen's Welford update and convergence
+// test (device/entry/raygen.cuh:52-67, 214-222: a few lines of a device-only file, written out
+// here) with the reference's own float3 operators and math::rcp / sqrt / max.  The device-only
+// parts of the path (OptiX programs, sampling.cuh) need the OptiX SDK and are not built here.
 // <cstdint> first: the reference's own build provides it through its precompiled header.
 #include <cstdint>
 
@@ -14,6 +17,7 @@
 #include "thesis/common/geometry/intersection.h"
 #include "thesis/host/params/camera.h"
 #include "thesis/host/utils/math.h"
+#include "device/core/constants.cuh"
 
 #include <cstring>
 
@@ -74,6 +78,44 @@ unsigned ref_morton3d(const float* pos3, const float* scene_min3, const float* i
   return thesis::host::utils::math::morton3D(make_float3(pos3[0], pos3[1], pos3[2]),
                                              make_float3(scene_min3[0], scene_min3[1], scene_min3[2]),
                                              make_float3(inv_extent3[0], inv_extent3[1], inv_extent3[2]));
+}
+
+// out4: ENABLE_ADAPTIVE_SAMPLING (0/1), ADAPTIVE_MIN_SAMPLES, ADAPTIVE_THRESHOLD,
+// ADAPTIVE_MIN_LUMINANCE
+void ref_adaptive_constants(float* out4) {
+  namespace k = thesis::device::consts;
+  out4[0] = k::ENABLE_ADAPTIVE_SAMPLING ? 1.0f : 0.0f;
+  out4[1] = static_cast<float>(k::ADAPTIVE_MIN_SAMPLES);
+  out4[2] = k::ADAPTIVE_THRESHOLD;
+  out4[3] = k::ADAPTIVE_MIN_LUMINANCE;
+}
+
+// The convergence statistic of raygen.cuh:56-63 for a pixel with prev_count >= 2 samples:
+// out4 = per-channel error (3) and its max.
+void ref_adaptive_error(const float* mean3, const float* m2_3, unsigned prev_count, float* out4) {
+  namespace m = thesis::common::math;
+  const auto mean = make_float3(mean3[0], mean3[1], mean3[2]);
+  const auto M2 = make_float3(m2_3[0], m2_3[1], m2_3[2]);
+  const auto variance = M2 * m::rcp(static_cast<float>(prev_count - 1));
+  const auto std_dev = m::sqrt(variance);
+  const auto lum = thesis::device::consts::ADAPTIVE_MIN_LUMINANCE;
+  const auto safe_mean = make_float3(m::max(mean.x, lum), m::max(mean.y, lum), m::max(mean.z, lum));
+  const auto err = std_dev / safe_mean;
+  out4[0] = err.x, out4[1] = err.y, out4[2] = err.z, out4[3] = m::max(err);
+}
+
+// One Welford step of raygen.cuh:214-222 for sample number k (1-based): io6 = mean[3], M2[3].
+void ref_welford_step(const float* L3, unsigned k, float* io6) {
+  namespace m = thesis::common::math;
+  const auto radiance = make_float3(L3[0], L3[1], L3[2]);
+  auto mean = make_float3(io6[0], io6[1], io6[2]);
+  auto M2 = make_float3(io6[3], io6[4], io6[5]);
+  const auto n_inv = m::rcp(static_cast<float>(k));
+  const auto delta1 = radiance - mean;
+  mean += delta1 * n_inv;
+  const auto delta2 = radiance - mean;
+  M2 += delta1 * delta2;
+  io6[0] = mean.x, io6[1] = mean.y, io6[2] = mean.z, io6[3] = M2.x, io6[4] = M2.y, io6[5] = M2.z;
 }
 
 }  // extern "C"

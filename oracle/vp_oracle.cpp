@@ -1326,6 +1326,85 @@ double or_render(void* sv, void* ev, const float* cam16, const uint32_t* pu, con
   return omp_get_wtime() - t0;
 }
 
+// Adaptive-sampling test of one pixel (raygen.cuh:52-67, constants.cuh:202-211): with at least
+// max(min_samples, 2) samples, converged when max over channels of
+// sqrt(M2 * rcp(n - 1)) * rcp(max(mean, 1e-6)) is below the threshold; threshold <= 0 is off.
+// max(a, b) is a > b ? a : b, as the reference's math::max.
+static bool adaptive_converged(float threshold, uint32_t min_samples, uint32_t n, const float* mean,
+                               const float* m2) {
+  if (!(threshold > 0.0f) || n < min_samples || n < 2u) return false;
+  auto mx = [](float a, float b) { return a > b ? a : b; };
+  const float inv_n1 = 1.0f / static_cast<float>(n - 1u);
+  float e[3];
+  for (int k = 0; k < 3; ++k) e[k] = std::sqrt(m2[k] * inv_n1) * (1.0f / mx(mean[k], 1e-6f));
+  return mx(mx(e[0], e[1]), e[2]) < threshold;
+}
+
+// One Welford step for the k-th sample (k = 1, 2, ...; raygen.cuh:214-222):
+//   delta1 = L - mean;  mean += delta1 * rcp(k);  M2 += delta1 * (L - mean)
+static inline void welford_update(float* m, float* q, const float* L, uint32_t k) {
+  const float n_inv = 1.0f / static_cast<float>(k);
+  for (int j = 0; j < 3; ++j) {
+    const float d1 = L[j] - m[j];
+    m[j] = m[j] + d1 * n_inv;
+    q[j] = q[j] + d1 * (L[j] - m[j]);
+  }
+}
+
+// io6 = mean[3], M2[3], updated by sample L3 as sample number k.
+void or_welford_step(const float* L3, uint32_t k, float* io6) { welford_update(io6, io6 + 3, L3, k); }
+
+// Flags of the adaptive-sampling test over n pixels' Welford states (mean3, m2_3, count).
+void or_adaptive_converged(const float* mean3, const float* m2_3, const uint32_t* count, uint32_t n,
+                           float threshold, uint32_t min_samples, uint8_t* out) {
+  for (uint32_t i = 0; i < n; ++i)
+    out[i] = adaptive_converged(threshold, min_samples, count[i], mean3 + 3ull * i, m2_3 + 3ull * i) ? 1 : 0;
+}
+
+// Progressive FP32 render into a Welford image (raygen.cuh:31-67 and :210-242): samples
+// [s0, s1) in batches of `batch`; before each batch a pixel whose state passes the adaptive test
+// skips it; otherwise each sample updates mean and M2 (welford_update) and the count, in sample
+// order.  mean3 / m2_3 / count hold the whole image (W*H pixels) and are updated in place.  Returns
+// elapsed seconds.
+double or_render_welford(void* sv, void* ev, const float* cam16, const uint32_t* pu, const float* pf, uint32_t s0,
+                         uint32_t s1, uint32_t batch, float threshold, uint32_t min_samples, int n_threads,
+                         float* mean3, float* m2_3, uint32_t* count) {
+  const Scene& S = *static_cast<Scene*>(sv);
+  const Env& E = *static_cast<Env*>(ev);
+  Camera c{mk(cam16[0], cam16[1], cam16[2]), mk(cam16[3], cam16[4], cam16[5]), mk(cam16[6], cam16[7], cam16[8]),
+           mk(cam16[9], cam16[10], cam16[11]), mk(cam16[12], cam16[13], cam16[14]), static_cast<int>(cam16[15])};
+  Params P{};
+  P.width = pu[0], P.height = pu[1], P.spp = pu[2], P.seed = pu[3], P.max_bounces = pu[4], P.rr_depth = pu[5];
+  P.nee_mode = static_cast<int32_t>(pu[6]), P.ris_k = pu[7], P.rng_mode = static_cast<int32_t>(pu[8]);
+  P.rr_max_survival = pf[0], P.hg_g = pf[1], P.firefly_clamp = pf[2], P.filter_stddev = pf[3];
+  fold_hg(P);
+  const uint32_t W = P.width;
+  if (batch == 0) batch = s1 - s0;
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  const double t0 = omp_get_wtime();
+#pragma omp parallel
+  {
+    Tracer t{S, E, c, P, {}};
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t k = 0; k < static_cast<int64_t>(P.height) * W; ++k) {
+      const uint32_t px = static_cast<uint32_t>(k % W), py = static_cast<uint32_t>(k / W);
+      float* m = mean3 + 3 * k;
+      float* q = m2_3 + 3 * k;
+      for (uint32_t b0 = s0; b0 < s1; b0 += batch) {
+        const uint32_t b1 = std::min(s1, b0 + batch);
+        if (adaptive_converged(threshold, min_samples, count[k], m, q)) continue;
+        for (uint32_t s = b0; s < b1; ++s) {
+          const F3 L = t.trace(px, py, s);
+          const float Lc[3] = {L.x, L.y, L.z};
+          welford_update(m, q, Lc, count[k] + (s - b0) + 1u);
+        }
+        count[k] += b1 - b0;
+      }
+    }
+  }
+  return omp_get_wtime() - t0;
+}
+
 // Candidate Gaussians of n rays over [0, inf): the caller's indices of every Gaussian whose padded
 // 3-sigma box the ray meets (CPU BVH; all Gaussians without one).  Two passes: with idx == NULL
 // it writes counts[n]; then, with offsets[n] = exclusive prefix sums of counts, it fills idx.

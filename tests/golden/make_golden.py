@@ -54,6 +54,51 @@ def primitive_cases():
     return cases
 
 
+def radiance_samples(rng, n):
+    """Path-tracer-like per-sample radiance: mostly log-normal, some zero paths, rare fireflies."""
+    L = np.exp(rng.normal(-1.0, 1.0, (n, 3))) * (rng.uniform(size=(n, 1)) < 0.8)
+    L[rng.uniform(size=n) < 0.02] *= 300.0
+    return L.astype(np.float32)
+
+
+def adaptive_cases(R):
+    """Adaptive-sampling constants (device/core/constants.cuh:196-211), Welford sequences
+    (raygen.cuh:214-222) and convergence statistics (raygen.cuh:56-63) from the reference's
+    own operators."""
+    k4 = np.empty(4, np.float32)
+    R.ref_adaptive_constants(O._p(k4))
+    rng = np.random.default_rng(99)
+    io = np.empty(6, np.float32)
+    welford, states = [], []
+    for n in (1, 2, 5, 33, 100, 300):
+        L = radiance_samples(rng, n)
+        io[:] = 0.0
+        for k in range(n):
+            R.ref_welford_step(f32p(L[k]), k + 1, O._p(io))
+        welford.append({"L": bits(L), "out": bits(io)})
+        if n >= 2:
+            states.append((io[:3].copy(), io[3:].copy(), n))
+    for n in (2, 3, 16, 32, 64, 1000, (1 << 24) + 3):  # synthetic states
+        mean = np.exp(rng.normal(-1.0, 1.0, 3)).astype(np.float32)
+        m2 = (mean * mean * rng.uniform(0.0, 0.2, 3) * (n - 1)).astype(np.float32)
+        states.append((mean, m2, n))
+    tiny = np.float32(1e-7)
+    states += [  # edges: a black channel (mean below 1e-6), constant samples (M2 = 0), and a
+        # rounding-negative M2 (a NaN error) in the first and in the last channel
+        (np.array([0.5, 0.0, 2e-7], np.float32), np.array([0.01, 0.0, 1e-12], np.float32), 40),
+        (np.array([0.3, 0.3, 0.3], np.float32), np.zeros(3, np.float32), 50),
+        (np.array([0.3, 0.2, 0.1], np.float32), np.array([-tiny, 0.02, 0.01], np.float32), 40),
+        (np.array([0.3, 0.2, 0.1], np.float32), np.array([0.02, 0.01, -tiny], np.float32), 40),
+    ]
+    e4 = np.empty(4, np.float32)
+    errors = []
+    for mean, m2, n in states:
+        R.ref_adaptive_error(f32p(mean), f32p(m2), n, O._p(e4))
+        errors.append({"mean": bits(mean), "m2": bits(m2), "count": int(n), "err": bits(e4)})
+    return {"enable": bool(k4[0]), "min_samples": int(k4[1]), "threshold": bits([k4[2]])[0],
+            "min_luminance": bits([k4[3]])[0], "welford": welford, "errors": errors}
+
+
 def main():
     O.build()
     R = O.ref_lib()
@@ -109,6 +154,7 @@ def main():
     # PCG32 reference implementation demo (pcg32_srandom_r(42, 54)): first six outputs
     out["pcg32"] = {"seed": 42, "sequence": 54,
                     "outputs": [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]}
+    out["adaptive"] = adaptive_cases(R)
     path = Path(__file__).resolve().parent / "reference_pin.json"
     path.write_text(json.dumps(out, indent=1))
     print(f"wrote {path} ({path.stat().st_size} bytes)")

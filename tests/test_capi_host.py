@@ -55,6 +55,8 @@ def test_version_and_defaults():
     assert p.firefly_clamp == 0.0 and p.pixel_filter_stddev == 0.0
     assert p.nee_mode == vp.VP_NEE_MIS and p.ris_candidates == 6 and p.batch_spp == 16
     assert p.engine == _capi.VP_ENGINE_WAVEFRONT
+    # ADAPTIVE_THRESHOLD (off) and ADAPTIVE_MIN_SAMPLES (device/core/constants.cuh:202-207)
+    assert p.adaptive_threshold == 0.0 and p.adaptive_min_samples == 32
 
 
 def test_scene_option_defaults():
@@ -79,12 +81,14 @@ def test_null_arguments_are_errors_not_crashes():
 def test_config_maps_to_c_params():
     cfg = vp.Config(num_samples_per_pixel=256, image_width=512, image_height=256, seed=9, max_bounces=64,
                     rr_depth=12, hg_g=0.0, use_ris=True, ris_num_candidates=4, engine="megakernel",
-                    precision="accurate", batch_spp=8, measure_caps=True)
+                    precision="accurate", batch_spp=8, measure_caps=True, adaptive_threshold=0.05,
+                    adaptive_min_samples=16)
     p = cfg.to_c()
     assert (p.width, p.height, p.spp, p.seed, p.max_bounces) == (512, 256, 256, 9, 64)
     assert p.nee_mode == vp.VP_NEE_RIS and p.ris_candidates == 4
     assert p.engine == vp.VP_ENGINE_MEGAKERNEL and p.precision == vp.VP_PRECISION_ACCURATE
     assert p.batch_spp == 8 and p.measure == 1
+    assert abs(p.adaptive_threshold - 0.05) < 1e-8 and p.adaptive_min_samples == 16
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -115,4 +119,4 @@ def test_struct_layouts_match_header(tmp_path):
             assert int(got[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
     assert C.sizeof(_capi.vp_gaussians) == 56
     assert C.sizeof(_capi.vp_camera) == 48
-    assert C.sizeof(_capi.vp_render_params) == 64
+    assert C.sizeof(_capi.vp_render_params) == 72

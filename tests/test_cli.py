@@ -40,6 +40,8 @@ def run(exe, *args, cwd=None):
     (["--rr-max-survival", "1.5"], "--rr-max-survival must be in"),
     (["--firefly-clamp", "-1"], "--firefly-clamp must be non-negative"),
     (["--max-depth", "0"], "--max-depth must be positive"),
+    (["--adaptive-threshold", "-0.1"], "--adaptive-threshold must be non-negative"),
+    (["--adaptive-min-samples", "x"], "not an unsigned integer"),
     (["--engine", "optix"], "unknown engine optix"),
     (["--precision", "half"], "unknown precision half"),
 ])

@@ -197,6 +197,9 @@ def test_invalid_requests_raise(vp_ctx, world):
     bad = vp.Config(**{**r.config.__dict__, "max_bounces": 0})
     with pytest.raises(vp.VpError, match="max_bounces"):
         srv.submit(0, r.camera, bad)
+    adaptive = vp.Config(**{**r.config.__dict__, "adaptive_threshold": 0.1})
+    with pytest.raises(vp.VpError, match="adaptive sampling"):
+        srv.submit(0, r.camera, adaptive)
     srv.close()
     tiny = new_server(vp_ctx, world)
     fixed = tiny.stats()["bytes_in_use"]

@@ -158,3 +158,88 @@ def test_live_reference_pin_random():
         R.ref_primitive(O._p(m), O._p(s), O._p(q), O._p(a), float(M), O._p(out))
         sc = O.OracleScene(m[None], s[None], q[None], np.array([M]), a[None])
         assert sc.records[0].view(np.uint32).tolist() == out.view(np.uint32).tolist()
+
+
+ADAPTIVE = GOLDEN["adaptive"]
+
+
+def test_adaptive_constants_match_reference():
+    """ENABLE_ADAPTIVE_SAMPLING, ADAPTIVE_MIN_SAMPLES, ADAPTIVE_THRESHOLD and
+    ADAPTIVE_MIN_LUMINANCE (device/core/constants.cuh:196-211): the render defaults keep the
+    reference's (off, 32), and the test's luminance floor is the reference's 1e-6f."""
+    import ctypes as C
+    from volprim_b200 import _capi
+    p = _capi.vp_render_params()
+    _capi.check(_capi.lib.vp_render_params_default(C.byref(p)))
+    assert ADAPTIVE["enable"] is False
+    assert p.adaptive_min_samples == ADAPTIVE["min_samples"] == 32
+    assert np.float32(p.adaptive_threshold).view(np.uint32) == ADAPTIVE["threshold"]
+    assert np.float32(1e-6).view(np.uint32) == ADAPTIVE["min_luminance"]
+
+
+def test_welford_matches_reference():
+    """The oracle's Welford step against the reference's own float3 operators (raygen.cuh:214-222),
+    bit for bit, over heavy-tailed radiance sequences."""
+    io = np.empty(6, np.float32)
+    for case in ADAPTIVE["welford"]:
+        L = f(case["L"]).reshape(-1, 3)
+        io[:] = 0.0
+        for k in range(L.shape[0]):
+            O.lib().or_welford_step(O._p(np.ascontiguousarray(L[k])), k + 1, O._p(io))
+        assert io.view(np.uint32).tolist() == case["out"], L.shape
+
+
+def test_adaptive_test_matches_reference():
+    """The oracle's convergence test decides err_max < threshold on the reference's own statistic
+    (raygen.cuh:56-65): not converged at threshold = err_max, converged one ulp above it, never
+    converged when the reference's max is NaN (a rounding-negative M2 in the last channel), and
+    the NaN of the first channel dropped as the reference's `a > b ? a : b` drops it."""
+    seen_nan = 0
+    for case in ADAPTIVE["errors"]:
+        mean, m2, n = f(case["mean"]), f(case["m2"]), case["count"]
+        err = f(case["err"])[3]
+        at = O.adaptive_converged(mean[None], m2[None], [n], float(err), 0)[0] if np.isfinite(err) else None
+        if not np.isfinite(err):
+            seen_nan += 1
+            for thr in (1e-3, 1.0, 1e30):
+                assert not O.adaptive_converged(mean[None], m2[None], [n], thr, 0)[0]
+            continue
+        above = float(np.nextafter(err, np.float32(np.inf)))
+        assert not at, case
+        assert O.adaptive_converged(mean[None], m2[None], [n], above, 0)[0], case
+        # below the minimum sample count the test never passes (raygen.cuh:55)
+        assert not O.adaptive_converged(mean[None], m2[None], [n], above, n + 1)[0]
+    assert seen_nan == 1
+
+
+def test_oracle_welford_render_and_adaptive_batches():
+    """The oracle's progressive render: its mean and M2 are those of the per-sample radiances, and
+    with adaptive sampling a pixel takes a batch exactly when its state before the batch fails the
+    test."""
+    import volprim_b200 as vp
+    rng = np.random.default_rng(3)
+    n = 40
+    g = vp.Gaussians(rng.uniform(-0.5, 0.5, (n, 3)), np.exp(rng.normal(math.log(0.2), 0.3, (n, 3))),
+                     scenes.uniform_quaternions(rng, n), np.exp(rng.normal(0, 0.5, n)),
+                     rng.uniform(0.3, 0.9, (n, 3)))
+    W = H = 8
+    cfg = vp.Config(num_samples_per_pixel=48, image_width=W, image_height=H, seed=4, hg_g=0.3, max_bounces=16,
+                    batch_spp=8)
+    sc = O.OracleScene.from_gaussians(g, sigma_multiplier=2.0)
+    env = O.OracleEnv.constant(1.0, 0.8, 0.6)
+    c16 = O.camera16(scenes.negz_camera(2.5, 40.0), W, H)
+    per = np.stack([O.render(sc, env, c16, cfg, s0=s, s1=s + 1)[0] for s in range(48)]).astype(np.float64)
+    (mean, m2, cnt), _ = O.render_welford(sc, env, c16, cfg)
+    assert np.all(cnt == 48)
+    np.testing.assert_allclose(mean, per.mean(0), rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(m2, ((per - per.mean(0)) ** 2).sum(0), rtol=1e-4, atol=1e-6)
+    cfg.adaptive_threshold, cfg.adaptive_min_samples = 0.6, 16
+    state = None
+    for b0 in range(0, 48, 8):
+        before = None if state is None else tuple(a.copy() for a in state)
+        state, _ = O.render_welford(sc, env, c16, cfg, state=state, s0=b0, s1=b0 + 8)
+        if before is not None:
+            conv = O.adaptive_converged(before[0], before[1], before[2], 0.6, 16)
+            assert np.array_equal(state[2], before[2] + np.where(conv, 0, 8))
+            assert np.array_equal(state[0][conv], before[0][conv])
+    assert 0 < np.sum(state[2] < 48) < W * H, "some, not all, pixels must stop early"
