@@ -39,7 +39,7 @@ enum {
   VP_ERROR_INVALID_ARGUMENT = -1, /* bad pointer, size or parameter */
   VP_ERROR_CUDA = -2,             /* a CUDA runtime call failed */
   VP_ERROR_OUT_OF_MEMORY = -3,    /* device allocation failed */
-  VP_ERROR_UNSUPPORTED = -4,      /* option not supported by this build */
+  VP_ERROR_UNSUPPORTED = -4,      /* option the library does not support */
   VP_ERROR_LIMIT = -5,            /* a size exceeds a documented limit */
   VP_ERROR_DEVICE_STATUS = -6,    /* a kernel reported an error word (e.g. stack bound) */
   VP_ERROR_INTERNAL = -7
