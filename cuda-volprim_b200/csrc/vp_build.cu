@@ -775,16 +775,70 @@ struct Scratch {  // stream-ordered temporary, freed on scope exit
 
 }  // namespace
 
+// A scene without Gaussians (the reference builds an instance AS over zero instances and every
+// ray misses; test/scenes/geometric_validation.cpp empty_scene): one BVH32 root and one binary
+// root whose children are all empty, and one zeroed element in each per-Gaussian array so that
+// no pointer is null.  Every traversal tests the root's children, finds none, and ends.
+vp_status build_empty_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier,
+                            const vp_scene_options& opt, vp_scene* sc) {
+  cudaStream_t st = ctx->stream;
+  float ref_empty;
+  std::memcpy(&ref_empty, &kEmptyRef, sizeof(ref_empty));
+  const float4 lo_empty = make_float4(INFINITY, INFINITY, INFINITY, ref_empty);
+  const float4 hi_empty = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+  float4 wide_h[64], bin_h[4];
+  for (int c = 0; c < 32; ++c) wide_h[c] = lo_empty, wide_h[32 + c] = hi_empty;
+  bin_h[0] = bin_h[2] = lo_empty;
+  bin_h[1] = bin_h[3] = hi_empty;
+  vp_status s;
+  if ((s = dev_alloc(&sc->prims, 4, st)) || (s = dev_alloc(&sc->perm, 1, st)) || (s = dev_alloc(&sc->pbox, 2, st)) ||
+      (s = dev_alloc(&sc->raw, 2, st)) || (s = dev_alloc(&sc->wide, 64, st)) || (s = dev_alloc(&sc->bin, 4, st)))
+    return s;
+  VP_CUDA(cudaMemsetAsync(sc->prims, 0, 4 * sizeof(float4), st));
+  VP_CUDA(cudaMemsetAsync(sc->perm, 0, sizeof(uint32_t), st));
+  VP_CUDA(cudaMemsetAsync(sc->pbox, 0, 2 * sizeof(float4), st));
+  VP_CUDA(cudaMemsetAsync(sc->raw, 0, 2 * sizeof(float4), st));
+  VP_CUDA(cudaMemcpyAsync(sc->wide, wide_h, sizeof(wide_h), cudaMemcpyHostToDevice, st));
+  VP_CUDA(cudaMemcpyAsync(sc->bin, bin_h, sizeof(bin_h), cudaMemcpyHostToDevice, st));
+  VP_CUDA(cudaStreamSynchronize(st));
+  sc->ctx = ctx;
+  sc->scale_is_log = g->scale_is_log ? 1 : 0;
+  sc->sigma_multiplier = sigma_multiplier;
+  SceneView& v = sc->view;
+  v.prims = sc->prims;
+  v.perm = sc->perm;
+  v.wide = sc->wide;
+  v.bin = sc->bin;
+  v.pbox = sc->pbox;
+  v.count = 0u;
+  v.wide_root = 0u;
+  v.bin_root = 0u;
+  v.stack_cap = 31u + 2u;
+  v.albedo_all_zero = 1;
+  vp_scene_info& info = sc->info;
+  info = vp_scene_info{};
+  info.wide_nodes = 1;
+  info.wide_depth = 1;
+  info.binary_nodes = 1;
+  info.wide_builder = opt.wide_builder;
+  info.binary_builder = opt.binary_builder;
+  info.leaf_max = opt.leaf_max;
+  info.wide_collapse = opt.wide_collapse;
+  info.albedo_all_zero = 1;
+  info.device_bytes = 64ull + 4ull + 32ull + 32ull + 1024ull + 64ull;
+  return VP_OK;
+}
+
 vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multiplier, const vp_scene_options& opt,
                       vp_scene* sc) {
   cudaStream_t st = ctx->stream;
   const uint32_t n = g->count;
-  if (n == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "scene has no Gaussians");
   if (n >= (1u << 26)) return fail(VP_ERROR_LIMIT, "scene exceeds 2^26 Gaussians");
-  if (!g->mean || !g->scale || !g->quat_wxyz || !g->density)
-    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_gaussians: mean, scale, quat_wxyz and density are required");
   if (!(sigma_multiplier > 0.f) || !std::isfinite(sigma_multiplier))
     return fail(VP_ERROR_INVALID_ARGUMENT, "sigma_multiplier must be positive and finite");
+  if (n == 0) return build_empty_scene(ctx, g, sigma_multiplier, opt, sc);
+  if (!g->mean || !g->scale || !g->quat_wxyz || !g->density)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_gaussians: mean, scale, quat_wxyz and density are required");
 
   VP_CUDA(cudaEventRecord(ctx->ev0, st));
   // Inputs on the device.

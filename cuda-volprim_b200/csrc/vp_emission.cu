@@ -413,6 +413,7 @@ struct Common {
 vp_status prepare(vp_scene* s, vp_env* e, const vp_camera* cam, const vp_render_params* p, Common& c) {
   if (!s || !e || !cam || !p) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
   if (s->ctx != e->ctx) return fail(VP_ERROR_INVALID_ARGUMENT, "objects belong to different contexts");
+  if (s->info.count == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "the emission model needs a scene with Gaussians");
   if (p->width == 0 || p->height == 0 || p->spp == 0)
     return fail(VP_ERROR_INVALID_ARGUMENT, "width, height and spp must be positive");
   if ((uint64_t)p->width * p->height >= (1ull << 32)) return fail(VP_ERROR_LIMIT, "image too large");
@@ -453,7 +454,9 @@ using namespace vp;
 extern "C" {
 
 vp_status vp_scene_set_emission(vp_scene* s, const float* rgb, int32_t memory) {
-  if (!s || !rgb) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (!s) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (s->info.count == 0) return fail(VP_ERROR_INVALID_ARGUMENT, "the emission model needs a scene with Gaussians");
+  if (!rgb) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
   if (memory != VP_MEMORY_HOST && memory != VP_MEMORY_DEVICE) return fail(VP_ERROR_INVALID_ARGUMENT, "bad memory kind");
   VP_CUDA(cudaSetDevice(s->ctx->device));
   cudaStream_t st = s->ctx->stream;

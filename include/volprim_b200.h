@@ -152,7 +152,8 @@ typedef struct vp_scene_info {
  * the BVH over 3-sigma ellipsoid bounds on the device (Morton codes, radix sort, PLOC clustering
  * or Karras hierarchy + refit, collapse to a 32-wide BVH).  Replaces Renderer::initPrimsAndGAS
  * (renderer.cpp:85-173: host Morton sort + OptiX GAS/IAS build).  No primitive-count cap below
- * 2^26 (the reference caps at 65,535, renderer.cpp:54-59). */
+ * 2^26 (the reference caps at 65,535, renderer.cpp:54-59).  count 0 makes an empty scene that
+ * every ray misses (the reference's IAS over zero instances); the emission model rejects it. */
 vp_status vp_scene_create(vp_context* ctx, const vp_gaussians* prims, float sigma_multiplier,
                           vp_scene** out);
 

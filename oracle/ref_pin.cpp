@@ -5,7 +5,8 @@
 // (include/thesis/common/geometry/intersection.h:56-61), the host camera build
 // (include/thesis/host/params/camera.h:106-216) and the Morton code
 // (include/thesis/host/utils/math.h:103-131), so the oracle's restatement of them can be checked
-// against the reference's code itself.  It also exposes the adaptive-sampling constants
+// against the reference's code itself.  It also returns the test runner's geometric validation
+// scenes (test/scenes/geometric_validation.cpp, compiled in), exposes the adaptive-sampling constants
 // (device/core/constants.cuh:196-211) and evaluates the raygen's Welford update and convergence
 // test (device/entry/raygen.cuh:52-67, 214-222: a few lines of a device-only file, written out
 // here) with the reference's own float3 operators and math::rcp / sqrt / max.  The device-only
@@ -18,6 +19,7 @@
 #include "thesis/host/params/camera.h"
 #include "thesis/host/utils/math.h"
 #include "device/core/constants.cuh"
+#include "scenes/geometric_validation.h"
 
 #include <cstring>
 
@@ -78,6 +80,30 @@ unsigned ref_morton3d(const float* pos3, const float* scene_min3, const float* i
   return thesis::host::utils::math::morton3D(make_float3(pos3[0], pos3[1], pos3[2]),
                                              make_float3(scene_min3[0], scene_min3[1], scene_min3[2]),
                                              make_float3(inv_extent3[0], inv_extent3[1], inv_extent3[2]));
+}
+
+// The test runner's geometric validation and stress scenes (test/scenes/geometric_validation.cpp,
+// compiled from the reference's source beside this file): the number of scenes, then scene i's
+// name (NUL-terminated, at most name_cap bytes) and, for its first `cap` Gaussians, 14 floats
+// each: centre[3], forward rotation (w, x, y, z) (the stored rotation is its conjugate), scale[3],
+// albedo[3], optical thickness.  Returns the scene's Gaussian count.
+int ref_validation_scene_count() { return static_cast<int>(thesis::test::scenes::get_all_test_scenes().size()); }
+
+int ref_validation_scene(int i, char* name, int name_cap, float* out14, int cap) {
+  const auto scenes = thesis::test::scenes::get_all_test_scenes();
+  if (i < 0 || i >= static_cast<int>(scenes.size())) return -1;
+  const auto& sc = scenes[static_cast<size_t>(i)];
+  std::strncpy(name, sc.name.c_str(), static_cast<size_t>(name_cap) - 1);
+  name[name_cap - 1] = '\0';
+  const int n = static_cast<int>(sc.primitives.size());
+  for (int j = 0; j < n && j < cap; ++j) {
+    const Primitive& p = sc.primitives[static_cast<size_t>(j)];
+    const float v[14] = {p.center_.x, p.center_.y, p.center_.z, p.rot_quat_.s_, -p.rot_quat_.u_.x,
+                         -p.rot_quat_.u_.y, -p.rot_quat_.u_.z, p.scale_.x, p.scale_.y, p.scale_.z,
+                         p.albedo_.x, p.albedo_.y, p.albedo_.z, p.optical_thickness_};
+    std::memcpy(out14 + 14 * j, v, sizeof(v));
+  }
+  return n;
 }
 
 // out4: ENABLE_ADAPTIVE_SAMPLING (0/1), ADAPTIVE_MIN_SAMPLES, ADAPTIVE_THRESHOLD,

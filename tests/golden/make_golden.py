@@ -3,8 +3,9 @@
 The reference's host-compilable headers (Primitive constructor and whitening transforms,
 include/thesis/device/params/primitive.h:70-122; point_inside_bvh_bound,
 include/thesis/common/geometry/intersection.h:56-61; host camera build,
-include/thesis/host/params/camera.h:106-216; morton3D, include/thesis/host/utils/math.h:103-131)
-are compiled by oracle/Makefile into oracle/_ref/libref_pin.so; this script calls them on fixed
+include/thesis/host/params/camera.h:106-216; morton3D, include/thesis/host/utils/math.h:103-131;
+the adaptive-sampling constants, device/core/constants.cuh:196-211) and its test runner's scenes
+(test/scenes/geometric_validation.cpp) are compiled by oracle/Makefile into oracle/_ref/libref_pin.so; this script calls them on fixed
 inputs and stores inputs and outputs (float32 bit patterns, so comparisons are exact).  It also
 stores the single-Gaussian closed form of experiments/mitsuba-reference/single_gaussian_analytic.py
 :78-80 (with the renderer's 3-sigma truncation) and the published PCG32 test vector.
@@ -99,6 +100,29 @@ def adaptive_cases(R):
             "min_luminance": bits([k4[3]])[0], "welford": welford, "errors": errors}
 
 
+def scene_rows_digest(rows: np.ndarray) -> str:
+    """sha256 of a scene's (count, 14) float32 rows: centre, forward rotation (w, x, y, z),
+    scale, albedo, optical thickness."""
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(rows, np.float32).tobytes()).hexdigest()
+
+
+def validation_scene_digests(R):
+    """The test runner's geometric validation and stress scenes (test/scenes/
+    geometric_validation.cpp, compiled into the pin library): name, Gaussian count and the digest
+    of each scene's rows."""
+    import ctypes as C
+    R.ref_validation_scene.argtypes = [C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_float), C.c_int]
+    name = C.create_string_buffer(64)
+    scenes = []
+    for i in range(R.ref_validation_scene_count()):
+        n = R.ref_validation_scene(i, name, 64, None, 0)
+        rows = np.zeros((max(n, 1), 14), np.float32)
+        R.ref_validation_scene(i, name, 64, rows.ctypes.data_as(C.POINTER(C.c_float)), n)
+        scenes.append({"name": name.value.decode(), "count": int(n), "sha256": scene_rows_digest(rows[:n])})
+    return scenes
+
+
 def main():
     O.build()
     R = O.ref_lib()
@@ -155,6 +179,7 @@ def main():
     out["pcg32"] = {"seed": 42, "sequence": 54,
                     "outputs": [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]}
     out["adaptive"] = adaptive_cases(R)
+    out["validation_scenes"] = validation_scene_digests(R)
     path = Path(__file__).resolve().parent / "reference_pin.json"
     path.write_text(json.dumps(out, indent=1))
     print(f"wrote {path} ({path.stat().st_size} bytes)")

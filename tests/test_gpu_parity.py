@@ -364,6 +364,14 @@ def test_invalid_inputs_raise(vp_ctx):
     g2 = vp.Gaussians(np.zeros((2, 3)), np.ones((2, 3)), np.tile([1.0, 0, 0, 0], (2, 1)), np.array([1.0, 0.0]))
     with pytest.raises(vp.VpError, match="Gaussian 1: invalid density"):
         vp.Scene(vp_ctx, g2)
+    # an empty scene is valid (the reference's IAS over zero instances): every ray misses
     g3 = vp.Gaussians(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 4)), np.zeros(0))
-    with pytest.raises(vp.VpError, match="no Gaussians"):
-        vp.Scene(vp_ctx, g3)
+    empty = vp.Scene(vp_ctx, g3)
+    info = empty.info()
+    assert info["count"] == 0 and info["wide_nodes"] == 1 and info["leaves"] == 0
+    o = np.zeros((3, 3), np.float32)
+    d = np.tile(np.array([0.0, 0.0, 1.0], np.float32), (3, 1))
+    assert np.all(empty.transmittance(o, d) == 1.0)
+    with pytest.raises(vp.VpError, match="emission model"):
+        empty.set_emission(np.zeros((0, 3), np.float32))
+    empty.close()

@@ -63,3 +63,25 @@ def test_procedural_environment():
     assert np.dot(d, s) > math.cos(math.radians(3.0))
     # ground below the horizon is dim, sky above is brighter
     assert env[100:, :, 0].mean() < 0.1 < env[:50, :, 2].mean()
+
+
+def test_validation_scenes_are_the_reference_runners():
+    """Every geometric validation and stress scene of the reference's test runner
+    (test/scenes/geometric_validation.cpp, compiled from the reference's source into the golden
+    generator's pin library): same names, order and Gaussian counts, and the same float32 centre,
+    rotation, scale, albedo and optical thickness bit for bit (digest of the rows)."""
+    import hashlib
+    import json
+    from pathlib import Path
+
+    from volprim_b200 import validation_scenes as VS
+    golden = json.loads((Path(__file__).resolve().parent / "golden" / "reference_pin.json").read_text())
+    want = golden["validation_scenes"]
+    got = VS.all_scenes()
+    assert [s.name for s in got] == [w["name"] for w in want]
+    assert len(VS.validation_scenes()) == 36 and len(VS.stress_scenes()) == 7
+    for s, w in zip(got, want):
+        g = s.gaussians
+        assert g.count == w["count"], s.name
+        rows = np.concatenate([g.mean, g.quat_wxyz, g.scale, g.albedo, g.density[:, None]], 1).astype(np.float32)
+        assert hashlib.sha256(np.ascontiguousarray(rows).tobytes()).hexdigest() == w["sha256"], s.name
