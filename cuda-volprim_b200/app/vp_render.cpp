@@ -23,6 +23,13 @@
 //                            getDefaultCamera, eye (0,0,-1) looking at the origin, vfov 90)
 //   --ortho-height H         orthographic camera of that viewport height instead
 //   --engine wavefront|warp|megakernel   --precision auto|fast|accurate
+//   --mitsuba-scene INIT_PY ARGS_JSON   the multi-view harness (test/test_runner.cpp
+//                            run_multiview_test with the cameras of a Mitsuba scene description,
+//                            test/scenes/cloud_validation.cpp:52-62): every camera, orthographic,
+//                            at its own resolution, to OUTPUT_DIR/NNNN.exr (NNNN = position among
+//                            the cameras rendered); --camera N keeps camera N only (the
+//                            reference's SG_CAM); --output-dir DIR (default multiview);
+//                            --list-cameras prints the parsed cameras and exits (no GPU needed)
 //   --raygen/--miss/--anyhit/--launch_params/--module_blob NAME   accepted and ignored (they name
 //                            OptiX programs; this library has one compiled path)
 //   --denoise                accepted; the OptiX AI denoiser is not part of this library, so the
@@ -33,9 +40,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <string>
 #include <vector>
 
+#include "mitsuba_scene.h"
 #include "volprim_b200.h"
 
 namespace {
@@ -59,6 +68,9 @@ struct Args {
   float albedo[3] = {-1.f, -1.f, -1.f};
   bool ris = false, measure = false;
   int engine = VP_ENGINE_WAVEFRONT, precision = VP_PRECISION_AUTO;
+  std::string mitsuba_py, mitsuba_json, output_dir = "multiview";
+  int camera_index = -1;
+  bool list_cameras = false;
 };
 
 Args parse(int argc, char** argv) {
@@ -111,6 +123,13 @@ Args parse(int argc, char** argv) {
       for (int k = 0; k < 3; ++k) dst[k] = f32(argv[++i]);
     } else if (o == "--vfov") need(i, 1), a.vfov = f32(argv[++i]);
     else if (o == "--ortho-height") need(i, 1), a.ortho_h = f32(argv[++i]);
+    else if (o == "--mitsuba-scene") {
+      need(i, 2);
+      a.mitsuba_py = argv[++i];
+      a.mitsuba_json = argv[++i];
+    } else if (o == "--output-dir") need(i, 1), a.output_dir = argv[++i];
+    else if (o == "--camera") need(i, 1), a.camera_index = (int)u32(argv[++i]);
+    else if (o == "--list-cameras") a.list_cameras = true;
     else if (o == "--engine") {
       need(i, 1);
       const std::string v = argv[++i];
@@ -135,13 +154,39 @@ Args parse(int argc, char** argv) {
   if (!(a.adaptive >= 0.f)) die("--adaptive-threshold must be non-negative");
   if (!(a.filter >= 0.f)) die("--filter-width must be non-negative");
   if (a.width == 0 || a.height == 0 || a.spp == 0) die("--width, --height and --samples_per_pixel must be positive");
+  if ((a.list_cameras || a.camera_index >= 0) && a.mitsuba_py.empty())
+    die("--list-cameras and --camera need --mitsuba-scene");
   return a;
+}
+
+// The cameras the multi-view harness renders: all, or the one --camera names.
+std::vector<vpapp::MitsubaCamera> harness_cameras(const Args& a) {
+  vpapp::MitsubaScene ms;
+  std::string err;
+  if (!vpapp::parse_mitsuba_scene(a.mitsuba_py, a.mitsuba_json, ms, err)) die(err);
+  if (a.camera_index < 0) return ms.cameras;
+  if (a.camera_index >= (int)ms.cameras.size())
+    die("--camera " + std::to_string(a.camera_index) + " out of range (" + std::to_string(ms.cameras.size()) +
+        " cameras)");
+  return {ms.cameras[(size_t)a.camera_index]};
 }
 
 }  // namespace
 
 int main(int argc, char** argv) {
   const Args a = parse(argc, argv);
+  std::vector<vpapp::MitsubaCamera> views;
+  if (!a.mitsuba_py.empty()) views = harness_cameras(a);
+  if (a.list_cameras) {
+    for (size_t i = 0; i < views.size(); ++i) {
+      const auto& c = views[i];
+      const vp_camera cam = vpapp::mitsuba_orthographic_camera(c);
+      std::printf("%zu %s %ux%u origin %.9g %.9g %.9g target %.9g %.9g %.9g up %.9g %.9g %.9g ortho_height %.9g\n",
+                  i, c.name.c_str(), c.width, c.height, c.origin[0], c.origin[1], c.origin[2], c.target[0],
+                  c.target[1], c.target[2], c.up[0], c.up[1], c.up[2], cam.ortho_height);
+    }
+    return 0;
+  }
   vp_context* ctx = nullptr;
   ok(vp_context_create(0, &ctx), "vp_context_create");
 
@@ -187,6 +232,29 @@ int main(int argc, char** argv) {
   p.engine = a.engine, p.precision = a.precision;
   p.measure = a.measure ? VP_MEASURE_COUNTERS : 0;
   p.adaptive_threshold = a.adaptive, p.adaptive_min_samples = a.adaptive_min;
+
+  if (!views.empty()) {  // the multi-view harness: one render per camera, the scene built once
+    std::error_code ec;
+    std::filesystem::create_directories(a.output_dir, ec);
+    if (ec) die("cannot create " + a.output_dir + ": " + ec.message());
+    for (size_t i = 0; i < views.size(); ++i) {
+      const vp_camera vc = vpapp::mitsuba_orthographic_camera(views[i]);
+      p.width = views[i].width, p.height = views[i].height;
+      std::vector<float> img(4ull * p.width * p.height);
+      vp_render_stats vs{};
+      ok(vp_render(scene, env, &vc, &p, img.data(), VP_MEMORY_HOST, &vs), "vp_render");
+      char name[32];
+      std::snprintf(name, sizeof(name), "%04zu.exr", i);
+      const std::string path = (std::filesystem::path(a.output_dir) / name).string();
+      ok(vp_exr_save(path.c_str(), img.data(), p.width, p.height, 1), "vp_exr_save");
+      std::printf("camera %zu (%s) %ux%u x %u spp (%.3f ms on the device) -> %s\n", i, views[i].name.c_str(), p.width,
+                  p.height, p.spp, vs.ms_kernels, path.c_str());
+    }
+    vp_env_destroy(env);
+    vp_scene_destroy(scene);
+    vp_context_destroy(ctx);
+    return 0;
+  }
 
   std::vector<float> rgba(4ull * a.width * a.height);
   vp_render_stats st{};

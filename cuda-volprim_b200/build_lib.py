@@ -85,7 +85,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
 def build_app(force: bool = False) -> Path:
     """Compiles the vp_render command-line program (app/vp_render.cpp) against the C ABI only;
     it finds libvolprim_b200.so beside itself through an $ORIGIN run path."""
-    if force or _stale(APP_BIN, [APP, INCLUDE / "volprim_b200.h", LIB]):
+    if force or _stale(APP_BIN, [APP, APP.parent / "mitsuba_scene.h", INCLUDE / "volprim_b200.h", LIB]):
         cxx = shutil.which("g++") or shutil.which("c++")
         if cxx is None:
             raise RuntimeError("a C++ compiler (g++) is required to build vp_render")

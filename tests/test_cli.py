@@ -132,3 +132,116 @@ def test_cli_orthographic_and_engines(exe, vp_ctx, tmp_path):
     cam = vp.Camera.orthographic_camera((0, 0, -1), (0, 0, 0), (0, 1, 0), 1.5)
     want = vp.Renderer(cfg, vp.Scene(vp_ctx, g), camera=cam, ctx=vp_ctx).render()
     assert np.all(near(imgs["wavefront"], want[..., :3]))
+
+
+# A Mitsuba scene description in the form the reference's parser reads
+# (src/thesis/host/utils/mitsuba_parser.cpp:39-149): camera blocks of a Python dict with an
+# optional resolution and a T().look_at(...) call that may span lines.
+MITSUBA_INIT = """\
+OBJECTS = {'cloud': {'type': 'ply', 'extent': 2.5}}
+SENSORS = {
+    'cam_0000': {
+        'type': 'orthographic',
+        'width': 40,
+        'height': 30,
+        'to_world': T().look_at(origin=[0.0, 0.0, -4.0], target=[0.0, 0.0, 0.0],
+                                up=[0.0, 1.0, 0.0]),
+    },
+    'cam_0001': {
+        'type': 'orthographic',
+        'to_world': T().look_at(
+            origin=[3.5, 1.25e+0, -2.0],
+            target=[0.1, -0.2, 0.3],
+            up=[0.0, 1.0, 0.0]),
+    },
+    'cam_0002': {
+        'to_world': T().look_at(origin=[1.0, 2.0, 3.0], target=[0.0, 0.0, 0.0]),
+    },
+    'cam_0003': {
+        'height': 16,
+        'to_world': T().look_at(origin=[-2.0, 0.5, 2.0], target=[0.0, 0.0, 0.0], up=[0, 1, 0]),
+    },
+}
+"""
+
+
+def mitsuba_files(tmp_path, init=MITSUBA_INIT, args='{"cam_res": 24, "spp": 64}'):
+    py, js = tmp_path / "__init__.py", tmp_path / "args.json"
+    py.write_text(init)
+    js.write_text(args)
+    return py, js
+
+
+def listed(stdout):
+    rows = []
+    for ln in stdout.splitlines():
+        t = ln.split()
+        f32 = lambda v: tuple(np.float32(x) for x in v)  # %.9g round-trips a float32
+        rows.append({"index": int(t[0]), "name": t[1], "res": tuple(map(int, t[2].split("x"))),
+                     "origin": f32(t[4:7]), "target": f32(t[8:11]), "up": f32(t[12:15]),
+                     "ortho_height": np.float32(t[16])})
+    return rows
+
+
+def test_cli_mitsuba_cameras_parsed(exe, tmp_path):
+    """Camera blocks, per-camera resolutions over the args.json default, look-at blocks over
+    several lines, a block without `up` dropped (as the reference drops it), and the orthographic
+    viewport height 2 / aspect of createOrthographicCamera (mitsuba_parser.cpp:213-225)."""
+    py, js = mitsuba_files(tmp_path)
+    r = run(exe, "--mitsuba-scene", py, js, "--list-cameras")
+    assert r.returncode == 0, r.stderr
+    rows = listed(r.stdout)
+    assert [c["name"] for c in rows] == ["cam_0000", "cam_0001", "cam_0003"]
+    assert [c["res"] for c in rows] == [(40, 30), (24, 24), (24, 16)]
+    assert rows[0]["origin"] == (0.0, 0.0, -4.0) and rows[0]["up"] == (0.0, 1.0, 0.0)
+    assert rows[1]["origin"] == (3.5, 1.25, -2.0)
+    assert rows[1]["target"] == tuple(np.float32(x) for x in ("0.1", "-0.2", "0.3"))
+    for c in rows:
+        w, h = c["res"]
+        assert c["ortho_height"] == np.float32(2.0) / (np.float32(w) / np.float32(h))
+    r = run(exe, "--mitsuba-scene", py, js, "--list-cameras", "--camera", 1)
+    assert r.returncode == 0 and [c["name"] for c in listed(r.stdout)] == ["cam_0001"]
+    _, js2 = mitsuba_files(tmp_path, args="{}")  # no cam_res: 800 x 800
+    r = run(exe, "--mitsuba-scene", py, js2, "--list-cameras")
+    assert [c["res"] for c in listed(r.stdout)] == [(40, 30), (800, 800), (800, 16)]
+
+
+@pytest.mark.parametrize("case, message", [
+    ("no_args_json", "failed to open args.json"),
+    ("no_cameras", "no cameras found"),
+    ("camera_out_of_range", "--camera 9 out of range (3 cameras)"),
+    ("list_without_scene", "--list-cameras and --camera need --mitsuba-scene"),
+])
+def test_cli_mitsuba_errors(exe, tmp_path, case, message):
+    py, js = mitsuba_files(tmp_path, init="SENSORS = {}\n" if case == "no_cameras" else MITSUBA_INIT)
+    args = {"no_args_json": ["--mitsuba-scene", py, tmp_path / "missing.json", "--list-cameras"],
+            "no_cameras": ["--mitsuba-scene", py, js, "--list-cameras"],
+            "camera_out_of_range": ["--mitsuba-scene", py, js, "--list-cameras", "--camera", 9],
+            "list_without_scene": ["--list-cameras"]}[case]
+    r = run(exe, *args)
+    assert r.returncode == 1
+    assert message in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_mitsuba_multiview(exe, vp_ctx, tmp_path):
+    """The harness renders each camera at its resolution to OUTPUT_DIR/NNNN.exr; each image is the
+    API's render through the same orthographic camera."""
+    py, js = mitsuba_files(tmp_path)
+    out = tmp_path / "views"
+    r = run(exe, "--mitsuba-scene", py, js, "--output-dir", out, "--samples_per_pixel", 4, "--seed", 3)
+    assert r.returncode == 0, r.stderr
+    g = vp.Gaussians(mean=np.zeros((1, 3), np.float32), scale=np.full((1, 3), 0.5, np.float32),
+                     quat_wxyz=np.array([[1, 0, 0, 0]], np.float32), density=np.array([0.5], np.float32),
+                     albedo=np.array([[0.5, 0.0, 0.5]], np.float32))
+    scene = vp.Scene(vp_ctx, g)
+    for i, c in enumerate(listed(run(exe, "--mitsuba-scene", py, js, "--list-cameras").stdout)):
+        w, h = c["res"]
+        cam = vp.Camera.orthographic_camera(c["origin"], c["target"], c["up"], c["ortho_height"])
+        cfg = vp.Config(num_samples_per_pixel=4, image_width=w, image_height=h, seed=3)
+        want = vp.Renderer(cfg, scene, camera=cam, ctx=vp_ctx).render()[..., :3]
+        got = flipped_exr(out / f"{i:04d}.exr")
+        assert got.shape == (h, w, 3)
+        assert np.all(near(got, want)), i
+        assert want.max() > 0.05
+    assert sorted(p.name for p in out.iterdir()) == ["0000.exr", "0001.exr", "0002.exr"]
