@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-baseline-engine", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the differentiation and serving forms")
     ap.add_argument("--serving-requests", type=int, default=128)
+    ap.add_argument("--rmse-sweep", action="store_true",
+                    help="instead of the timed run: RMSE against a high-spp render versus device time, for the "
+                         "wavefront and the plain megakernel, and the speed-up at matched RMSE")
+    ap.add_argument("--ref-spp", type=int, default=1024, help="samples of the --rmse-sweep reference render")
     return ap.parse_args()
 
 
@@ -599,9 +603,76 @@ def serving_form(device, n_requests):
                         "80% of the offline throughput; 150 GB budget"}
 
 
+def rmse_sweep(args):
+    """Equal-RMSE comparison by measurement: each engine renders the showcase progressively in
+    16-spp batches; after each batch its RMSE against an independent high-spp render (other seed,
+    wavefront) and its cumulative device time are recorded.  At every RMSE level the wavefront
+    reaches, the megakernel's time is interpolated on log(time) vs log(RMSE); the speed-up at
+    matched RMSE is their ratio.  The reference's own noise adds the same variance to both curves."""
+    import numpy as np
+    import volprim_b200 as vp
+
+    w = workload(args)
+    cfg = w.config
+    cfg.batch_spp = BATCH_SPP
+    W, H = cfg.image_width, cfg.image_height
+    ctx = vp.Context(0)
+    scene = vp.Scene(ctx, w.gaussians, w.sigma_multiplier)
+    env = vp.Environment(ctx, rgb=w.env)
+    ref_cfg = vp.Config(**{**cfg.__dict__, "seed": cfg.seed + 1000, "num_samples_per_pixel": args.ref_spp,
+                           "engine": "wavefront"})
+    ref_img = vp.ProgressiveImage(ctx, W, H)
+    for off in range(0, args.ref_spp, 64):
+        ref_img.accumulate(scene, env, w.camera, ref_cfg, off, min(64, args.ref_spp - off))
+    ref = ref_img.read()[..., :3].astype(np.float64)
+    ref_img.close()
+
+    def curve(engine, sc):
+        c = vp.Config(**{**cfg.__dict__, "engine": engine})
+        im = vp.ProgressiveImage(ctx, W, H)
+        im.accumulate(sc, env, w.camera, c, 0, BATCH_SPP)  # warm-up batch, then start again
+        im.clear()
+        pts, t = [], 0.0
+        for off in range(0, args.spp, BATCH_SPP):
+            t += im.accumulate(sc, env, w.camera, c, off, BATCH_SPP)["ms_kernels"]
+            rmse = float(np.sqrt(np.mean((im.read()[..., :3] - ref) ** 2)))
+            pts.append({"spp": off + BATCH_SPP, "ms": t, "rmse": rmse})
+        im.close()
+        return pts
+
+    wave = curve("wavefront", scene)
+    lbvh = vp.Scene(ctx, w.gaussians, w.sigma_multiplier, binary_builder="lbvh")
+    mega = curve("megakernel", lbvh)
+    lbvh.close()
+    lr_m = np.log([p["rmse"] for p in mega])
+    lt_m = np.log([p["ms"] for p in mega])
+    order = np.argsort(lr_m)
+    matched = []
+    for p in wave:
+        lr = math.log(p["rmse"])
+        if lr_m.min() <= lr <= lr_m.max():
+            t_m = float(np.exp(np.interp(lr, lr_m[order], lt_m[order])))
+            matched.append({"rmse": p["rmse"], "wavefront_ms": p["ms"], "megakernel_ms": t_m,
+                            "speedup": t_m / p["ms"]})
+    scale = float(np.sqrt(np.mean(ref ** 2)))
+    ratio = [m["rmse"] / p["rmse"] for p, m in zip(wave, mega)]  # same estimator and random numbers
+    line = {"metric": "speed-up at matched RMSE (wavefront vs plain per-pixel megakernel over the Karras LBVH)",
+            "value": statistics.median([m["speedup"] for m in matched]) if matched else None, "unit": "x",
+            "higher_is_better": True,
+            "config": {"workload": f"showcase_{args.n // 1000}k", "width": W, "height": H, "spp": args.spp,
+                       "reference": f"wavefront, {args.ref_spp} spp, seed {ref_cfg.seed}", "rms_of_reference": scale},
+            "rmse_ratio_megakernel_over_wavefront_at_equal_spp": {"min": min(ratio), "max": max(ratio)},
+            "time_ratio_at_equal_spp": mega[-1]["ms"] / wave[-1]["ms"],
+            "wavefront": wave, "megakernel": mega, "matched": matched}
+    print(json.dumps(line), flush=True)
+    scene.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.rmse_sweep:
+        rmse_sweep(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
