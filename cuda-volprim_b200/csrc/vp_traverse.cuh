@@ -326,14 +326,27 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           status |= kStatusStackOverflow;
           break;
         }
-        int rank = 0;  // farther children sit deeper in the stack; rank nh-1 is the nearest
-        for (unsigned mm = m; mm; mm &= mm - 1u) {
-          const int j = __ffs(mm) - 1;
-          const float tj = __shfl_sync(kFull, tnear, j);
-          rank += (tj > tnear || (tj == tnear && j < lane)) ? 1 : 0;
+        // The traversal continues into the nearest child.  The argmin stacks the others by
+        // distance (farther deeper; rank nh-1 is the nearest), so its culling at the best t*
+        // pops the near ones first.  Transmittance sums every chord whatever the order: it picks
+        // the nearest child by a warp min and stacks the others in lane order, which costs a
+        // fixed few instructions instead of a pass over the hit children.
+        int rank = 0;
+        int src;
+        if constexpr (kKind == kTau) {
+          const unsigned key = hit ? __float_as_uint(tnear) : 0xFFFFFFFFu;  // tnear >= 0: bit order
+          const unsigned mn = __reduce_min_sync(kFull, key);
+          src = __ffs(__ballot_sync(kFull, hit && key == mn)) - 1;
+          rank = __popc(m & lt_mask & ~(1u << src));
+        } else {
+          for (unsigned mm = m; mm; mm &= mm - 1u) {
+            const int j = __ffs(mm) - 1;
+            const float tj = __shfl_sync(kFull, tnear, j);
+            rank += (tj > tnear || (tj == tnear && j < lane)) ? 1 : 0;
+          }
+          src = __ffs(__ballot_sync(kFull, hit && rank == nh - 1)) - 1;
         }
-        const bool nearest = hit && rank == nh - 1;
-        const int src = __ffs(__ballot_sync(kFull, nearest)) - 1;
+        const bool nearest = lane == src;
         if (hit && !nearest) {
           W.st_ref[sp + rank] = cref;
           W.st_t[sp + rank] = tnear;
