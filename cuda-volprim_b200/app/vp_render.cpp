@@ -35,7 +35,7 @@
 //   --denoise                accepted; the OptiX AI denoiser is not part of this library, so the
 //                            image is written undenoised with a warning
 // Exit status 0 on success; on failure the library's message and status 1 (the reference exits
-// through try_unwrap_or_exit, src/thesis/host/utils/result.h:89-97).
+// through try_unwrap_or_exit, include/thesis/host/utils/result.h:89-97).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>

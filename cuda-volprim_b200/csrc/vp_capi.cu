@@ -354,7 +354,7 @@ vp_status vp_env_destroy(vp_env* e) {
 vp_status vp_render_params_default(vp_render_params* p) {
   if (!p) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
   std::memset(p, 0, sizeof(*p));
-  p->width = 1000;  // Config defaults (config.h:119-136)
+  p->width = 1000;  // Config defaults (config.h:30-47)
   p->height = 750;
   p->spp = 1;
   p->seed = 42;

@@ -129,7 +129,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
                       vp_scene* s);
 vp_status build_env(vp_context* ctx, const float* rgb, uint32_t w, uint32_t h, uint32_t channels,
                     int32_t memory, vp_env* env);
-// Host restatement of host::params::Camera::build (camera.h:106-177).
+// Host restatement of host::params::Camera::build (camera.h:32-111).
 void build_camera(const vp_camera& cam, uint32_t width, uint32_t height, CameraView& out);
 ParamsView make_params(const vp_render_params& p, const vp_scene* s);
 vp_status check_params(const vp_render_params* p);

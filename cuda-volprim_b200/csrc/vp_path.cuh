@@ -1,11 +1,11 @@
 // One path vertex of the integrator (device/entry/raygen.cuh:115-208 with
-// device/entry/path_stages.cuh:25-472), split from the queries so the persistent warp engine
+// device/entry/path_stages.cuh:25-226), split from the queries so the persistent warp engine
 // and the wavefront engine run the same shading code: given the outcome of the free-flight
 // argmin of this bounce (scatter distance and the albedo there), draw the phase sample, build
 // the transmittance queries of the bounce (the bounce-0 analytic direct term and the NEE shadow
 // rays) with their radiance weights, apply the escape rule, throughput update and Russian
 // roulette.  Random numbers are drawn in the reference's order: [free-flight key] -> phase
-// sample (sampling.cuh:537) -> NEE (path_stages.cuh:394-472) -> roulette (:25-37).
+// sample (sampling.cuh:537) -> NEE (path_stages.cuh:148-226) -> roulette (:25-37).
 #pragma once
 
 #include "vp_device.cuh"
@@ -66,13 +66,13 @@ __device__ __forceinline__ bool shade_bounce(const EnvView& E, const ParamsView&
     sh.seed[0] = kNoGauss;
     sh.n = 1;
   }
-  if (!scattered) {  // accumulate_escape_radiance (path_stages.cuh:368-386)
+  if (!scattered) {  // accumulate_escape_radiance (path_stages.cuh:122-146)
     if (P.nee_mode == VP_NEE_NONE && s.bounce > 0) s.rad = add(s.rad, mul(s.thr, env_lookup(E, s.d)));
     return false;
   }
   const float3 base = mul(s.thr, albedo);
   if (P.nee_mode != VP_NEE_NONE && (base.x != 0.f || base.y != 0.f || base.z != 0.f)) {
-    // accumulate_nee_direct (path_stages.cuh:394-472); a zero `base` adds nothing and the path
+    // accumulate_nee_direct (path_stages.cuh:148-226); a zero `base` adds nothing and the path
     // ends below, so its draws are skipped.
     if (P.nee_mode == VP_NEE_MIS) {
       float pdf_a;

@@ -6,7 +6,7 @@ Reference interface (kfernandez31/cuda-volprim):
                                      include/thesis/host/app/renderer.h:77-81,
                                      src/thesis/host/app/renderer.cpp:34-439
   host::params::Camera::createPerspective / createOrthographic / getDefaultCamera
-                                     include/thesis/host/params/camera.h:182-216
+                                     include/thesis/host/params/camera.h:114-150
   io::loadPrimitives (PLY semantics: log-scales, (w,x,y,z) quaternions, mass x sigma-multiplier)
                                      src/thesis/host/utils/io/ply.cpp:21-175
 Differences: the image is returned in memory (H x W x 4 float32, alpha = 1) instead of written
@@ -194,6 +194,7 @@ class Scene:
             d = dirs.detach().to(torch.float32).contiguous()
             n = o.numel() // 3
             out = torch.empty(n, dtype=torch.float32, device=o.device)
+            _sync_torch(o, d, out)
             check(lib.vp_transmittance(self.handle, o.data_ptr(), d.data_ptr(), n, precision, engine,
                                        out.data_ptr(), _capi.VP_MEMORY_DEVICE))
             return out
@@ -214,6 +215,7 @@ class Scene:
             d = dirs.detach().to(torch.float32).contiguous()
             n = o.numel() // 3
             out = torch.empty(n, dtype=torch.float32, device=o.device)
+            _sync_torch(o, d, out)
             check(lib.vp_transmittance_static(self.handle, o.data_ptr(), d.data_ptr(), n, precision, out.data_ptr(),
                                               _capi.VP_MEMORY_DEVICE))
             return out
@@ -277,6 +279,7 @@ class Environment:
                 import torch
                 t = rgb.detach().to(torch.float32).contiguous()
                 hgt, wid, ch = t.shape
+                _sync_torch(t)
                 check(lib.vp_env_create(ctx.handle, t.data_ptr(), wid, hgt, ch, _capi.VP_MEMORY_DEVICE,
                                         C.byref(h)))
             else:
@@ -307,7 +310,7 @@ class Environment:
 
 @dataclass
 class Camera:
-    """host::params::Camera (camera.h:84-228)."""
+    """host::params::Camera (include/thesis/host/params/camera.h:18-166)."""
 
     eye: tuple = (0.0, 0.0, -1.0)
     lookat: tuple = (0.0, 0.0, 0.0)
@@ -325,7 +328,7 @@ class Camera:
         return Camera(tuple(origin), tuple(target), tuple(up), 90.0, float(ortho_height), True)
 
     @staticmethod
-    def default() -> "Camera":  # getDefaultCamera (camera.h:183-188)
+    def default() -> "Camera":  # getDefaultCamera (include/thesis/host/params/camera.h:117-121)
         return Camera()
 
     def to_c(self) -> _capi.vp_camera:
@@ -414,6 +417,7 @@ class Renderer:
         cam = self.camera.to_c()
         st = _capi.vp_render_stats()
         if out is not None and _is_cuda_tensor(out):
+            _sync_torch(out)
             check(lib.vp_render(self.scene.handle, self.env.handle, C.byref(cam), C.byref(p), out.data_ptr(),
                                 _capi.VP_MEMORY_DEVICE, C.byref(st)))
             self.last_stats = st.as_dict()

@@ -48,8 +48,8 @@ enum {
 typedef enum vp_memory { VP_MEMORY_HOST = 0, VP_MEMORY_DEVICE = 1 } vp_memory;
 
 /* Next-event estimator at a scatter vertex.  Replaces the compile-time ENABLE_NEE / ENABLE_MIS
- * switches and the runtime --ris flag (device/core/constants.cuh:419,429; launch_params.h:43;
- * device/entry/path_stages.cuh:394-472). */
+ * switches and the runtime --ris flag (device/core/constants.cuh:156-177; launch_params.h:43;
+ * device/entry/path_stages.cuh:148-226). */
 typedef enum vp_nee_mode {
   VP_NEE_MIS = 0,   /* balance-heuristic MIS of phase-IS and env-IS, 2 shadow rays (default) */
   VP_NEE_PHASE = 1, /* phase importance sampling only, 1 shadow ray */
@@ -213,7 +213,7 @@ vp_status vp_env_destroy(vp_env* env);
 /* ---------------------------------------------------------------------------------------- */
 
 /* Mirrors host::params::Camera::createPerspective / createOrthographic
- * (include/thesis/host/params/camera.h:106-216). */
+ * (include/thesis/host/params/camera.h:32-150). */
 typedef struct vp_camera {
   float eye[3];
   float lookat[3];
@@ -254,7 +254,7 @@ typedef struct vp_render_params {
   uint32_t adaptive_min_samples;   /* default 32 */
 } vp_render_params;
 
-/* Fills the reference's defaults (config.h:119-136, launch_params.h:38-58). */
+/* Fills the reference's defaults (config.h:30-47, launch_params.h:38-58). */
 vp_status vp_render_params_default(vp_render_params* out);
 
 typedef struct vp_render_stats {
@@ -339,8 +339,10 @@ vp_status vp_transmittance(vp_scene* scene, const float* origins, const float* d
  * staged host rays and results, the work-queue head and the status word -- is one file-scope
  * static __device__ array sized for at most 65536 rays (about 1.8 MB), which every GPU that loads
  * the library holds until the process exits.  n > 65536 returns VP_ERROR_LIMIT.  The first call
- * on a device looks up the array's address on that device; make it before any stream capture.
- * All calls share the array and leave their data in it (the queue head and status word are
+ * on a device looks up the array's address on that device and keeps it for the life of the
+ * process; make that first call before any stream capture, and reset no device
+ * (cudaDeviceReset) while the library is in use.  Each call synchronises the context's stream
+ * before it returns.  All calls share the array and leave their data in it (the queue head and status word are
  * cleared at the start of each call): calls whose work overlaps on the GPU race and must be
  * serialised by the caller.  No counterpart in the reference. */
 vp_status vp_transmittance_static(vp_scene* scene, const float* origins, const float* dirs,

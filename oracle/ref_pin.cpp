@@ -3,7 +3,7 @@
 // It exposes the reference's Primitive constructor and whitening transforms
 // (include/thesis/device/params/primitive.h:70-122), the 3-sigma containment test
 // (include/thesis/common/geometry/intersection.h:56-61), the host camera build
-// (include/thesis/host/params/camera.h:106-216) and the Morton code
+// (include/thesis/host/params/camera.h:32-150) and the Morton code
 // (include/thesis/host/utils/math.h:103-131), so the oracle's restatement of them can be checked
 // against the reference's code itself.  It also returns the test runner's geometric validation
 // scenes (test/scenes/geometric_validation.cpp, compiled in), exposes the adaptive-sampling constants

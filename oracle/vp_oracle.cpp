@@ -15,9 +15,9 @@
 //       point_inside_bvh_bound / exit_from_inside / compute_exit_from_entry
 //         (include/thesis/common/geometry/intersection.h:56-173),
 //       sampling stages, phase, env_is, transmittance (device/core/sampling.cuh:74-583),
-//       russian_roulette / finalize_sample / escape / NEE (device/entry/path_stages.cuh:25-472),
+//       russian_roulette / finalize_sample / escape / NEE (device/entry/path_stages.cuh:25-226),
 //       the raygen loop (device/entry/raygen.cuh:72-230), PCG32 (device/core/random.cuh:16-72),
-//       camera (include/thesis/device/params/camera.h:33-57, host/params/camera.h:106-177),
+//       camera (include/thesis/device/params/camera.h:33-57, host/params/camera.h:32-111),
 //       env CDF build + lookup (include/thesis/host/params/environment_map.h:45-101,
 //         device/params/environment_map.h:36-61).
 //     OptiX traversal order is replaced by ascending entry distance (the reference's order is

@@ -3,7 +3,7 @@
 The reference's host-compilable headers (Primitive constructor and whitening transforms,
 include/thesis/device/params/primitive.h:70-122; point_inside_bvh_bound,
 include/thesis/common/geometry/intersection.h:56-61; host camera build,
-include/thesis/host/params/camera.h:106-216; morton3D, include/thesis/host/utils/math.h:103-131;
+include/thesis/host/params/camera.h:32-150; morton3D, include/thesis/host/utils/math.h:103-131;
 the adaptive-sampling constants, device/core/constants.cuh:196-211) and its test runner's scenes
 (test/scenes/geometric_validation.cpp) are compiled by oracle/Makefile into oracle/_ref/libref_pin.so; this script calls them on fixed
 inputs and stores inputs and outputs (float32 bit patterns, so comparisons are exact).  It also

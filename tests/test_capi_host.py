@@ -49,7 +49,7 @@ def test_version_and_defaults():
     assert (mj.value, mn.value) == (0, 1)
     p = _capi.vp_render_params()
     _capi.check(_capi.lib.vp_render_params_default(C.byref(p)))
-    # app::Config defaults (include/thesis/host/app/config.h:119-136), BATCH_SIZE (renderer.cpp:32)
+    # app::Config defaults (include/thesis/host/app/config.h:30-47), BATCH_SIZE (renderer.cpp:32)
     assert (p.width, p.height, p.spp, p.seed, p.max_bounces, p.rr_depth) == (1000, 750, 1, 42, 128, 12)
     assert abs(p.rr_max_survival - 0.99) < 1e-7 and abs(p.hg_g - 0.85) < 1e-7
     assert p.firefly_clamp == 0.0 and p.pixel_filter_stddev == 0.0

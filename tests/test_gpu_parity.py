@@ -82,6 +82,22 @@ def test_fast_transmittance_vs_fp64(scene256):
     assert np.all(np.abs(T - T64) <= 2e-4 * T64 + 1e-8)
 
 
+def test_transmittance_waits_for_torch_stream(scene256):
+    """float64, non-contiguous CUDA inputs: their float32 copies are made by kernels on torch's
+    stream, queued behind a busy-wait, so the query must wait for that stream before it reads."""
+    import torch
+    sc, _, _ = scene256
+    o, d = random_rays(np.random.default_rng(9), 8000)
+    ref = sc.transmittance(o, d, precision=VP_PRECISION_FAST).astype(np.float64)
+    o64 = torch.from_numpy(np.repeat(o.astype(np.float64), 2, axis=1)).cuda()[:, ::2]
+    d64 = torch.from_numpy(np.repeat(d.astype(np.float64), 2, axis=1)).cuda()[:, ::2]
+    assert not o64.is_contiguous()
+    for engine in (VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL):
+        torch.cuda._sleep(20_000_000)
+        got = sc.transmittance(o64, d64, precision=VP_PRECISION_FAST, engine=engine).cpu().numpy()
+        assert np.all(np.abs(got.astype(np.float64) - ref) <= 2e-5 * ref + 1e-9)
+
+
 def test_single_gaussian_closed_form(vp_ctx):
     """single_gaussian_validation: unit isotropic Gaussian of mass M, rays along +z at
     perpendicular distance d -> tau(d) = M/(2 pi) exp(-d^2/2) erf(sqrt((9 - d^2)/2))

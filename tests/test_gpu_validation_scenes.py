@@ -1,5 +1,5 @@
 """GPU: the reference test runner's geometric validation scenes (test/scenes/
-geometric_validation.cpp; volprim_b200.validation_scenes) as regression fixtures, every one
+geometric_validation.cpp; tests/validation_scenes.py) as regression fixtures, every one
 through every engine.
 
 Per scene:
@@ -21,7 +21,8 @@ import pytest
 
 import oracle as O
 import volprim_b200 as vp
-from volprim_b200 import scenes, validation_scenes as VS
+from volprim_b200 import scenes
+import validation_scenes as VS
 from volprim_b200._capi import VP_ENGINE_MEGAKERNEL, VP_ENGINE_WARP, VP_PRECISION_ACCURATE
 
 pytestmark = pytest.mark.gpu

@@ -74,7 +74,7 @@ def test_validation_scenes_are_the_reference_runners():
     import json
     from pathlib import Path
 
-    from volprim_b200 import validation_scenes as VS
+    import validation_scenes as VS
     golden = json.loads((Path(__file__).resolve().parent / "golden" / "reference_pin.json").read_text())
     want = golden["validation_scenes"]
     got = VS.all_scenes()

@@ -67,3 +67,18 @@ def test_static_rejects_more_rays_than_its_scratch(scene):
     o, d = _rays(4, 65537)
     with pytest.raises(vp.VpError, match="at most 65536 rays"):
         scene.transmittance_static(o, d)
+
+
+def test_static_waits_for_torch_stream(scene):
+    """float64, non-contiguous CUDA inputs: their float32 copies are made by kernels on torch's
+    stream, queued behind a busy-wait, so the query must wait for that stream before it reads."""
+    import torch
+    o, d = _rays(5, 8000)
+    ref = scene.transmittance(o, d, precision=VP_PRECISION_FAST, engine=VP_ENGINE_WARP).astype(np.float64)
+    o64 = torch.from_numpy(np.repeat(o.astype(np.float64), 2, axis=1)).cuda()[:, ::2]
+    d64 = torch.from_numpy(np.repeat(d.astype(np.float64), 2, axis=1)).cuda()[:, ::2]
+    assert not o64.is_contiguous()
+    for _ in range(2):
+        torch.cuda._sleep(20_000_000)
+        got = scene.transmittance_static(o64, d64, precision=VP_PRECISION_FAST).cpu().numpy().astype(np.float64)
+        assert np.all(np.abs(got - ref) <= 2e-5 * ref + 1e-9)

@@ -21,7 +21,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .api import Camera, Gaussians
+from volprim_b200.api import Camera, Gaussians
 
 _ROOT_TWO_PI = np.float32(2.5066282746)  # math::ROOT_TWO_PI_F
 _TWO_PI = np.float32(2.0) * np.float32(np.pi)  # math::TWO_PI_F (float32 product)
