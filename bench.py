@@ -126,10 +126,15 @@ def measured_peaks():
 
 
 class CpuBaseline:
-    """The reference's path restated on the host (oracle port, reference RNG order) on a bounded
-    sample of the workload: image rows spread evenly over the image, 2 spp, all host threads."""
+    """The reference's path restated on the host (oracle port, reference RNG order, CPU BVH) on a
+    bounded sample of the workload: pixels drawn from a seeded random permutation of the whole
+    image (so every sample covers sky, cloud edge and cloud core in proportion), 2 spp each, all
+    host threads.  Successive samples continue the permutation."""
+
+    SPP = 2
 
     def __init__(self, w):
+        import numpy as np
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
         self.O, self.w = O, w
@@ -140,29 +145,37 @@ class CpuBaseline:
         cfg = w.config
         self.c16 = O.camera16(w.camera, cfg.image_width, cfg.image_height)
         self.threads = O.max_threads()
-        H = cfg.image_height
-        self.stride = max(1, H // 64)
-        self.rows = list(range(self.stride // 2, H, self.stride))
+        self.perm = np.random.default_rng(20240).permutation(cfg.image_width * cfg.image_height)
         self.next = 0
 
     def sample(self, seconds_target=15.0) -> dict:
+        import numpy as np
         cfg = self.w.config
-        spent, paths, nrows = 0.0, 0, 0
-        while spent < seconds_target and nrows < len(self.rows):
-            y = self.rows[self.next % len(self.rows)]
-            self.next += 1
-            _, secs = self.O.render(self.osc, self.env, self.c16, cfg, y0=y, y1=y + 1, s0=0, s1=2,
-                                    rng_mode="sequential", threads=self.threads)
+        W = cfg.image_width
+        chunk = 4 * self.threads
+        spent = trace_s = scan_s = 0.0
+        pixels = 0
+        while spent < seconds_target and pixels < self.perm.size:
+            idx = self.perm[np.arange(self.next, self.next + chunk) % self.perm.size]
+            self.next += chunk
+            _, secs, tr, sc = self.O.render_pixels(self.osc, self.env, self.c16, cfg, idx % W, idx // W, 0, self.SPP,
+                                                   rng_mode="sequential", threads=self.threads)
             spent += secs
-            paths += cfg.image_width * 2
-            nrows += 1
+            trace_s += tr
+            scan_s += sc
+            pixels += idx.size
+        paths = pixels * self.SPP
         return {"value": paths / spent / 1e6, "unit": UNIT, "cores": self.threads, "kind": "port",
-                "sample": f"{nrows} image rows from an even spread (every {self.stride}th of "
-                          f"{cfg.image_height}) x {cfg.image_width} px x 2 spp, reference RNG order, CPU BVH; "
-                          f"{paths} paths in {spent:.1f} s (scene + BVH build {self.build_s:.1f} s untimed)"}
+                "scan_fraction": scan_s / max(trace_s, 1e-12),
+                "sample": f"{pixels} pixels of a seeded random permutation of the whole {W}x{cfg.image_height} image "
+                          f"x {self.SPP} spp, reference RNG order, CPU BVH; {paths} paths in {spent:.1f} s on "
+                          f"{self.threads} threads, {100 * scan_s / max(trace_s, 1e-12):.0f}% of the threads' time in "
+                          f"the bounce-0 origin-inside scan over all {self.w.gaussians.count} Gaussians "
+                          f"(build_origin_inside_set, once per camera path); scene + BVH build "
+                          f"{self.build_s:.1f} s untimed"}
 
 
-def cpu_baseline(w, seconds_target=15.0):
+def cpu_baseline(w, seconds_target=20.0):
     return CpuBaseline(w).sample(seconds_target)
 
 
@@ -204,10 +217,47 @@ F_CROSS_FLOPS = 111  # FP32 flops of one closed-form chord evaluation (FMA = 2),
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
-def roofline(args, m, step_stats):
-    """Roofline of the dominant kernel, from the counters of one measured batch (m) and the CUDA-event
-    stage times of the timed steps (the steps are the same batch size over the same image)."""
-    peak, peak_kind = measured_peaks()
+def l2_copy_gbs(device_bytes=32 << 20, reps=50):
+    """Measured L2-resident copy rate: torch copy_ between two 32 MiB buffers (64 MiB, inside the
+    126 MB L2), replayed from a captured CUDA graph so launch gaps do not count; read + write bytes
+    over CUDA-event time, best of 3."""
+    import torch
+    a = torch.empty(device_bytes // 4, dtype=torch.float32, device="cuda").fill_(1.0)
+    b = torch.empty_like(a)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            b.copy_(a)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(reps):
+            b.copy_(a)
+    best = 0.0
+    for _ in range(3):
+        g.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * device_bytes * reps / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del g
+    return best
+
+
+def roofline(args, m, step_stats, sm_mhz=None):
+    """Roofline of the dominant kernel, from the counters of one measured batch (m), the CUDA-event
+    stage times of the timed steps (the steps are the same batch size over the same image) and the
+    per-unit ncu figures of profiles/traffic.json (warp instructions and DRAM bytes per unit).
+
+    The traversal kernels are issue-bound (the scene is L2-resident, DRAM runs below 1% of peak),
+    so the binding roof is the SMs' issue rate: 148 SMs x 4 schedulers x one warp instruction per
+    cycle at the SM clock sampled during the timed region.  The bytes the traversal touches are
+    reported against a measured L2 copy rate (l2_demand) and the DRAM bytes against the measured
+    HBM copy rate (hbm)."""
+    peak_hbm, peak_kind = measured_peaks()
 
     def query_bytes(k):
         node = BINARY_NODE_BYTES if args.engine == "megakernel" else WIDE_NODE_BYTES
@@ -218,54 +268,76 @@ def roofline(args, m, step_stats):
         ms = [sum(st["ms_stage"][k] for st in step_stats) / n for k in range(3)]
         nl = [sum(st["stage_launches"][k] for st in step_stats) / n for k in range(3)]
         kern = [("k_wf_extend", query_bytes(0) + query_bytes(2) + m["bounces"] * EXTEND_STATE_BYTES,
-                 "free-flight argmin + scatter-point albedo", m["bounces"], "path bounces"),
+                 "free-flight argmin + scatter-point albedo", m["bounces"], "path bounces", EXTEND_STATE_BYTES),
                 ("k_wf_shadow", query_bytes(1) + m["shadow_rays"] * SHADOW_STATE_BYTES,
-                 "transmittance (NEE shadow rays)", m["shadow_rays"], "shadow rays")]
+                 "transmittance (NEE shadow rays)", m["shadow_rays"], "shadow rays", SHADOW_STATE_BYTES)]
         k = 0 if ms[0] >= ms[1] else 1
-        name, alg, what, units, unit_name = kern[k]
+        name, alg, what, units, unit_name, state_bytes = kern[k]
         step_ms, launches = ms[k], nl[k]
         share = ms[k] / max(1e-9, sum(st["ms_kernels"] for st in step_stats) / n)
     else:
         name = "k_render_mega" if args.engine == "megakernel" else "k_render_warp"
         alg = query_bytes(0) + query_bytes(1) + query_bytes(2)
-        what, units, unit_name = "whole path loop", m["paths"], "paths"
+        what, units, unit_name, state_bytes = "whole path loop", m["paths"], "paths", None
         step_ms = sum(st["ms_kernels"] for st in step_stats) / n
         launches, share = 1, 1.0
-    achieved = alg / (step_ms / 1e3) / 1e9  # per-launch bytes / per-launch time = per-step ratio
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": peak_kind, "kernel": name, "kernel_work": what,
-            "kernel_share_of_step": share, "launches_per_step": launches,
-            "algorithmic_bytes_per_launch": alg / launches, "kernel_ms_per_launch": step_ms / launches,
-            "units_per_launch": units / launches, "units": unit_name,
-            "note": "achieved = algorithmic bytes of the kernel's launches in one step (3-sigma boxes tested x 32 B + "
-                    "Gaussian records loaded x 64 B + BVH32 inner nodes x 1 KiB + per-item path state) / their "
-                    "CUDA-event time in the timed steps; the 70 MB scene is L2-resident, so most of these bytes "
-                    "are L2 hits (traffic = DRAM bytes from ncu)",
-            "per_step": {"crossings": m["crossings"], "bounces": m["bounces"], "shadow_rays": m["shadow_rays"],
-                         "query_nodes[argmin,tau,albedo]": m["query_nodes"],
-                         "query_leaves[argmin,tau,albedo]": m["query_leaves"],
-                         "query_box_tests[argmin,tau,albedo]": m["query_prim_tests"],
-                         "query_record_loads[argmin,tau,albedo]": m["query_geo_loads"],
-                         "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"]}}
+    sec_per_launch = step_ms / launches / 1e3
+    units_per_launch = units / launches
+    prof = {}
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        try:
+            prof = json.loads(traffic_file.read_text()).get(name) or {}
+        except (ValueError, TypeError):
+            prof = {}
+    clock = sm_mhz or 1965.0
+    issue_peak = 148 * 4 * clock * 1e6 / 1e9  # G warp-instructions / s
+    inst = prof.get("warp_inst_per_unit")
+    traffic = prof["dram_bytes_per_unit"] * units_per_launch if prof.get("dram_bytes_per_unit") else None
+    l2_peak = l2_copy_gbs()
+    l2_achieved = alg / launches / sec_per_launch / 1e9
+    roof = {"kernel": name, "kernel_work": what, "kernel_share_of_step": share, "launches_per_step": launches,
+            "kernel_ms_per_launch": step_ms / launches, "units_per_launch": units_per_launch, "units": unit_name}
+    if inst:
+        achieved = inst * units_per_launch / sec_per_launch / 1e9
+        roof.update({"bound": "issue", "achieved": achieved, "peak": issue_peak, "unit": "G warp-instructions/s",
+                     "frac": achieved / issue_peak,
+                     "peak_source": f"148 SMs x 4 schedulers x 1 warp-instruction/cycle x {clock:.0f} MHz "
+                                    f"({'median SM clock sampled in the timed region' if sm_mhz else 'max clock'})",
+                     "warp_instructions_per_unit": inst, "instructions_source": prof.get("source")})
+    else:
+        roof.update({"bound": "issue", "achieved": None, "peak": issue_peak, "unit": "G warp-instructions/s",
+                     "frac": None, "note": "no ncu instruction count per unit in profiles/traffic.json"})
+    roof["traffic"] = traffic
+    roof["traffic_source"] = prof.get("source")
+    roof["traffic_per_unit"] = prof.get("dram_bytes_per_unit")
+    roof["declared_state_bytes_per_unit"] = state_bytes
+    roof["l2_demand"] = {"achieved": l2_achieved, "peak": l2_peak, "unit": "GB/s", "frac": l2_achieved / l2_peak,
+                         "algorithmic_bytes_per_launch": alg / launches,
+                         "peak_source": "measured: L2-resident torch copy, 2 x 32 MiB, read + write bytes",
+                         "note": "3-sigma boxes tested x 32 B + Gaussian records loaded x 64 B + BVH32 inner nodes "
+                                 "x 1 KiB + per-item path state, per launch, over its CUDA-event time; the 70 MB "
+                                 "scene is L2-resident and L1 serves about half of the requests (ncu L1 hit rate "
+                                 "54-60%), so frac can exceed 1"}
+    if traffic is not None:
+        roof["hbm"] = {"achieved": traffic / sec_per_launch / 1e9, "peak": peak_hbm, "unit": "GB/s",
+                       "frac": traffic / sec_per_launch / 1e9 / peak_hbm, "peak_source": peak_kind}
+    roof["per_step"] = {"crossings": m["crossings"], "bounces": m["bounces"], "shadow_rays": m["shadow_rays"],
+                        "query_nodes[argmin,tau,albedo]": m["query_nodes"],
+                        "query_leaves[argmin,tau,albedo]": m["query_leaves"],
+                        "query_box_tests[argmin,tau,albedo]": m["query_prim_tests"],
+                        "query_record_loads[argmin,tau,albedo]": m["query_geo_loads"],
+                        "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"]}
     if args.engine == "wavefront":
         roof["stage_ms_per_step[extend,shadow,other]"] = ms
     # The FP32 side: closed-form (ray, Gaussian) evaluations of the step's traversal kernels times
-    # the declared 111 FP32 flops of one (FMA = 2; erf and MUFU work not counted), against the
+    # the declared 111 FP32 flops each (FMA = 2; erf and MUFU work not counted), against the
     # nominal FP32 rate (148 SMs x 128 lanes x 2 flops x 1965 MHz) -- no FP32 peak is measured.
     trav_ms = (ms[0] + ms[1]) if args.engine == "wavefront" else step_ms
     fp32_tflops = m["crossings"] * F_CROSS_FLOPS / (trav_ms / 1e3) / 1e12
     roof["fp32_side"] = {"crossings_per_step": m["crossings"], "flops_per_crossing": F_CROSS_FLOPS,
                          "achieved_tflops": fp32_tflops, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
                          "frac": fp32_tflops / FP32_NOMINAL_TFLOPS, "peak_source": "nominal"}
-    traffic_file = ROOT / "profiles" / "traffic.json"
-    if traffic_file.exists():
-        try:
-            tr = json.loads(traffic_file.read_text()).get(name)
-            if tr:  # DRAM bytes per unit from an ncu capture, scaled to this launch's units
-                roof["traffic"] = tr["dram_bytes_per_unit"] * units / launches
-                roof["traffic_source"] = tr["source"]
-        except (ValueError, KeyError, TypeError):
-            pass
     return roof
 
 
@@ -307,6 +379,9 @@ def run_ours(args):
         off = base + (i * BATCH_SPP) % args.spp
         return img.accumulate(scene, env, w.camera, tcfg, off, BATCH_SPP)
 
+    def new_render_starts(i):  # steps past spp/BATCH_SPP begin a fresh render of the same image
+        return i > 0 and (i * BATCH_SPP) % args.spp == 0
+
     # warm-up (also the first steps of the image)
     for i in range(args.warmup):
         step(i)
@@ -327,6 +402,8 @@ def run_ours(args):
     t_wall = time.perf_counter()
     step_stats = []
     for i in range(args.steps):
+        if new_render_starts(i):
+            img.clear()  # outside the step's events: each spp/16 consecutive steps are one full render
         with torch.cuda.stream(stream):
             flush.fill_(float(i))  # L2 flush, outside the step's events
             starts[i].record(stream)
@@ -357,14 +434,17 @@ def run_ours(args):
     value = paths_per_rank * world / (total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
 
-    roof = roofline(args, mstats, step_stats)
+    roof = roofline(args, mstats, step_stats, clk.get("sm_mhz"))
     launches = sum(st["launches"] for st in step_stats)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
             "config": {"workload": f"showcase_{args.n // 1000}k", "gaussians": args.n, "width": W, "height": H,
-                       "spp_per_rank": args.spp, "step": f"{BATCH_SPP} spp over the full image", "nee": "mis",
+                       "spp_per_rank": args.spp,
+                       "step": f"{BATCH_SPP} spp over the full image; every {args.spp // BATCH_SPP} consecutive steps "
+                               f"are one complete {args.spp}-spp render (the image is cleared, untimed, between renders)",
+                       "nee": "mis",
                        "max_depth": cfg.max_bounces, "rr_depth": cfg.rr_depth, "env": "procedural 2048x1024",
                        "engine": args.engine, "precision": "fast (FP32)",
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"samples x{world}"},
@@ -455,8 +535,8 @@ def differentiation_form(device):
     import torch
     import volprim_b200 as vp
     from volprim_b200 import _capi, scenes
-    from volprim_b200.autograd import render_emission_images
-    from volprim_b200.emission import render_emission, render_emission_backward
+    from volprim_b200.autograd import EmissionRender, render_emission_images
+    from volprim_b200.emission import render_emission
 
     w = scenes.emission_100k()
     ctx = vp.Context(device)
@@ -482,76 +562,114 @@ def differentiation_form(device):
 
     one()
     one()
-    times = []
+    times, splits = [], []
     for _ in range(7):
         t0 = time.perf_counter()
         one()
         times.append(time.perf_counter() - t0)
-    # kernel split on the built scene
-    sc = vp.Scene(ctx, g, w.sigma_multiplier)
-    sc.set_emission(w.emission)
-    n = g.count
-    grads = {k: np.zeros(m * n, np.float32) for k, m in (("mean", 3), ("scale", 3), ("quat_wxyz", 4), ("density", 1),
-                                                          ("emission", 3))}
-    img = torch.empty((w.config.image_height, w.config.image_width, 4), device=dev)
-    fwd_ms = bwd_ms = 0.0
-    for cam in w.cameras:
-        st = _capi.vp_render_stats()
-        p, cc = w.config.to_c(), cam.to_c()
-        _capi.check(_capi.lib.vp_render_emission(sc.handle, env.handle, C.byref(cc), C.byref(p), img.data_ptr(),
-                                                 _capi.VP_MEMORY_DEVICE, C.byref(st)))
-        fwd_ms += st.ms_kernels
-        dl = np.full((w.config.image_height, w.config.image_width, 4), 1e-3, np.float32)
-        bwd_ms += render_emission_backward(sc, env, cam, w.config, dl, grads)["ms_kernels"]
-    info = sc.info()
-    sc.close()
+        splits.append(dict(EmissionRender.last_ms))
     env.close()
     ctx.close()
     paths = len(w.cameras) * w.config.image_width * w.config.image_height * w.config.num_samples_per_pixel
     med = statistics.median(times)
+    split = {k: statistics.median(s[k] for s in splits) for k in splits[0]}
     return {"metric": "grad/s", "value": 1.0 / med, "unit": "grad/s",
             "ms_per_grad": 1e3 * med, "ms_per_grad_min": 1e3 * min(times), "timed_gradients": len(times),
             "workload": "emission_100k (100k Gaussians, 4 cameras, "
-            "256x256, 8 spp, FAST)", "paths_per_forward": paths, "forward_kernel_ms": fwd_ms,
-            "backward_kernel_ms": bwd_ms, "scene_build_ms": info["build_ms"],
+            "256x256, 8 spp, FAST)", "paths_per_forward": paths,
+            "scene_build_ms": split["scene_build"], "forward_kernel_ms": split["forward_kernels"],
+            "backward_kernel_ms": split["backward_kernels"],
             "note": "one gradient = scene build from the parameter tensors + 4 forward + 4 adjoint renders "
                     "(autograd Function), host-timed around torch.cuda.synchronize: median of 7 after 2 warm-up "
-                    "gradients (the host loop is sensitive to other load on the host); kernel split from CUDA events"}
+                    "gradients (the host loop is sensitive to other load on the host); scene build, forward and "
+                    "adjoint kernel times are CUDA-event times inside the same timed gradients (medians)"}
 
 
 def other_configs(device):
-    """The other two configurations, one timed pass each (wavefront engine, inputs resident):
-    the 256-Gaussian absorption case (128x128, 16 spp, ACCURATE, the FP64-gated image) and the
-    2M-Gaussian traversal stress case (1024x1024, one 16-spp batch of its 64 spp) with its BVH
-    build time and the overlap / hit counts of the measured batch."""
+    """The other two configurations (wavefront engine, inputs resident):
+    * the 256-Gaussian absorption case (128x128, 16 spp), in AUTO precision (the ACCURATE
+      float-pair set-up this albedo-0 scene selects) and in FAST, both FP32 arithmetic: 5 timed
+      renders each (median, min, max);
+    * the 2M-Gaussian traversal stress case at its stated size (1024x1024, all 64 spp as four
+      16-spp batches, timed twice), its BVH build time (3 builds) and, from one measured 16-spp
+      batch, the per-query chord-count histograms (power-of-two bins) behind its overlap and
+      hit maxima."""
     import torch
     import volprim_b200 as vp
     from volprim_b200 import scenes
 
+    def spread(v):
+        return {"median": statistics.median(v), "min": min(v), "max": max(v), "runs": len(v)}
+
     out = {}
     ctx = vp.Context(device)
-    for name, w, spp in (("absorption_256", scenes.absorption_256(), 16), ("stress_2m", scenes.stress_2m(), 16)):
-        cfg = w.config
-        cfg.engine = "wavefront"
+    w = scenes.absorption_256()
+    cfg = w.config
+    cfg.engine = "wavefront"
+    sc = vp.Scene(ctx, w.gaussians, w.sigma_multiplier)
+    env = vp.Environment(ctx, constant=(1.0, 1.0, 1.0))
+    img = vp.ProgressiveImage(ctx, cfg.image_width, cfg.image_height)
+    for prec in ("auto", "fast"):
+        c = vp.Config(**{**cfg.__dict__, "precision": prec})
+        img.accumulate(sc, env, w.camera, c, 0, cfg.num_samples_per_pixel)  # warm-up
+        rates, ms = [], []
+        for _ in range(5):
+            img.clear()
+            torch.cuda.synchronize()
+            st = img.accumulate(sc, env, w.camera, c, 0, cfg.num_samples_per_pixel)
+            rates.append(st["paths"] / (st["ms_kernels"] / 1e3) / 1e6)
+            ms.append(st["ms_kernels"])
+        out["absorption_256" if prec == "auto" else "absorption_256_fast"] = {
+            "mpaths_per_s": statistics.median(rates), "mpaths_per_s_spread": spread(rates), "ms": statistics.median(ms),
+            "paths": st["paths"], "gaussians": sc.info()["count"],
+            "precision": "auto = ACCURATE: FP32 with float-pair set-up and sums" if prec == "auto" else
+                         "FAST: FP32, hardware exp/log approximations"}
+    img.close()
+    env.close()
+    sc.close()
+
+    w = scenes.stress_2m()
+    cfg = w.config
+    cfg.engine = "wavefront"
+    builds = []
+    for _ in range(3):
         sc = vp.Scene(ctx, w.gaussians, w.sigma_multiplier)
-        env = vp.Environment(ctx, rgb=w.env) if w.env is not None else vp.Environment(ctx, constant=(1.0, 1.0, 1.0))
-        img = vp.ProgressiveImage(ctx, cfg.image_width, cfg.image_height)
-        img.accumulate(sc, env, w.camera, cfg, 0, min(spp, cfg.num_samples_per_pixel))  # warm-up
+        builds.append(sc.info()["build_ms"])
+        if len(builds) < 3:
+            sc.close()
+    env = vp.Environment(ctx, rgb=w.env)
+    img = vp.ProgressiveImage(ctx, cfg.image_width, cfg.image_height)
+    spp = cfg.num_samples_per_pixel
+    img.accumulate(sc, env, w.camera, cfg, 0, BATCH_SPP)  # warm-up
+    rates, totals = [], []
+    for _ in range(2):
         img.clear()
         torch.cuda.synchronize()
-        st = img.accumulate(sc, env, w.camera, cfg, 0, min(spp, cfg.num_samples_per_pixel))
-        mcfg = vp.Config(**{**cfg.__dict__, "measure_caps": True})
-        img.clear()
-        ms = img.accumulate(sc, env, w.camera, mcfg, 0, min(spp, cfg.num_samples_per_pixel))
-        info = sc.info()
-        out[name] = {"mpaths_per_s": st["paths"] / (st["ms_kernels"] / 1e3) / 1e6, "paths": st["paths"],
-                     "ms": st["ms_kernels"], "gaussians": info["count"], "bvh_build_ms": info["build_ms"],
-                     "bvh32_nodes": info["wide_nodes"], "precision": cfg.precision,
-                     "max_point_overlap": ms["max_point_overlap"], "max_hits_per_ray": ms["max_hits_per_ray"],
-                     "crossings": ms["crossings"]}
-        img.close()
-        env.close()
-        sc.close()
+        ms = paths = 0
+        for off in range(0, spp, BATCH_SPP):
+            st = img.accumulate(sc, env, w.camera, cfg, off, BATCH_SPP)
+            ms += st["ms_kernels"]
+            paths += st["paths"]
+        rates.append(paths / (ms / 1e3) / 1e6)
+        totals.append(ms)
+    mcfg = vp.Config(**{**cfg.__dict__, "measure_caps": True})
+    img.clear()
+    m = img.accumulate(sc, env, w.camera, mcfg, 0, BATCH_SPP)
+    info = sc.info()
+    out["stress_2m"] = {"mpaths_per_s": statistics.median(rates), "mpaths_per_s_spread": spread(rates),
+                        "ms_per_render": statistics.median(totals), "spp": spp, "paths": paths,
+                        "gaussians": info["count"], "bvh_build_ms": statistics.median(builds),
+                        "bvh_build_ms_spread": spread(builds), "bvh32_nodes": info["wide_nodes"],
+                        "precision": cfg.precision,
+                        "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"],
+                        "crossings_per_16spp": m["crossings"],
+                        "chords_per_query_hist": {
+                            "bins": "0, [1,2), [2,4), ..., [2^13, 2^14), >= 2^14",
+                            "argmin": m["hits_hist"][0], "transmittance": m["hits_hist"][1],
+                            "sample": "one measured 16-spp batch of the 1024x1024 image"}}
+    img.close()
+    env.close()
+    sc.close()
     ctx.close()
     return out
 

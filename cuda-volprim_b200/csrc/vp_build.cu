@@ -75,35 +75,61 @@ __global__ void k_precompute(uint32_t n, const float* __restrict__ mean,
   const float rx = __fdiv_rn(1.0f, sx), ry = __fdiv_rn(1.0f, sy), rz = __fdiv_rn(1.0f, sz);
   const float dnf = __fmul_rn(0.0634936359f, __fmul_rn(__fmul_rn(rx, ry), rz));
   const float icf = __fmul_rn(__fmul_rn(M, dnf), 1.2533141373f);
-  // Forward rotation matrix R(q) (include/thesis/host/utils/math.h:52-97 without scale).
-  const double dw = w, dx = x, dy = y, dz = z;
-  double R[3][3];
-  R[0][0] = 1.0 - 2.0 * (dy * dy + dz * dz);
-  R[0][1] = 2.0 * (dx * dy - dw * dz);
-  R[0][2] = 2.0 * (dx * dz + dw * dy);
-  R[1][0] = 2.0 * (dx * dy + dw * dz);
-  R[1][1] = 1.0 - 2.0 * (dx * dx + dz * dz);
-  R[1][2] = 2.0 * (dy * dz - dw * dx);
-  R[2][0] = 2.0 * (dx * dz - dw * dy);
-  R[2][1] = 2.0 * (dy * dz + dw * dx);
-  R[2][2] = 1.0 - 2.0 * (dx * dx + dy * dy);
-  const double rs[3] = {rx, ry, rz};
-  const double ss[3] = {sx, sy, sz};
+  // Forward rotation matrix R(q) (include/thesis/host/utils/math.h:52-97 without scale) as float
+  // pairs: each product of two quaternion components is exact as a TwoProduct pair, so every
+  // entry carries ~44 bits, and W = diag(rcp_scale) R^T is rounded to FP32 once.
+  auto sq2 = [](float a, float b, float c, float d, float sgn) {  // a*b + sgn*c*d as a float pair
+    float p, pe, q, qe, s, se;
+    two_prod(a, b, p, pe);
+    two_prod(c, d, q, qe);
+    if (sgn < 0.f) q = -q, qe = -qe;
+    two_sum(p, q, s, se);
+    FF r;
+    fast_two_sum(s, __fadd_rn(se, __fadd_rn(pe, qe)), r.hi, r.lo);
+    return r;
+  };
+  auto one_minus_2 = [](FF v) {  // 1 - 2 v
+    float s, se;
+    two_sum(1.0f, -2.0f * v.hi, s, se);
+    FF r;
+    fast_two_sum(s, __fsub_rn(se, 2.0f * v.lo), r.hi, r.lo);
+    return r;
+  };
+  auto twice = [](FF v) { return FF{2.0f * v.hi, 2.0f * v.lo}; };
+  FF R[3][3];
+  R[0][0] = one_minus_2(sq2(y, y, z, z, 1.f));
+  R[0][1] = twice(sq2(x, y, w, z, -1.f));
+  R[0][2] = twice(sq2(x, z, w, y, 1.f));
+  R[1][0] = twice(sq2(x, y, w, z, 1.f));
+  R[1][1] = one_minus_2(sq2(x, x, z, z, 1.f));
+  R[1][2] = twice(sq2(y, z, w, x, -1.f));
+  R[2][0] = twice(sq2(x, z, w, y, -1.f));
+  R[2][1] = twice(sq2(y, z, w, x, 1.f));
+  R[2][2] = one_minus_2(sq2(x, x, y, y, 1.f));
+  const float rs[3] = {rx, ry, rz};
+  const float ss[3] = {sx, sy, sz};
   float W[3][3];
   for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 3; ++c) W[r][c] = (float)(rs[r] * R[c][r]);
+    for (int c = 0; c < 3; ++c) {
+      float p, pe;
+      two_prod(rs[r], R[c][r].hi, p, pe);
+      W[r][c] = __fadd_rn(p, __fmaf_rn(rs[r], R[c][r].lo, pe));
+    }
   rec[4 * i + 0] = make_float4(cx, cy, cz, W[0][0]);
   rec[4 * i + 1] = make_float4(W[0][1], W[0][2], W[1][0], W[1][1]);
   rec[4 * i + 2] = make_float4(W[1][2], W[2][0], W[2][1], W[2][2]);
   rec[4 * i + 3] = make_float4(icf, ar, ag, ab);
-  double e[3];
+  float e[3];
+  const float cen[3] = {cx, cy, cz};
   for (int k = 0; k < 3; ++k) {
-    const double a0 = R[k][0] * ss[0], a1 = R[k][1] * ss[1], a2 = R[k][2] * ss[2];
-    // 3-sigma half extent along world axis k, padded so FP32 chord tests never escape it.
-    e[k] = 3.0 * sqrt(a0 * a0 + a1 * a1 + a2 * a2) * (1.0 + 1e-5) + 1e-7 * (1.0 + fabs((double)mean[3 * i + k]));
+    const float a0 = R[k][0].hi * ss[0], a1 = R[k][1].hi * ss[1], a2 = R[k][2].hi * ss[2];
+    // 3-sigma half extent along world axis k, padded (1e-5 relative, far above the few-ulp error
+    // of this FP32 evaluation) so FP32 chord tests never escape it; the box is rounded outward.
+    e[k] = __fadd_ru(__fmul_ru(3.0f * sqrtf(fmaf(a0, a0, fmaf(a1, a1, a2 * a2))), 1.0f + 1e-5f),
+                     1e-7f * (1.0f + fabsf(cen[k])));
   }
-  lo[i] = make_float4((float)((double)cx - e[0]), (float)((double)cy - e[1]), (float)((double)cz - e[2]), 0.f);
-  hi[i] = make_float4((float)((double)cx + e[0]), (float)((double)cy + e[1]), (float)((double)cz + e[2]), 0.f);
+  lo[i] = make_float4(__fsub_rd(cx, e[0]), __fsub_rd(cy, e[1]), __fsub_rd(cz, e[2]), 0.f);
+  hi[i] = make_float4(__fadd_ru(cx, e[0]), __fadd_ru(cy, e[1]), __fadd_ru(cz, e[2]), 0.f);
 }
 
 __device__ __forceinline__ unsigned int f2ord(float f) {

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "vp_internal.h"
 
@@ -339,6 +340,32 @@ vp_status vp_env_build_ms(vp_env* e, double* out) {
   return VP_OK;
 }
 
+vp_status vp_env_read_tables(vp_env* e, uint32_t* out_w, uint32_t* out_h, float* cond_prob, uint32_t* cond_alias,
+                             float* marg_prob, uint32_t* marg_alias, float* joint, float* out_total) {
+  if (!e || !e->ctx) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  const uint32_t W = e->view.width, H = e->view.height;
+  if (out_w) *out_w = W;
+  if (out_h) *out_h = H;
+  if (out_total) *out_total = e->view.total;
+  const size_t n = (size_t)W * H;
+  VP_CUDA(cudaSetDevice(e->ctx->device));
+  cudaStream_t st = e->ctx->stream;
+  std::vector<float2> cond(cond_prob || cond_alias ? n : 0), marg(marg_prob || marg_alias ? H : 0);
+  if (!cond.empty()) VP_CUDA(cudaMemcpyAsync(cond.data(), e->cond, n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  if (!marg.empty()) VP_CUDA(cudaMemcpyAsync(marg.data(), e->marg, H * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  if (joint) VP_CUDA(cudaMemcpyAsync(joint, e->joint, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  VP_CUDA(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < cond.size(); ++i) {
+    if (cond_prob) cond_prob[i] = cond[i].x;
+    if (cond_alias) std::memcpy(cond_alias + i, &cond[i].y, sizeof(uint32_t));
+  }
+  for (size_t i = 0; i < marg.size(); ++i) {
+    if (marg_prob) marg_prob[i] = marg[i].x;
+    if (marg_alias) std::memcpy(marg_alias + i, &marg[i].y, sizeof(uint32_t));
+  }
+  return VP_OK;
+}
+
 vp_status vp_env_destroy(vp_env* e) {
   if (!e) return VP_OK;
   cudaStream_t st = e->ctx ? e->ctx->stream : nullptr;
@@ -542,6 +569,8 @@ vp_status vp_render_accumulate(vp_scene* s, vp_env* e, const vp_camera* cam, con
     stats->max_point_overlap = c.max_overlap;
     stats->device_status = c.status;
     stats->launches = ctx->launches;
+    for (int q = 0; q < 2; ++q)
+      for (int b = 0; b < 16; ++b) stats->hits_hist[q][b] = c.hits_hist[q][b];
     if (ctx->time_stages) {
       stats->ms_stage[0] = ctx->stage_ms[0];
       stats->ms_stage[1] = ctx->stage_ms[1];

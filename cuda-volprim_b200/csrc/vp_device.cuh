@@ -17,7 +17,10 @@
 // with icf = M (2 pi)^(-3/2) / prod(s) * sqrt(pi/2) (the reference's inv_cdf_factor_).
 // Computing p_perp from o - c + t_c d in world space avoids the cancellation of the
 // reference's p + t w form (|p| ~ distance/scale), which bounds FP32 transmittance accuracy
-// well above 1e-5; the ACCURATE variant does this set-up in FP64.
+// well above 1e-5.  Everything here is FP32.  The ACCURATE variant carries the closest-approach
+// vector, p_perp and d2 as unevaluated float pairs (hi + lo, built from the error-free TwoSum and
+// FMA TwoProduct transforms), so 9 - d2 and the half-chord keep their bits on grazing chords,
+// and sums optical depth in float pairs too.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -111,7 +114,11 @@ struct Counters {  // device-side statistics (only touched when ParamsView::meas
   unsigned long long kind_nodes[3], kind_leaves[3], kind_prims[3], kind_geo[3];
   unsigned int max_hits, max_overlap, status;
   unsigned long long skipped;  // paths of converged pixels not traced (adaptive sampling)
+  unsigned long long hits_hist[2][16];  // queries by chords evaluated, power-of-two bins (argmin, tau)
 };
+
+// Power-of-two bin of a per-query chord count: 0 -> 0, [2^(k-1), 2^k) -> k, >= 2^14 -> 15.
+__device__ __forceinline__ int hits_bin(unsigned int n) { return n == 0u ? 0 : min(15, 32 - __clz(n)); }
 
 // ---- small vector helpers ----------------------------------------------------------------
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -126,6 +133,78 @@ __device__ __forceinline__ float fmax3(float3 v) { return fmaxf(fmaxf(v.x, v.y),
 __device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
 __device__ __forceinline__ float3 fma3(float a, float3 b, float3 c) {
   return f3(fmaf(a, b.x, c.x), fmaf(a, b.y, c.y), fmaf(a, b.z, c.z));
+}
+
+// ---- float pairs: a value carried as an unevaluated sum hi + lo of two floats --------------
+// Error-free transforms (Knuth's TwoSum, Dekker's FastTwoSum, the FMA TwoProduct) with IEEE
+// round-to-nearest intrinsics, which the compiler neither contracts nor reassociates.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+__device__ __forceinline__ void fast_two_sum(float a, float b, float& s, float& e) {  // |a| >= |b|
+  s = __fadd_rn(a, b);
+  e = __fsub_rn(b, __fsub_rn(s, a));
+}
+__device__ __forceinline__ void two_prod(float a, float b, float& p, float& e) {
+  p = __fmul_rn(a, b);
+  e = __fmaf_rn(a, b, -p);
+}
+struct FF {
+  float hi, lo;
+};
+// hi + lo of a + b, with a and b float pairs
+__device__ __forceinline__ FF ff_add(FF a, FF b) {
+  float s, e;
+  two_sum(a.hi, b.hi, s, e);
+  FF r;
+  fast_two_sum(s, __fadd_rn(e, __fadd_rn(a.lo, b.lo)), r.hi, r.lo);
+  return r;
+}
+// acc += v (float), compensated
+__device__ __forceinline__ void ff_accumulate(FF& acc, float v) {
+  float s, e;
+  two_sum(acc.hi, v, s, e);
+  acc.hi = s;
+  acc.lo = __fadd_rn(acc.lo, e);
+}
+// W x for x = xh + xl, as float pairs per component: sum_j W_ij xh_j exactly (TwoProduct +
+// TwoSum) plus the first-order terms W_ij xl_j.
+__device__ __forceinline__ void mat_vec_ff(const float (&W)[9], const float (&xh)[3], const float (&xl)[3],
+                                           FF (&y)[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float s, lo;
+    two_prod(W[3 * i], xh[0], s, lo);
+    lo = __fmaf_rn(W[3 * i], xl[0], lo);
+#pragma unroll
+    for (int j = 1; j < 3; ++j) {
+      float p, pe, s2, se;
+      two_prod(W[3 * i + j], xh[j], p, pe);
+      two_sum(s, p, s2, se);
+      s = s2;
+      lo = __fadd_rn(lo, __fadd_rn(se, __fmaf_rn(W[3 * i + j], xl[j], pe)));
+    }
+    fast_two_sum(s, lo, y[i].hi, y[i].lo);
+  }
+}
+// |y|^2 of a float-pair vector, as a float pair
+__device__ __forceinline__ FF norm2_ff(const FF (&y)[3]) {
+  float s, lo;
+  two_prod(y[0].hi, y[0].hi, s, lo);
+  lo = __fmaf_rn(2.0f * y[0].hi, y[0].lo, lo);
+#pragma unroll
+  for (int i = 1; i < 3; ++i) {
+    float p, pe, s2, se;
+    two_prod(y[i].hi, y[i].hi, p, pe);
+    two_sum(s, p, s2, se);
+    s = s2;
+    lo = __fadd_rn(lo, __fadd_rn(se, __fmaf_rn(2.0f * y[i].hi, y[i].lo, pe)));
+  }
+  FF r;
+  fast_two_sum(s, lo, r.hi, r.lo);
+  return r;
 }
 
 // ---- RNG: PCG32 + 64-bit mixer, restated from device/core/random.cuh:16-58 ----------------
@@ -220,11 +299,12 @@ __device__ __forceinline__ float3 whiten(const PrimGeo& g, float3 v) {
 
 // Chord of a ray through a Gaussian's 3-sigma ellipsoid, in the closest-approach frame.
 struct Chord {
-  float tc;   // ray parameter of the closest whitened approach
-  float rw;   // 1 / |W d|
-  float d2;   // squared whitened distance of closest approach
-  float h;    // whitened half-chord sqrt(9 - d2)
+  float tc;    // ray parameter of the closest whitened approach
+  float rw;    // 1 / |W d|
+  float d2;    // squared whitened distance of closest approach
+  float h;     // whitened half-chord sqrt(9 - d2)
   float t_in, t_out;
+  float d2lo;  // ACCURATE: low part of d2 (d2 + d2lo is the float-pair value); 0 otherwise
 };
 
 // FP32 set-up.  o - c is split into hi + lo parts (TwoSum) so the world-space closest-approach
@@ -263,38 +343,58 @@ __device__ __forceinline__ bool chord_fast(const PrimGeo& g, float3 o, float3 d,
   ch.h = h;
   ch.t_in = fmaf(-h, rw, tc);
   ch.t_out = fmaf(h, rw, tc);
+  ch.d2lo = 0.0f;
   return true;
 }
 
-// FP64 set-up (ACCURATE).  Results are rounded to FP32 once at the end.
+// ACCURATE set-up, FP32 with float pairs.  o - c is exact as hi + lo (TwoSum); the closest
+// approach r = (o - c) + t_c d is formed as a float pair (TwoProduct of t_c d, TwoSum with the
+// hi part), p_perp = W r and d2 = |p_perp|^2 as float pairs; 9 - d2 is then exact up to the
+// pair's rounding, and h = sqrt(9 - d2) gets its first-order correction.  t_c itself needs no
+// extra bits: an error in it moves r along d, which changes d2 only to second order.
 __device__ __forceinline__ bool chord_accurate(const PrimGeo& g, float3 o, float3 d, Chord& ch) {
-  const double W00 = g.a.w, W01 = g.b.x, W02 = g.b.y, W10 = g.b.z, W11 = g.b.w, W12 = g.c.x,
-               W20 = g.c.y, W21 = g.c.z, W22 = g.c.w;
-  const double Dx = (double)o.x - (double)g.a.x, Dy = (double)o.y - (double)g.a.y,
-               Dz = (double)o.z - (double)g.a.z;
-  const double dx = d.x, dy = d.y, dz = d.z;
-  const double wx = W00 * dx + W01 * dy + W02 * dz;
-  const double wy = W10 * dx + W11 * dy + W12 * dz;
-  const double wz = W20 * dx + W21 * dy + W22 * dz;
-  const double qx = W00 * Dx + W01 * Dy + W02 * Dz;
-  const double qy = W10 * Dx + W11 * Dy + W12 * Dz;
-  const double qz = W20 * Dx + W21 * Dy + W22 * Dz;
-  const double a2 = wx * wx + wy * wy + wz * wz;
-  const double tc = -(qx * wx + qy * wy + qz * wz) / a2;
-  const double rx = Dx + tc * dx, ry = Dy + tc * dy, rz = Dz + tc * dz;
-  const double px = W00 * rx + W01 * ry + W02 * rz;
-  const double py = W10 * rx + W11 * ry + W12 * rz;
-  const double pz = W20 * rx + W21 * ry + W22 * rz;
-  const double d2 = px * px + py * py + pz * pz;
-  if (!(d2 < 9.0)) return false;
-  const double h = sqrt(9.0 - d2);
-  const double rw = 1.0 / sqrt(a2);
-  ch.tc = (float)tc;
-  ch.rw = (float)rw;
-  ch.d2 = (float)d2;
-  ch.h = (float)h;
-  ch.t_in = (float)(tc - h * rw);
-  ch.t_out = (float)(tc + h * rw);
+  float Dh[3], Dl[3];
+  two_sum(o.x, -g.a.x, Dh[0], Dl[0]);
+  two_sum(o.y, -g.a.y, Dh[1], Dl[1]);
+  two_sum(o.z, -g.a.z, Dh[2], Dl[2]);
+  const float3 w = whiten(g, d);
+  const float3 q = whiten(g, f3(Dh[0], Dh[1], Dh[2]));
+  const float a2 = dot3(w, w);
+  const float ra = __frcp_rn(a2);
+  const float qw = dot3(q, w);
+  {  // the FAST path's conservative early miss (same chords with or without it)
+    const float qq = dot3(q, q);
+    if (fmaf(-qw * qw, ra, qq) > fmaf(1e-5f, qq, kExtent2 + 1e-4f)) return false;
+  }
+  const float tc = -qw * ra;
+  const float dd[3] = {d.x, d.y, d.z};
+  float rh[3], rl[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float p, pe, s, se;
+    two_prod(tc, dd[k], p, pe);
+    two_sum(Dh[k], p, s, se);
+    fast_two_sum(s, __fadd_rn(se, __fadd_rn(pe, Dl[k])), rh[k], rl[k]);
+  }
+  const float W[9] = {g.a.w, g.b.x, g.b.y, g.b.z, g.b.w, g.c.x, g.c.y, g.c.z, g.c.w};
+  FF pp[3];
+  mat_vec_ff(W, rh, rl, pp);
+  const FF d2 = norm2_ff(pp);
+  if (!(d2.hi < kExtent2)) return false;
+  float m, me;
+  two_sum(kExtent2, -d2.hi, m, me);
+  me = __fsub_rn(me, d2.lo);
+  if (!(m + me > 0.0f)) return false;
+  const float hs = __fsqrt_rn(m);
+  const float h = __fmaf_rn(me, __fdividef(0.5f, hs), hs);
+  const float rw = __frsqrt_rn(a2);
+  ch.tc = tc;
+  ch.rw = rw;
+  ch.d2 = d2.hi;
+  ch.h = h;
+  ch.t_in = fmaf(-h, rw, tc);
+  ch.t_out = fmaf(h, rw, tc);
+  ch.d2lo = d2.lo;
   return true;
 }
 
@@ -318,12 +418,20 @@ __device__ __forceinline__ float erf_diff(float a, float b) {
 
 // Optical depth of one Gaussian over the ray segment [max(t_in, t_lo), t_out]
 // (Primitive::optical_depth, primitive.h:249-318; zero below RAY_SEGMENT_MIN_LENGTH).
+// exp(-(d2 + d2lo) / 2) for a float-pair d2 (first order in the low part).
+template <bool kAcc>
+__device__ __forceinline__ float gauss_d2(float d2, float d2lo) {
+  const float e = vexp<kAcc>(-0.5f * d2);
+  if constexpr (kAcc) return __fmaf_rn(e, -0.5f * d2lo, e);
+  else return e;
+}
+
 template <bool kAcc>
 __device__ __forceinline__ float chord_tau(float tc, float rw, float d2, float h, float u0,
-                                           float t_start, float t_out, float icf) {
+                                           float t_start, float t_out, float icf, float d2lo = 0.0f) {
   (void)tc;
   if (t_out - t_start <= kSegmentMin) return 0.0f;
-  return icf * rw * vexp<kAcc>(-0.5f * d2) * erf_diff(u0, h);
+  return icf * rw * gauss_d2<kAcc>(d2, d2lo) * erf_diff(u0, h);
 }
 
 // Analog free flight inside one Gaussian, restricted to t >= segment start, with the
@@ -333,9 +441,9 @@ __device__ __forceinline__ float chord_tau(float tc, float rw, float d2, float h
 template <bool kAcc>
 __device__ __forceinline__ float chord_free_flight(float tc, float rw, float d2, float h,
                                                    float u0, float t_in, float t_out, float icf,
-                                                   float tau) {
+                                                   float tau, float d2lo = 0.0f) {
   (void)h;
-  const float K = icf * rw * vexp<kAcc>(-0.5f * d2);
+  const float K = icf * rw * gauss_d2<kAcc>(d2, d2lo);
   const float raw = erff(u0 * kInvSqrt2) + tau / K;
   if (!(raw <= 1.0f)) return kInf;  // raw > 1 (or NaN): no scatter in this Gaussian
   const float arg = fmaxf(raw, -1.0f);
@@ -526,10 +634,16 @@ __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
   return v;
 }
-__device__ __forceinline__ double warp_sum(double v) {
+// Sum of the lanes' float pairs, as a float.
+__device__ __forceinline__ float warp_sum_ff(FF v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-  return v;
+  for (int o = 16; o > 0; o >>= 1) {
+    FF w;
+    w.hi = __shfl_xor_sync(0xFFFFFFFFu, v.hi, o);
+    w.lo = __shfl_xor_sync(0xFFFFFFFFu, v.lo, o);
+    v = ff_add(v, w);
+  }
+  return __fadd_rn(v.hi, v.lo);
 }
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll

@@ -106,7 +106,8 @@ __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3
 // tau of one chord over [max(t_in, 0), t_out] (0 for a segment below RAY_SEGMENT_MIN_LENGTH).
 template <bool kAcc>
 __device__ __forceinline__ float chord_tau0(const Chord& ch, float icf) {
-  return chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, icf);
+  return chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, icf,
+                         ch.d2lo);
 }
 
 // The ray of (pixel, sample): the renderer's jittered camera ray (raygen.cuh:82-99).
@@ -159,7 +160,7 @@ __device__ __forceinline__ float3 ray_radiance(const RaySums& rs, float3 env) {
 }
 
 // Resident 256-thread blocks per SM the FP32 emission kernels' register budgets are sized for
-// (64 registers; the FP64 variants keep 2).  On the differentiation workload 4 blocks take the
+// (64 registers; the ACCURATE float-pair variants keep 2, which holds their ~100 registers).  On the differentiation workload 4 blocks take the
 // forward from 56.5 to 49.2 ms and the adjoint from 127 to 114 ms against the compiler's own
 // budgets (76 and 80 registers: 3 blocks).
 #ifndef VP_EMIS_FWD_BLOCKS
@@ -210,62 +211,68 @@ __global__ void __launch_bounds__(256, kAcc ? 2 : VP_EMIS_FWD_BLOCKS) k_emis_for
 // For a ray that enters the chord (t_in >= 0) tau depends on the line only, so x0 is the closest
 // approach o + t_c d: then |p| <= 3 and no term carries the camera's lever arm |o - mu| / s (which
 // would make the accumulated dLoss/dW cancel to a few digits).  For an origin inside the chord,
-// x0 = o, already within 3 whitened units.  v returns x0 - mu.  ACCURATE runs this in FP64.
-// Returns false (no contribution) for a segment below RAY_SEGMENT_MIN_LENGTH.
+// x0 = o, already within 3 whitened units.  v returns x0 - mu, formed as the chord set-up forms it
+// (o - mu exact as a float pair, plus t_c d).  FP32; under kAcc p and d2 are float pairs, as in
+// chord_accurate.  Returns false (no contribution) for a segment below RAY_SEGMENT_MIN_LENGTH.
 template <bool kAcc>
 __device__ __forceinline__ bool tau_grad(const PrimGeo& g, const Chord& ch, float3 o, float3 d, float& tau,
                                          float3& v, float3& dp, float3& dw) {
   const float t0 = fmaxf(ch.t_in, 0.0f);
   if (ch.t_out - t0 <= kSegmentMin) return false;
   const bool inside = !(ch.t_in >= 0.0f);
-  using R = typename std::conditional<kAcc, double, float>::type;
-  R vx, vy, vz;
-  if constexpr (kAcc) {
-    vx = (double)o.x - g.a.x;
-    vy = (double)o.y - g.a.y;
-    vz = (double)o.z - g.a.z;
-    if (!inside) {
-      vx += (double)ch.tc * d.x;
-      vy += (double)ch.tc * d.y;
-      vz += (double)ch.tc * d.z;
-    }
-  } else {  // o - mu as hi + lo (TwoSum), then + t_c d, as the FP32 chord set-up does
-    float3 dh, dl;
-    dh.x = o.x - g.a.x; { const float bb = dh.x - o.x; dl.x = (o.x - (dh.x - bb)) + (-g.a.x - bb); }
-    dh.y = o.y - g.a.y; { const float bb = dh.y - o.y; dl.y = (o.y - (dh.y - bb)) + (-g.a.y - bb); }
-    dh.z = o.z - g.a.z; { const float bb = dh.z - o.z; dl.z = (o.z - (dh.z - bb)) + (-g.a.z - bb); }
-    const float t = inside ? 0.0f : ch.tc;
-    vx = fmaf(t, d.x, dh.x) + dl.x;
-    vy = fmaf(t, d.y, dh.y) + dl.y;
-    vz = fmaf(t, d.z, dh.z) + dl.z;
+  float Dh[3], Dl[3];
+  two_sum(o.x, -g.a.x, Dh[0], Dl[0]);
+  two_sum(o.y, -g.a.y, Dh[1], Dl[1]);
+  two_sum(o.z, -g.a.z, Dh[2], Dl[2]);
+  const float t = inside ? 0.0f : ch.tc;
+  const float dd[3] = {d.x, d.y, d.z};
+  float vh[3], vl[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float pr, pe, sm, se;
+    two_prod(t, dd[k], pr, pe);
+    two_sum(Dh[k], pr, sm, se);
+    fast_two_sum(sm, __fadd_rn(se, __fadd_rn(pe, Dl[k])), vh[k], vl[k]);
   }
-  const R W00 = g.a.w, W01 = g.b.x, W02 = g.b.y, W10 = g.b.z, W11 = g.b.w, W12 = g.c.x, W20 = g.c.y,
-          W21 = g.c.z, W22 = g.c.w;
-  const R px = W00 * vx + W01 * vy + W02 * vz, py = W10 * vx + W11 * vy + W12 * vz,
-          pz = W20 * vx + W21 * vy + W22 * vz;
-  const R wx = W00 * d.x + W01 * d.y + W02 * d.z, wy = W10 * d.x + W11 * d.y + W12 * d.z,
-          wz = W20 * d.x + W21 * d.y + W22 * d.z;
-  const R A = wx * wx + wy * wy + wz * wz, B = px * wx + py * wy + pz * wz;
-  const R rA = R(1) / A, rw = R(1) / sqrt(A);
-  const R d2 = px * px + py * py + pz * pz - B * B * rA;
-  if (!(d2 < R(9))) return false;
-  const R h = sqrt(R(9) - d2);
-  const R u = inside ? B * rw : -h;
-  const R E = exp(R(-0.5) * d2);
-  const R base = R(g.icf) * rw;
-  const R k2pi = R(0.79788456080286535588), kis2 = R(0.70710678118654752440);
-  const R D = inside ? erf(h * kis2) - erf(u * kis2) : R(2) * erf(h * kis2);
-  const R t = base * E * D;
-  const R dtau_dh = (inside ? R(1) : R(2)) * base * k2pi * R(0.011108996538242306);
-  const R dtau_dd2 = R(-0.5) * t - dtau_dh * R(0.5) / h;
-  const R dtau_du = inside ? -base * E * k2pi * exp(R(-0.5) * u * u) : R(0);
-  const R gP = dtau_dd2;
-  const R gB = dtau_dd2 * (R(-2) * B * rA) + dtau_du * rw;
-  const R gA = R(-0.5) * t * rA + dtau_dd2 * B * B * rA * rA - dtau_du * R(0.5) * B * rA * rw;
-  tau = (float)t;
-  v = f3((float)vx, (float)vy, (float)vz);
-  dp = f3((float)(R(2) * gP * px + gB * wx), (float)(R(2) * gP * py + gB * wy), (float)(R(2) * gP * pz + gB * wz));
-  dw = f3((float)(R(2) * gA * wx + gB * px), (float)(R(2) * gA * wy + gB * py), (float)(R(2) * gA * wz + gB * pz));
+  const float W[9] = {g.a.w, g.b.x, g.b.y, g.b.z, g.b.w, g.c.x, g.c.y, g.c.z, g.c.w};
+  float px, py, pz, pp, pplo = 0.0f;
+  if constexpr (kAcc) {
+    FF p3[3];
+    mat_vec_ff(W, vh, vl, p3);
+    const FF n2 = norm2_ff(p3);
+    px = p3[0].hi, py = p3[1].hi, pz = p3[2].hi;
+    pp = n2.hi;
+    pplo = n2.lo;
+  } else {
+    const float3 pv = whiten(g, f3(vh[0] + vl[0], vh[1] + vl[1], vh[2] + vl[2]));
+    px = pv.x, py = pv.y, pz = pv.z;
+    pp = dot3(pv, pv);
+  }
+  const float3 w3 = whiten(g, d);
+  const float wx = w3.x, wy = w3.y, wz = w3.z;
+  const float A = dot3(w3, w3), B = fmaf(px, wx, fmaf(py, wy, pz * wz));
+  const float rA = __frcp_rn(A), rw = __frsqrt_rn(A);
+  // d2 = p.p - B^2 / A; at the closest approach B = 0 up to rounding, so the pair's low part
+  // carries the bits that matter on grazing chords
+  const float d2 = __fadd_rn(fmaf(-B * B, rA, pp), pplo);
+  if (!(d2 < 9.0f)) return false;
+  const float h = sqrtf(9.0f - d2);
+  const float u = inside ? B * rw : -h;
+  const float E = expf(-0.5f * d2);
+  const float base = g.icf * rw;
+  const float k2pi = 0.79788456080286535588f, kis2 = 0.70710678118654752440f;
+  const float D = inside ? erff(h * kis2) - erff(u * kis2) : 2.0f * erff(h * kis2);
+  const float tt = base * E * D;
+  const float dtau_dh = (inside ? 1.0f : 2.0f) * base * k2pi * 0.011108996538242306f;
+  const float dtau_dd2 = -0.5f * tt - dtau_dh * 0.5f / h;
+  const float dtau_du = inside ? -base * E * k2pi * expf(-0.5f * u * u) : 0.0f;
+  const float gP = dtau_dd2;
+  const float gB = dtau_dd2 * (-2.0f * B * rA) + dtau_du * rw;
+  const float gA = -0.5f * tt * rA + dtau_dd2 * B * B * rA * rA - dtau_du * 0.5f * B * rA * rw;
+  tau = tt;
+  v = f3(vh[0] + vl[0], vh[1] + vl[1], vh[2] + vl[2]);
+  dp = f3(2.0f * gP * px + gB * wx, 2.0f * gP * py + gB * wy, 2.0f * gP * pz + gB * wz);
+  dw = f3(2.0f * gA * wx + gB * px, 2.0f * gA * wy + gB * py, 2.0f * gA * wz + gB * pz);
   return true;
 }
 
@@ -338,41 +345,40 @@ __global__ void k_emis_finish(uint32_t n, const uint32_t* __restrict__ perm, con
   if (i >= n) return;
   const uint32_t c = perm[i];
   const float4 a0 = acc[4 * i], a1 = acc[4 * i + 1], a2 = acc[4 * i + 2], a3 = acc[4 * i + 3];
-  const double gW[3][3] = {{a0.x, a0.y, a0.z}, {a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x}};
-  const double gP[3] = {a2.y, a2.z, a2.w};
-  const double gK = a3.x;
+  const float gW[3][3] = {{a0.x, a0.y, a0.z}, {a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x}};
+  const float gP[3] = {a2.y, a2.z, a2.w};
+  const float gK = a3.x;
   const float4 r0 = prims[4 * i], r1 = prims[4 * i + 1], r2 = prims[4 * i + 2];
-  const double W[3][3] = {{r0.w, r1.x, r1.y}, {r1.z, r1.w, r2.x}, {r2.y, r2.z, r2.w}};
+  const float W[3][3] = {{r0.w, r1.x, r1.y}, {r1.z, r1.w, r2.x}, {r2.y, r2.z, r2.w}};
   const float4 q4 = raw[2 * i], sd = raw[2 * i + 1];
-  for (int l = 0; l < 3; ++l)
-    g_mean[3 * c + l] += (float)-(W[0][l] * gP[0] + W[1][l] * gP[1] + W[2][l] * gP[2]);
-  double s[3] = {sd.x, sd.y, sd.z};
+  for (int l = 0; l < 3; ++l) g_mean[3 * c + l] += -(W[0][l] * gP[0] + W[1][l] * gP[1] + W[2][l] * gP[2]);
+  float s[3] = {sd.x, sd.y, sd.z};
   if (scale_is_log)
-    for (int k = 0; k < 3; ++k) s[k] = exp(s[k]);
+    for (int k = 0; k < 3; ++k) s[k] = expf(s[k]);
   for (int k = 0; k < 3; ++k) {
-    const double gs = -(gW[k][0] * W[k][0] + gW[k][1] * W[k][1] + gW[k][2] * W[k][2] + gK) / s[k];
-    g_scale[3 * c + k] += (float)(scale_is_log ? gs * s[k] : gs);
+    const float gs = -(gW[k][0] * W[k][0] + gW[k][1] * W[k][1] + gW[k][2] * W[k][2] + gK) / s[k];
+    g_scale[3 * c + k] += scale_is_log ? gs * s[k] : gs;
   }
   // dL/dR_lk = gW_kl / s_k
-  double gR[3][3];
+  float gR[3][3];
   for (int l = 0; l < 3; ++l)
     for (int k = 0; k < 3; ++k) gR[l][k] = gW[k][l] / s[k];
-  const double qn = sqrt((double)q4.x * q4.x + (double)q4.y * q4.y + (double)q4.z * q4.z + (double)q4.w * q4.w);
-  const double w = q4.x / qn, x = q4.y / qn, y = q4.z / qn, z = q4.w / qn;
+  const float qn = sqrtf(q4.x * q4.x + q4.y * q4.y + q4.z * q4.z + q4.w * q4.w);
+  const float w = q4.x / qn, x = q4.y / qn, y = q4.z / qn, z = q4.w / qn;
   // R(q) = [[1-2(y2+z2), 2(xy-wz), 2(xz+wy)], [2(xy+wz), 1-2(x2+z2), 2(yz-wx)], [2(xz-wy), 2(yz+wx), 1-2(x2+y2)]]
-  const double gw = 2.0 * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
-  const double gx = 2.0 * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0 * x * gR[1][1] - w * gR[1][2] +
-                           z * gR[2][0] + w * gR[2][1] - 2.0 * x * gR[2][2]);
-  const double gy = 2.0 * (-2.0 * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] -
-                           w * gR[2][0] + z * gR[2][1] - 2.0 * y * gR[2][2]);
-  const double gz = 2.0 * (-2.0 * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0 * z * gR[1][1] +
+  const float gw = 2.0f * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
+  const float gx = 2.0f * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0f * x * gR[1][1] - w * gR[1][2] +
+                           z * gR[2][0] + w * gR[2][1] - 2.0f * x * gR[2][2]);
+  const float gy = 2.0f * (-2.0f * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] -
+                           w * gR[2][0] + z * gR[2][1] - 2.0f * y * gR[2][2]);
+  const float gz = 2.0f * (-2.0f * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0f * z * gR[1][1] +
                            y * gR[1][2] + x * gR[2][0] + y * gR[2][1]);
-  const double dotq = w * gw + x * gx + y * gy + z * gz;
-  g_quat[4 * c + 0] += (float)((gw - w * dotq) / qn);
-  g_quat[4 * c + 1] += (float)((gx - x * dotq) / qn);
-  g_quat[4 * c + 2] += (float)((gy - y * dotq) / qn);
-  g_quat[4 * c + 3] += (float)((gz - z * dotq) / qn);
-  g_dens[c] += (float)(gK / (double)sd.w);
+  const float dotq = w * gw + x * gx + y * gy + z * gz;
+  g_quat[4 * c + 0] += (gw - w * dotq) / qn;
+  g_quat[4 * c + 1] += (gx - x * dotq) / qn;
+  g_quat[4 * c + 2] += (gy - y * dotq) / qn;
+  g_quat[4 * c + 3] += (gz - z * dotq) / qn;
+  g_dens[c] += gK / sd.w;
   if (g_emis) {
     g_emis[3 * c + 0] += a3.y;
     g_emis[3 * c + 1] += a3.z;

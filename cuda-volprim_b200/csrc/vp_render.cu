@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
   const uint32_t n_pix = P.width * P.height;
   uint32_t status = 0;
   WarpStats ws;
+  if (kMeasure && P.measure != 0) ws.hist = &ctr->hits_hist[0][0];
   PathStats ps;
   WarpQueries<kAcc> q{S, W, status, ws, kMeasure && P.measure != 0};
   while (true) {
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(128) k_render_mega(SceneView S, EnvView E, Cam
   const uint32_t px = blockIdx.x * 16 + (threadIdx.x & 15);
   const uint32_t py = blockIdx.y * 8 + (threadIdx.x >> 4);
   uint32_t status = 0;
-  WarpStats ws;
+  WarpStats ws;  // no hit histogram here: the baseline kernel keeps its registers
   PathStats ps;
   const bool inside = px < P.width && py < P.height;
   if (inside) {

@@ -36,7 +36,7 @@ constexpr uint32_t kAliveBit = 1u << 18;
 // Resident 256-thread blocks per SM the extend / shadow kernels' register budgets are sized for:
 // 4 (64 registers) for extend; 5 (48 registers, 52 B of spills) for the FP32 shadow kernel, whose
 // smaller state gains more from the extra warps than it loses to the spills (-2% shadow time on
-// the showcase; extend at 5 spills 116 B and loses 9%).  The FP64 (ACCURATE) shadow kernel keeps
+// the showcase; extend at 5 spills 116 B and loses 9%).  The ACCURATE (float-pair) shadow kernel keeps
 // the extend budget.
 #ifndef VP_WF_MIN_BLOCKS
 #define VP_WF_MIN_BLOCKS 4
@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
   unsigned long long bounces = 0, scatters = 0;
   WarpStats ws;
   const bool measure = kMeasure && P.measure != 0;
+  if (measure) ws.hist = &ctr->hits_hist[0][0];
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(work, 1u);
@@ -252,6 +253,7 @@ __global__ void __launch_bounds__(256, kAcc ? VP_WF_MIN_BLOCKS : VP_WF_SHADOW_MI
   uint32_t status = 0;
   WarpStats ws;
   const bool measure = kMeasure && measure_i != 0;
+  if (measure) ws.hist = &ctr->hits_hist[0][0];
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(work, 1u);

@@ -136,6 +136,7 @@ class vp_render_stats(C.Structure):
         ("stage_launches", C.c_uint32 * 3),
         ("reserved", C.c_uint32),
         ("paths_skipped", C.c_uint64),
+        ("hits_hist", (C.c_uint64 * 16) * 2),
     ]
 
     def as_dict(self) -> dict:
@@ -144,7 +145,9 @@ class vp_render_stats(C.Structure):
             if name == "reserved":
                 continue
             v = getattr(self, name)
-            out[name] = list(v) if isinstance(v, C.Array) else v
+            if isinstance(v, C.Array):
+                v = [list(x) if isinstance(x, C.Array) else x for x in v]
+            out[name] = v
         return out
 
 
@@ -227,6 +230,7 @@ SIGNATURES = {
     "vp_env_create": [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, PP],
     "vp_env_create_constant": [P, C.c_float, C.c_float, C.c_float, PP],
     "vp_env_build_ms": [P, C.POINTER(C.c_double)],
+    "vp_env_read_tables": [P, P, P, P, P, P, P, P, P],
     "vp_env_destroy": [P],
     "vp_render_params_default": [C.POINTER(vp_render_params)],
     "vp_image_create": [P, C.c_uint32, C.c_uint32, PP],

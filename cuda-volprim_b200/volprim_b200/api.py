@@ -295,6 +295,21 @@ class Environment:
         check(lib.vp_env_build_ms(self.handle, C.byref(v)))
         return v.value
 
+    def tables(self) -> dict:
+        """The device-built sampling tables (vp_env_read_tables): per texel the alias probability,
+        alias texel and joint weight (H x W), per row the marginal alias probability and row, and
+        the total weight."""
+        w, h, tot = C.c_uint32(), C.c_uint32(), C.c_float()
+        check(lib.vp_env_read_tables(self.handle, C.byref(w), C.byref(h), None, None, None, None, None, None))
+        W, H = w.value, h.value
+        t = {"cond_prob": np.empty((H, W), np.float32), "cond_alias": np.empty((H, W), np.uint32),
+             "marg_prob": np.empty(H, np.float32), "marg_alias": np.empty(H, np.uint32),
+             "joint": np.empty((H, W), np.float32)}
+        check(lib.vp_env_read_tables(self.handle, None, None, *(t[k].ctypes.data for k in
+                                     ("cond_prob", "cond_alias", "marg_prob", "marg_alias", "joint")), C.byref(tot)))
+        t["total"] = tot.value
+        return t
+
     def close(self):
         if getattr(self, "handle", None):
             if _alive(self.ctx):

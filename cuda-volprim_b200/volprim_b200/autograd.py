@@ -21,6 +21,10 @@ from .emission import render_emission, render_emission_backward
 
 
 class EmissionRender(torch.autograd.Function):
+    # Device times of the most recent forward (scene build, forward kernels) and backward (adjoint
+    # kernels) in milliseconds, from the library's CUDA events.
+    last_ms = {"scene_build": 0.0, "forward_kernels": 0.0, "backward_kernels": 0.0}
+
     @staticmethod
     def forward(ctx, mean, log_scale, quat_wxyz, density, emission, cameras, config, env, sigma_multiplier, vp_ctx):
         dev = mean.device
@@ -29,8 +33,13 @@ class EmissionRender(torch.autograd.Function):
         scene.set_emission(emission.detach())
         H, W = config.image_height, config.image_width
         imgs = torch.empty((len(cameras), H, W, 4), dtype=torch.float32, device=dev)
+        fwd_ms = 0.0
         for k, cam in enumerate(cameras):
-            render_emission(scene, env, cam, config, out=imgs[k])
+            st = {}
+            render_emission(scene, env, cam, config, out=imgs[k], stats=st)
+            fwd_ms += st.get("ms_kernels", 0.0)
+        EmissionRender.last_ms = {"scene_build": scene.info()["build_ms"], "forward_kernels": fwd_ms,
+                                  "backward_kernels": 0.0}
         ctx.scene, ctx.cameras, ctx.config, ctx.env = scene, list(cameras), config, env
         ctx.shapes = (mean.shape, log_scale.shape, quat_wxyz.shape, density.shape, emission.shape)
         return imgs[..., :3].clone()
@@ -46,9 +55,11 @@ class EmissionRender(torch.autograd.Function):
                  "emission": torch.zeros(3 * n, dtype=torch.float32, device=dev)}
         H, W = ctx.config.image_height, ctx.config.image_width
         dl = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+        bwd_ms = 0.0
         for k, cam in enumerate(ctx.cameras):
             dl[..., :3] = grad_images[k]
-            render_emission_backward(ctx.scene, ctx.env, cam, ctx.config, dl, grads)
+            bwd_ms += render_emission_backward(ctx.scene, ctx.env, cam, ctx.config, dl, grads).get("ms_kernels", 0.0)
+        EmissionRender.last_ms["backward_kernels"] = bwd_ms
         ctx.scene.close()
         out = [grads["mean"].view(ctx.shapes[0]), grads["scale"].view(ctx.shapes[1]),
                grads["quat_wxyz"].view(ctx.shapes[2]), grads["density"].view(ctx.shapes[3]),

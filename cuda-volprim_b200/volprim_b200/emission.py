@@ -17,8 +17,9 @@ from ._capi import check, lib
 from .api import Camera, Config, Environment, Scene, _is_cuda_tensor, _sync_torch
 
 
-def render_emission(scene: Scene, env: Environment, camera: Camera, config: Config, out=None):
-    """(H, W, 4) float32 image; into `out` (a CUDA tensor) when given, else a new host array."""
+def render_emission(scene: Scene, env: Environment, camera: Camera, config: Config, out=None, stats: dict | None = None):
+    """(H, W, 4) float32 image; into `out` (a CUDA tensor) when given, else a new host array.
+    `stats`, when given, receives the call's vp_render_stats."""
     p, cam = config.to_c(), camera.to_c()
     st = _capi.vp_render_stats()
     if out is not None and _is_cuda_tensor(out):
@@ -27,10 +28,14 @@ def render_emission(scene: Scene, env: Environment, camera: Camera, config: Conf
         _sync_torch(out)
         check(lib.vp_render_emission(scene.handle, env.handle, C.byref(cam), C.byref(p), out.data_ptr(),
                                      _capi.VP_MEMORY_DEVICE, C.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
         return out
     img = np.empty((config.image_height, config.image_width, 4), dtype=np.float32)
     check(lib.vp_render_emission(scene.handle, env.handle, C.byref(cam), C.byref(p), img.ctypes.data,
                                  _capi.VP_MEMORY_HOST, C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
     return img
 
 

@@ -66,11 +66,16 @@ typedef enum vp_engine {
 } vp_engine;
 
 /* Precision of the per-(ray, Gaussian) chord set-up (whitening transform, closest approach,
- * 3-sigma chord).  The erf/erfinv/exp evaluations are FP32 in both. */
+ * 3-sigma chord) and of the optical-depth sums.  Both are FP32 arithmetic; no precision uses
+ * FP64 (the only FP64 on the device is the environment table build).  Both meet the 1e-5
+ * relative per-pixel transmittance gate against the FP64 closed form on rays from outside the
+ * Gaussians (FAST: 6e-6 worst on the 256-Gaussian absorption image, ACCURATE: 3e-6). */
 typedef enum vp_precision {
   VP_PRECISION_AUTO = 0,    /* ACCURATE for absorption-only scenes (albedo == 0), else FAST */
-  VP_PRECISION_FAST = 1,    /* FP32 throughout */
-  VP_PRECISION_ACCURATE = 2 /* FP64 chord set-up; meets 1e-5 relative transmittance */
+  VP_PRECISION_FAST = 1,    /* FP32, hardware exp/log approximations (the reference's fast math) */
+  VP_PRECISION_ACCURATE = 2 /* FP32 with error-free transforms: o - c, the closest approach and d2
+                               as float pairs (TwoSum / FMA TwoProduct), correctly rounded exp,
+                               compensated optical-depth sums */
 } vp_precision;
 
 /* Bits of vp_render_params.measure. */
@@ -206,6 +211,16 @@ vp_status vp_env_create(vp_context* ctx, const float* rgb, uint32_t width, uint3
 vp_status vp_env_create_constant(vp_context* ctx, float r, float g, float b, vp_env** out);
 /* Device time of the last env build in milliseconds. */
 vp_status vp_env_build_ms(vp_env* env, double* out_ms);
+/* Copies the sampling tables the device built back to host arrays, for checking them against
+ * the reference's distribution (EnvironmentMap::buildCdf,
+ * include/thesis/host/params/environment_map.h:45-101).  out_width / out_height receive the map
+ * size; the arrays may be NULL to query it.  Per texel (width*height, row-major, row = polar
+ * angle): the alias probability and alias texel within its row, and the joint weight
+ * luminance x sin(theta); per row (height): the marginal alias probability and alias row.
+ * out_total: the sum of the joint weights (0 selects the uniform-sphere fallback). */
+vp_status vp_env_read_tables(vp_env* env, uint32_t* out_width, uint32_t* out_height,
+                             float* cond_prob, uint32_t* cond_alias, float* marg_prob,
+                             uint32_t* marg_alias, float* joint, float* out_total);
 vp_status vp_env_destroy(vp_env* env);
 
 /* ---------------------------------------------------------------------------------------- */
@@ -286,6 +301,12 @@ typedef struct vp_render_stats {
   uint32_t reserved;
   uint64_t paths_skipped;      /* paths not traced because their pixel had converged (adaptive
                                   sampling); paths counts only the traced ones (always counted) */
+  uint64_t hits_hist[2][16];   /* queries by the number of Gaussian chords they evaluated, in
+                                  power-of-two bins: bin 0 = none, bin k = [2^(k-1), 2^k) for
+                                  k = 1..14, bin 15 = 2^14 or more; [0] free-flight argmin
+                                  queries, [1] transmittance queries.  The distribution behind
+                                  max_hits_per_ray (the reference's --measure-caps hit-buffer
+                                  demand; warp and wavefront engines)         (measure != 0) */
 } vp_render_stats;
 
 /* ---------------------------------------------------------------------------------------- */

@@ -67,6 +67,9 @@ def lib() -> C.CDLL:
         L.or_render.restype = C.c_double
         L.or_render.argtypes = [C.c_void_p, C.c_void_p, F, U, F, C.c_uint32, C.c_uint32, C.c_uint32,
                                 C.c_uint32, C.c_int, F]
+        L.or_render_pixels.restype = C.c_double
+        L.or_render_pixels.argtypes = [C.c_void_p, C.c_void_p, F, U, F, U, U, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_int, F, D]
         L.or_render_welford.restype = C.c_double
         L.or_render_welford.argtypes = [C.c_void_p, C.c_void_p, F, U, F, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_float, C.c_uint32, C.c_int, F, F, U]
@@ -291,6 +294,22 @@ def render(scene: OracleScene, env: OracleEnv, cam16, config, y0=0, y1=None, s0=
     out = np.empty((y1 - y0) * W * 3, np.float32)
     secs = lib().or_render(scene.h, env.h, _p(_f(cam16)), _p(pu, U), _p(pf), y0, y1, s0, s1, int(threads), _p(out))
     return out.reshape(y1 - y0, W, 3), secs
+
+
+def render_pixels(scene: OracleScene, env: OracleEnv, cam16, config, px, py, s0=0, s1=1, rng_mode="sequential",
+                  threads=0):
+    """FP32 restatement of the path tracer over a list of pixels, samples [s0, s1) each.
+
+    Returns (per-pixel means (n, 3) float32, elapsed seconds, threads' trace seconds, threads'
+    seconds in the bounce-0 origin-inside scan)."""
+    px = np.ascontiguousarray(px, np.uint32)
+    py = np.ascontiguousarray(py, np.uint32)
+    pu, pf = _render_params(config, rng_mode)
+    out = np.empty(px.size * 3, np.float32)
+    times = np.zeros(2, np.float64)
+    secs = lib().or_render_pixels(scene.h, env.h, _p(_f(cam16)), _p(pu, U), _p(pf), _p(px, U), _p(py, U), px.size,
+                                  s0, s1, int(threads), _p(out), _p(times, D))
+    return out.reshape(-1, 3), secs, float(times[0]), float(times[1])
 
 
 def morton3d(pos, scene_min, inv_extent) -> int:

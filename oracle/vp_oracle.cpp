@@ -743,6 +743,8 @@ struct Tracer {
   const Camera& C;
   const Params& P;
   std::vector<uint32_t> cand;
+  double scan_s = 0.0;  // thread time in the bounce-0 origin-inside scan (timed renders only)
+  bool time_scan = false;
 
   void candidates_ray(F3 o, F3 d) {
     cand.clear();
@@ -816,9 +818,11 @@ struct Tracer {
     const bool alias = P.rng_mode == 1;
     for (uint32_t bounce = 0; bounce < P.max_bounces; ++bounce) {
       if (bounce == 0) {  // build_origin_inside_set (:322-341)
+        const double ts = time_scan ? omp_get_wtime() : 0.0;
         active.clear();
         for (uint32_t i = 0; i < S.prims.size(); ++i)
           if (point_inside(o, S.prims[i])) active.push_back(i);
+        if (time_scan) scan_s += omp_get_wtime() - ts;
       }
       origin_inside = active;
       hits.clear();  // collect_hits (:287-305), canonical order = ascending entry distance
@@ -1324,6 +1328,52 @@ double or_render(void* sv, void* ev, const float* cam16, const uint32_t* pu, con
     }
   }
   return omp_get_wtime() - t0;
+}
+
+// The same path tracer over a list of n pixels (px[i], py[i]), samples [s0, s1) each: the CPU
+// baseline's bounded sample of a workload.  out_rgb: n*3 per-pixel means.  out_times[0] = the
+// threads' total time in trace(), out_times[1] = their time in the bounce-0 origin-inside scan
+// (build_origin_inside_set, sampling.cuh:322-341: every Gaussian, every camera path).  Returns
+// elapsed seconds.
+double or_render_pixels(void* sv, void* ev, const float* cam16, const uint32_t* pu, const float* pf,
+                        const uint32_t* px, const uint32_t* py, uint32_t n, uint32_t s0, uint32_t s1, int n_threads,
+                        float* out_rgb, double* out_times) {
+  const Scene& S = *static_cast<Scene*>(sv);
+  const Env& E = *static_cast<Env*>(ev);
+  Camera c{mk(cam16[0], cam16[1], cam16[2]), mk(cam16[3], cam16[4], cam16[5]), mk(cam16[6], cam16[7], cam16[8]),
+           mk(cam16[9], cam16[10], cam16[11]), mk(cam16[12], cam16[13], cam16[14]), static_cast<int>(cam16[15])};
+  Params P{};
+  P.width = pu[0], P.height = pu[1], P.spp = pu[2], P.seed = pu[3], P.max_bounces = pu[4], P.rr_depth = pu[5];
+  P.nee_mode = static_cast<int32_t>(pu[6]), P.ris_k = pu[7], P.rng_mode = static_cast<int32_t>(pu[8]);
+  P.rr_max_survival = pf[0], P.hg_g = pf[1], P.firefly_clamp = pf[2], P.filter_stddev = pf[3];
+  fold_hg(P);
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  double trace_total = 0.0, scan_total = 0.0;
+  const double t0 = omp_get_wtime();
+#pragma omp parallel reduction(+ : trace_total, scan_total)
+  {
+    Tracer t{S, E, c, P, {}};
+    t.time_scan = true;
+    const double tt = omp_get_wtime();
+#pragma omp for schedule(dynamic, 4)
+    for (int64_t k = 0; k < static_cast<int64_t>(n); ++k) {
+      double acc[3] = {0, 0, 0};
+      for (uint32_t s = s0; s < s1; ++s) {
+        const F3 L = t.trace(px[k], py[k], s);
+        acc[0] += L.x, acc[1] += L.y, acc[2] += L.z;
+      }
+      const double inv = 1.0 / static_cast<double>(s1 - s0);
+      for (int j = 0; j < 3; ++j) out_rgb[3 * k + j] = static_cast<float>(acc[j] * inv);
+    }
+    trace_total += omp_get_wtime() - tt;
+    scan_total += t.scan_s;
+  }
+  const double el = omp_get_wtime() - t0;
+  if (out_times) {
+    out_times[0] = trace_total;
+    out_times[1] = scan_total;
+  }
+  return el;
 }
 
 // Adaptive-sampling test of one pixel (raygen.cuh:52-67, constants.cuh:202-211): with at least

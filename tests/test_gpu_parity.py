@@ -1,9 +1,13 @@
 """GPU parity of the CUDA path (through the C ABI) against the oracle.
 
 Tolerances:
-  * transmittance / absorption images vs the FP64 closed form (ACCURATE set-up):
+  * transmittance / absorption images vs the FP64 closed form, both precisions (all FP32
+    arithmetic: FAST, and ACCURATE with float-pair set-up and sums):
       |T - T64| <= 1e-5 * T64 where T64 >= 1e-4, else |T - T64| <= 1e-9   (the stated gate)
-  * FAST (FP32 set-up) transmittance: |T - T64| <= 2e-4 * T64 + 1e-8
+  * rays starting inside the cloud: |T - T64| <= 2e-5 * T64 + 1e-8.  A chord that only grazes a
+    Gaussian's 3-sigma surface (h = sqrt(9 - d2) -> 0) is ill-conditioned in the record itself:
+    at d2 = 8.9989 the FP32 rounding of the stored whitening matrix moves that chord's tau by
+    3e-4 relative, whatever the arithmetic (an FP64 set-up gave the same 1.4e-5 on that ray).
   * scattering vs the oracle with the same keyed free-flight draws: per-pixel relative difference
     below 1e-3 on >= 97% of pixels and mean relative difference below 2e-4
   * scattering vs the oracle with the reference's sequential draws: seed-stack z-scores with
@@ -52,11 +56,12 @@ def scene256(vp_ctx):
     return vp.Scene(vp_ctx, g), O.OracleScene.from_gaussians(g), g
 
 
+@pytest.mark.parametrize("precision", [VP_PRECISION_ACCURATE, VP_PRECISION_FAST])
 @pytest.mark.parametrize("engine", [VP_ENGINE_WARP, VP_ENGINE_MEGAKERNEL])
-def test_transmittance_accurate_vs_fp64(scene256, engine):
+def test_transmittance_vs_fp64(scene256, engine, precision):
     sc, osc, _ = scene256
     o, d = random_rays(np.random.default_rng(1), 20000)
-    T = sc.transmittance(o, d, precision=VP_PRECISION_ACCURATE, engine=engine)
+    T = sc.transmittance(o, d, precision=precision, engine=engine)
     T64, _ = osc.transmittance_fp64(o, d)
     ok, err = gate_T(T, T64)
     assert (T64 < 0.999).sum() > 2000, "rays must actually cross Gaussians"
@@ -68,7 +73,7 @@ def test_transmittance_inside_origins(scene256, engine):
     sc, osc, _ = scene256
     o, d = random_rays(np.random.default_rng(2), 20000, inside_frac=1.0)
     T64, _ = osc.transmittance_fp64(o, d)
-    for prec, tol in ((VP_PRECISION_ACCURATE, 2e-5), (VP_PRECISION_FAST, 2e-4)):
+    for prec, tol in ((VP_PRECISION_ACCURATE, 2e-5), (VP_PRECISION_FAST, 2e-5)):
         T = sc.transmittance(o, d, precision=prec, engine=engine).astype(np.float64)
         err = np.abs(T - T64)
         assert np.all(err <= tol * T64 + 1e-8), (prec, np.max(err / np.maximum(T64, 1e-30)))
@@ -79,7 +84,8 @@ def test_fast_transmittance_vs_fp64(scene256):
     o, d = random_rays(np.random.default_rng(3), 20000)
     T = sc.transmittance(o, d, precision=VP_PRECISION_FAST).astype(np.float64)
     T64, _ = osc.transmittance_fp64(o, d)
-    assert np.all(np.abs(T - T64) <= 2e-4 * T64 + 1e-8)
+    ok, err = gate_T(T, T64)
+    assert ok.all(), f"{(~ok).sum()} rays fail; worst rel {np.max(err / np.maximum(T64, 1e-30)):.3e}"
 
 
 def test_transmittance_waits_for_torch_stream(scene256):
@@ -116,12 +122,15 @@ def test_single_gaussian_closed_form(vp_ctx):
             np.testing.assert_allclose(-np.log(T), tau, rtol=2e-6, atol=2e-7)
 
 
+@pytest.mark.parametrize("precision", ["auto", "fast"])
 @pytest.mark.parametrize("engine", ["warp", "megakernel", "wavefront"])
-def test_absorption_image_matches_fp64(vp_ctx, engine):
+def test_absorption_image_matches_fp64(vp_ctx, engine, precision):
     """128x128x16 absorption render of the 256-Gaussian workload vs the FP64 oracle, replaying
-    the reference's PCG32 jitter stream per (pixel, sample)."""
+    the reference's PCG32 jitter stream per (pixel, sample).  "auto" is the ACCURATE float-pair
+    set-up for this albedo-0 scene; both are FP32 arithmetic."""
     w = scenes.absorption_256()
     w.config.engine = engine
+    w.config.precision = precision
     r = vp.Renderer(w.config, w.gaussians, w.camera, env=None, ctx=vp_ctx)
     img = r.render()[..., :3].astype(np.float64)
     osc = O.OracleScene.from_gaussians(w.gaussians, use_bvh=True)
