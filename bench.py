@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-baseline-engine", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the differentiation and serving forms")
-    ap.add_argument("--serving-requests", type=int, default=128)
+    ap.add_argument("--serving-requests", type=int, default=1000)
     ap.add_argument("--rmse-sweep", action="store_true",
                     help="instead of the timed run: RMSE against a high-spp render versus device time, for the "
                          "wavefront and the plain megakernel, and the speed-up at matched RMSE")
@@ -674,51 +674,39 @@ def other_configs(device):
     return out
 
 
+SERVING_P99_TARGET_S = 3.0  # stated p99 latency target at 80% of offline throughput
+
+
 def serving_form(device, n_requests):
-    """The serving workload on its 4 resident scenes (50k / 100k / 250k / 500k Gaussians, seeds 1-4):
-    the first n_requests of the seeded request stream, (1) all at t = 0 (offline throughput),
-    (2) with Poisson arrivals at 80% of that throughput (p50 / p99 latency, served Mpaths/s) and
-    (3) the same arrivals through one vp_render per request (the plain per-request launch)."""
+    """The serving workload (volprim_b200.serving.serving_study) on its 4 resident scenes
+    (50k / 100k / 250k / 500k Gaussians, seeds 1-4): offline capacity (one vp_render per request,
+    back to back) and served capacity on the first 300 requests of the seeded stream at t = 0;
+    then `n_requests` with Poisson arrivals at 80% of the offline capacity, served (SRPT) and
+    through the plain per-request loop on the same arrivals (p50 / p99 latency)."""
     import volprim_b200 as vp
-    from volprim_b200 import scenes
-    from volprim_b200.serving import Server, make_trace, run_trace, run_trace_plain
+    from volprim_b200.serving import serving_study
 
     ctx = vp.Context(device)
-    gs, sigma, env_img = scenes.serving_scenes()
-    scs = [vp.Scene(ctx, g, sigma) for g in gs]
-    env = vp.Environment(ctx, rgb=env_img)
-    envs = [env] * len(scs)
-
-    def server():
-        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9)
-        for sc in scs:
-            s.add_scene(sc, env)
-        return s
-
-    burst = make_trace(2024, n_requests, rate=0.0, n_scenes=len(scs))
-    srv = server()
-    off = run_trace(srv, burst)
-    srv.close()
-    mean_paths = off["paths"] / n_requests
-    rate = 0.8 * off["mpaths_per_s"] * 1e6 / mean_paths
-    trace = make_trace(2024, n_requests, rate=rate, n_scenes=len(scs))
-    srv = server()
-    served = run_trace(srv, trace)
-    srv.close()
-    plain = run_trace_plain(scs, envs, trace)
-    for s in scs:
-        s.close()
-    env.close()
+    res = serving_study(ctx, n_requests=n_requests, capacity_requests=min(300, n_requests), load=0.8,
+                        schedules=("srpt",))
     ctx.close()
-    return {"metric": "p50/p99 request latency", "unit": "s", "p50_s": served["p50_s"], "p99_s": served["p99_s"],
-            "mpaths_per_s": served["mpaths_per_s"], "offline_mpaths_per_s": off["mpaths_per_s"],
-            "fraction_of_offline": served["mpaths_per_s"] / off["mpaths_per_s"],
-            "arrival_rate_per_s": rate, "requests": n_requests, "paths": served["paths"],
-            "plain_per_request": {"p50_s": plain["p50_s"], "p99_s": plain["p99_s"],
-                                  "mpaths_per_s": plain["mpaths_per_s"]},
+    served, plain, cap = res["served"]["srpt"], res["plain"], res["served_capacity"]["srpt"]
+    return {"metric": "p50/p99 request latency", "unit": "s", "p50_s": served["p50_s"], "p90_s": served["p90_s"],
+            "p99_s": served["p99_s"], "max_s": served["max_s"], "p99_target_s": SERVING_P99_TARGET_S,
+            "meets_p99_target": served["p99_s"] <= SERVING_P99_TARGET_S,
+            "mpaths_per_s": served["mpaths_per_s"],
+            "offline_mpaths_per_s": res["offline_mpaths_per_s"],
+            "served_capacity_mpaths_per_s": cap["mpaths_per_s"],
+            "capacity_fraction_of_offline": cap["fraction_of_offline"],
+            "served_device_busy_at_capacity": cap["device_busy"],
+            "arrival_rate_per_s": res["arrival_rate_per_s"], "load_of_offline": res["load"],
+            "requests": n_requests, "capacity_requests": res["capacity_requests"],
+            "mean_paths_per_request": res["mean_paths_per_request"],
+            "plain_per_request": {k: plain[k] for k in ("p50_s", "p90_s", "p99_s", "max_s", "mpaths_per_s")},
             "workload": "4 resident scenes (50k/100k/250k/500k Gaussians), requests: resolution in "
                         "{64,128,256,512}^2, spp in {1,4,16,64}, random camera at distance 3.5; Poisson arrivals at "
-                        "80% of the offline throughput; 150 GB budget"}
+                        "80% of the offline capacity (plain per-request loop at t = 0); 150 GB budget; SRPT "
+                        "schedule (half the free slots kept for the oldest request), 2^18 path slots"}
 
 
 def rmse_sweep(args):

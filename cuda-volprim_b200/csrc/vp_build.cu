@@ -9,8 +9,6 @@
 // include/thesis/host/optix/acceleration_structure.h:23-87) and the Primitive precompute
 // (include/thesis/device/params/primitive.h:70-87) plus PLY-load validation
 // (src/thesis/host/utils/io/ply.cpp:124-172).
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -938,28 +936,25 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
                                                ": NaN/Inf in centre or rotation");
 
   // Morton codes + radix sort (stable: ties keep the caller's order).
-  Scratch<uint64_t> codes(st), codes_sorted(st);
-  Scratch<uint32_t> idx(st), morton(st), pos(st);
-  Scratch<unsigned char> cub_tmp(st);
+  Scratch<uint64_t> codes(st);
+  Scratch<uint32_t> idx(st), pos(st);
+  Scratch<unsigned char> sort_tmp(st);
   if ((s = dev_alloc(&codes.p, n, st))) return s;
-  if ((s = dev_alloc(&codes_sorted.p, n, st))) return s;
   if ((s = dev_alloc(&idx.p, n, st))) return s;
-  if ((s = dev_alloc(&morton.p, n, st))) return s;
   if ((s = dev_alloc(&pos.p, n, st))) return s;
   k_morton<<<nb, TB, 0, st>>>(n, mean, bounds.p, codes.p, idx.p);
   VP_CUDA(cudaGetLastError());
-  size_t sort_bytes = 0, scan_bytes = 0;
-  VP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, codes.p, codes_sorted.p, idx.p, morton.p,
-                                          (int)n, 0, 63, st));
-  VP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long*)nullptr,
-                                        (unsigned long long*)nullptr, (int)n, st));
-  const size_t tmp_bytes = std::max(sort_bytes, scan_bytes);
-  if ((s = dev_alloc(&cub_tmp.p, tmp_bytes, st))) return s;
-  VP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, sort_bytes, codes.p, codes_sorted.p, idx.p, morton.p,
-                                          (int)n, 0, 63, st));
+  // Stable radix sort of the 63-bit codes (ties keep the caller's order), in place: codes become
+  // the sorted codes and idx the Morton order.  The same scratch serves the clustering's scans.
+  const size_t scan_bytes = exclusive_scan_tmp_bytes(n);
+  const size_t tmp_bytes = std::max(radix_sort_tmp_bytes_u64(n), scan_bytes);
+  if ((s = dev_alloc(&sort_tmp.p, tmp_bytes, st))) return s;
+  if ((s = radix_sort_pairs(codes.p, idx.p, n, 63, sort_tmp.p, tmp_bytes, st))) return s;
+  const uint64_t* codes_sorted = codes.p;
+  const uint32_t* morton = idx.p;
   if ((s = dev_alloc(&plo.p, n, st))) return s;
   if ((s = dev_alloc(&phi.p, n, st))) return s;
-  k_gather_boxes<<<nb, TB, 0, st>>>(n, morton.p, lo0.p, hi0.p, plo.p, phi.p);
+  k_gather_boxes<<<nb, TB, 0, st>>>(n, morton, lo0.p, hi0.p, plo.p, phi.p);
   VP_CUDA(cudaGetLastError());
 
   // PLOC clustering: the binary tree of the BVH32 and of the megakernel unless the options ask for
@@ -1007,8 +1002,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
         VP_CUDA(cudaGetLastError());
         k_ploc_flags<<<(m + TB - 1) / TB, TB, 0, st>>>(m, cin, nn.p, fl.p);
         VP_CUDA(cudaGetLastError());
-        size_t sb = scan_bytes;
-        VP_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp.p, sb, fl.p, sc_x.p, (int)m, st));
+        if ((s = exclusive_scan(fl.p, sc_x.p, m, sort_tmp.p, scan_bytes, st))) return s;
         k_ploc_write<<<(m + TB - 1) / TB, TB, 0, st>>>(cin, cout, nn.p, fl.p, sc_x.p, ca.p, cb.p, oa.p, ob.p,
                                                        pleft.p, pright.p, pnlo.p, pnhi.p);
         VP_CUDA(cudaGetLastError());
@@ -1054,7 +1048,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
     if ((s = dev_alloc(&flags.p, ni, st))) return s;
     if (n > 1) {
       VP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned int) * ni, st));
-      k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted.p, left.p, right.p, first.p, last.p,
+      k_karras<<<(ni + TB - 1) / TB, TB, 0, st>>>((int)n, codes_sorted, left.p, right.p, first.p, last.p,
                                                   par_i.p, par_l.p);
       VP_CUDA(cudaGetLastError());
       k_refit<<<nb, TB, 0, st>>>((int)n, left.p, right.p, par_i.p, par_l.p, plo.p, phi.p, nlo.p, nhi.p, flags.p);
@@ -1173,7 +1167,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   uint32_t* perm = nullptr;
   if ((s = dev_alloc(&perm, n, st))) return s;
   sc->perm = perm;
-  k_compose<<<nb, TB, 0, st>>>(n, morton.p, pos.p, perm);
+  k_compose<<<nb, TB, 0, st>>>(n, morton, pos.p, perm);
   VP_CUDA(cudaGetLastError());
   float4* prims = nullptr;
   if ((s = dev_alloc(&prims, 4ull * n, st))) return s;

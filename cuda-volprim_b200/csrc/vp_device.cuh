@@ -413,6 +413,7 @@ __device__ __forceinline__ float chord_u0(const Chord& ch, float t_lo) {
 // near erf -> 1).
 __device__ __forceinline__ float erf_diff(float a, float b) {
   if (a >= 0.0f) return erfcf(a * kInvSqrt2) - erfcf(b * kInvSqrt2);
+  if (a == -b) return 2.0f * erff(b * kInvSqrt2);  // the whole chord, entered from outside (erf is odd)
   return erff(b * kInvSqrt2) - erff(a * kInvSqrt2);
 }
 

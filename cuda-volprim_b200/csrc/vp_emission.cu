@@ -13,6 +13,8 @@
 // single Gaussian, for disjoint chords of equal colour, and in the optically thin limit, where
 // L -> sum_i tau_i e_i).  It depends on the Gaussians only through the order-independent sums S
 // and C, so a ray's Gaussians are visited in any order and no hit list is sorted or stored.
+// Limitation: no occlusion between Gaussians -- a Gaussian behind an opaque one still colours the
+// pixel with its tau-weighted share; only the background term is attenuated.
 //
 // Adjoint.  For one ray with upstream gradient G = dLoss/dL (RGB):
 //     dL/dS = C (T - a) / S - T env,  a = (1 - T) / S,      dL/dC = a
@@ -44,7 +46,7 @@ template <bool kAcc, class F>
 __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3 d, uint32_t& status, F&& f) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
-  const float3 inv = safe_inv(d);
+  const RayBox rb = ray_box(o, d);
   int sp = 0;
   uint32_t ref = S.wide_root;
   bool have = true;
@@ -71,7 +73,7 @@ __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3
       __syncwarp();
       if (lane < total) {
         float tb;
-        if (slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, kInf, tb)) {
+        if (slab(rb, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, kInf, tb)) {
           const PrimGeo g = load_geo(S.prims, pi);
           Chord ch;
           if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f) f(pi, g, ch);
@@ -83,7 +85,7 @@ __device__ void warp_visit(const SceneView& S, uint32_t* stack, float3 o, float3
       const float4 hi = __ldg(node + 32 + lane);
       const uint32_t cref = __float_as_uint(lo.w);
       float tnear = 0.f;
-      const bool hit = (cref != kEmptyRef) && slab(o, inv, lo, hi, 0.0f, kInf, tnear);
+      const bool hit = (cref != kEmptyRef) && slab(rb, lo, hi, 0.0f, kInf, tnear);
       const unsigned m = __ballot_sync(kFull, hit);
       const int nh = __popc(m);
       if (nh > 0) {

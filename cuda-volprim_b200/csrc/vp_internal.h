@@ -56,14 +56,14 @@ struct WfBuffers {
                                   // seed Gaussian's bits in .w), weight
   float4* L4;                     // finished sample radiance
   uint32_t *qa, *qb, *qs;         // path queues (current / next) and shadow-query queue
-  uint32_t *qt, *sk_a, *sk_b;     // sorting: a spare queue and the Morton keys of path origins
+  uint32_t* sk_a;                 // sorting: the Morton keys of path origins
   uint32_t* ctr;                  // [0] paths now, [1] paths next, [2] shadow queries, [3..4] work heads
 };
 struct WfWorkspace {
   size_t cap = 0;  // paths
   WfBuffers b{};
   void* base = nullptr;
-  void* sort_tmp = nullptr;  // CUB radix-sort scratch for `cap` keys
+  void* sort_tmp = nullptr;  // radix-sort scratch for `cap` keys (radix_sort_pairs)
   size_t sort_tmp_bytes = 0;
   uint32_t* host_count = nullptr;  // pinned, for polling the active-path count
 };
@@ -143,4 +143,20 @@ void free_wavefront(vp_context* ctx);
 vp_status launch_albedo(vp_scene* s, const float* pts, uint32_t n, bool accurate, int32_t engine, float* rgb,
                         uint32_t* cnt);
 vp_status launch_normalize(const float4* in, float4* out, size_t n, float scale, cudaStream_t st);
+
+// Device-wide sort and scan (vp_sort.cu).  radix_sort_pairs sorts (key, value) pairs in place by
+// the key bits [0, end_bit), stably; `tmp` holds radix_sort_tmp_bytes_*(n) bytes.  exclusive_scan
+// writes the exclusive prefix sums of n counts (in may equal out); `tmp` holds
+// exclusive_scan_tmp_bytes(n) bytes.  `launches`, when given, counts the kernels launched.
+size_t radix_sort_tmp_bytes_u64(size_t n);
+size_t radix_sort_tmp_bytes_u32(size_t n);
+size_t exclusive_scan_tmp_bytes(size_t n);
+vp_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int end_bit, void* tmp, size_t tmp_bytes,
+                           cudaStream_t st, uint32_t* launches = nullptr);
+vp_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int end_bit, void* tmp, size_t tmp_bytes,
+                           cudaStream_t st, uint32_t* launches = nullptr);
+vp_status exclusive_scan(const uint32_t* in, uint32_t* out, size_t n, void* tmp, size_t tmp_bytes, cudaStream_t st,
+                         uint32_t* launches = nullptr);
+vp_status exclusive_scan(const unsigned long long* in, unsigned long long* out, size_t n, void* tmp, size_t tmp_bytes,
+                         cudaStream_t st, uint32_t* launches = nullptr);
 }  // namespace vp

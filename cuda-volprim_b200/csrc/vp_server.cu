@@ -21,11 +21,16 @@
 // camera, params, pixel, sample).
 //
 // The host side admits from a FIFO when a table entry is free and the request's accumulator fits
-// the memory budget, replays the iterations as one captured CUDA graph (two iterations: the path
-// queues ping-pong), reads the per-request done counters, and completes requests whose paths have
-// all finished (mean = sum / spp into the caller's buffer).  Admission writes happen only while
-// the stream is idle (after the step's synchronisation), so the graph never sees a half-written
-// table entry.
+// the memory budget and replays the iterations as one captured CUDA graph (two iterations: the
+// path queues ping-pong).  The loop is pipelined so the GPU never waits for the host: a call
+// queues step k (graphs, then an asynchronous copy of the per-request done counters and the
+// status word to pinned memory) and only then waits for step k-1 and harvests it, while step k
+// runs.  Harvesting completes the requests whose paths have all finished: the mean (sum / spp) is
+// formed on the compute stream behind step k and, for host outputs, copied on a second stream
+// into pinned staging; the request is delivered (its id becomes visible to vp_server_poll) once
+// those copies have landed, by a later call.  Admission writes go to pinned staging and reach the
+// device table by stream-ordered copies, so every iteration sees whole table entries; an entry's
+// done counter is read only from steps queued after its admission.
 #include <algorithm>
 #include <cstring>
 #include <deque>
@@ -150,13 +155,14 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 //   VP_SCHEDULE_FIFO  in admission order, each request taking all it still has;
 //   VP_SCHEDULE_FAIR  an equal quota ceil(free / k) to each of the k requests (capped at what each
 //                     still has), then what is left over in table order;
-//   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order), with half of the
-//                     free slots kept for the oldest request that still has unstarted paths.
+//   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order), with a fraction
+//                     (srpt_reserve, default half) of the free slots kept for the oldest request
+//                     that still has unstarted paths.
 // Writes the per-entry offsets of this iteration's new paths (alloc_off, size R + 1) and their
 // first pixel-major path index (alloc_start).
 __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, unsigned long long* __restrict__ started,
                               uint32_t* __restrict__ alloc_off, unsigned long long* __restrict__ alloc_start,
-                              int schedule) {
+                              int schedule, float srpt_reserve) {
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t s_free, s_surv;
   __shared__ unsigned long long s_key[kMaxRequests], s_seq[kMaxRequests];
@@ -193,8 +199,8 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
     const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? rem64 : seq);
     s_key[e] = key;
     s_seq[e] = seq;
-    // SRPT: half of the free slots stay with the oldest request that has unstarted paths, so a
-    // large request keeps progressing while smaller ones overtake it
+    // SRPT: a fraction of the free slots stays with the oldest request that has unstarted paths,
+    // so a large request keeps progressing while smaller ones overtake it
     uint32_t reserve = 0, Fs = F;
     if (schedule == VP_SCHEDULE_SRPT) {
       if (e == 0) {
@@ -205,7 +211,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
       if (rem) atomicMin(&s_oldest, seq);
       __syncthreads();
       if (rem && seq == s_oldest) {
-        reserve = min(rem, F / 2u);
+        reserve = min(rem, (uint32_t)((float)F * srpt_reserve));
         s_reserve = reserve;
       }
       __syncthreads();
@@ -461,6 +467,15 @@ struct vp_server {
   int ext_blocks = 0, shd_blocks = 0, thr_blocks = 0;
   size_t smem_ext = 0, smem_shd = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // pipelining: two step slots, each with its own events and pinned copies of the done counters
+  // and status word
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_beg[2] = {}, ev_end[2] = {}, ev_step[2] = {};
+  unsigned long long* h_done_slot[2] = {};
+  unsigned int* h_status = nullptr;  // [2]
+  uint64_t slot_step[2] = {};
+  std::deque<int> inflight;  // step slots queued and not yet harvested (oldest first)
+  uint64_t step_no = 0;      // steps queued so far
   // host bookkeeping
   struct Active {
     bool used = false;
@@ -471,8 +486,27 @@ struct vp_server {
     int32_t memory = 0;
     float4* sum = nullptr;
     size_t bytes = 0;
+    uint64_t admit_step = 0;  // the first step queued after the admission
   };
   std::vector<Active> active;
+  // completed requests whose outputs are still being formed / copied
+  struct Delivery {
+    uint64_t id;
+    unsigned long long paths;
+    float* host_out;  // host output: copied from the pinned staging buffer at delivery
+    void* pinned;
+    size_t bytes, pinned_bytes;
+    size_t held;  // the request's share of the memory budget, released at delivery
+  };
+  struct OutBatch {
+    cudaEvent_t ev;
+    std::vector<Delivery> items;
+  };
+  std::deque<OutBatch> outs;
+  std::vector<cudaEvent_t> spare_events;
+  std::vector<std::pair<size_t, void*>> pinned_free;  // reusable pinned staging buffers
+  std::vector<void*> pinned_all;
+  uint32_t n_entries = 0;  // table entries in use (admitted, not harvested)
   struct Pending {
     uint64_t id;
     vp_request r;
@@ -498,6 +532,20 @@ void srv_free(vp_server* s) {
   cudaSetDevice(s->ctx->device);
   cudaStream_t st = s->ctx->stream;
   if (st) cudaStreamSynchronize(st);
+  if (s->copy_stream) {
+    cudaStreamSynchronize(s->copy_stream);
+    cudaStreamDestroy(s->copy_stream);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (s->ev_beg[k]) cudaEventDestroy(s->ev_beg[k]);
+    if (s->ev_end[k]) cudaEventDestroy(s->ev_end[k]);
+    if (s->ev_step[k]) cudaEventDestroy(s->ev_step[k]);
+  }
+  for (auto& b : s->outs) cudaEventDestroy(b.ev);
+  for (cudaEvent_t e : s->spare_events) cudaEventDestroy(e);
+  for (void* p : s->pinned_all) cudaFreeHost(p);
+  if (s->h_done_slot[0]) cudaFreeHost(s->h_done_slot[0]);
+  if (s->h_status) cudaFreeHost(s->h_status);
   if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
   if (s->graph) cudaGraphDestroy(s->graph);
   for (auto& a : s->active)
@@ -526,7 +574,7 @@ vp_status enqueue_iteration(vp_server* s, bool even) {
   uint32_t* qnext = even ? s->paths.qb : s->paths.qa;
   Counters* ctr = s->ctx->counters;
   k_srv_advance<<<1, R, 0, st>>>(s->d_ctl, s->d_table, s->d_started, s->d_alloc_off, s->d_alloc_start,
-                                 s->cfg.schedule);
+                                 s->cfg.schedule, s->cfg.srpt_reserve);
   k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_alloc_off, s->d_alloc_start, R, s->paths, qcur);
   if (s->accurate)
     k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
@@ -584,7 +632,7 @@ vp_status prepare_launch(vp_server* s) {
 
 vp_status admit(vp_server* s) {
   cudaStream_t st = s->ctx->stream;
-  while (!s->pending.empty() && s->n_active < s->cfg.max_requests) {
+  while (!s->pending.empty() && s->n_entries < s->cfg.max_requests) {
     const vp_request& rq = s->pending.front().r;
     const size_t need = request_bytes(rq);
     if (s->cfg.memory_budget_bytes && s->bytes_fixed + s->bytes_active + need > s->cfg.memory_budget_bytes) break;
@@ -618,23 +666,60 @@ vp_status admit(vp_server* s) {
     a.memory = rq.memory;
     a.sum = sum;
     a.bytes = need;
+    a.admit_step = s->step_no;
     s->bytes_active += need;
     s->n_active += 1;
+    s->n_entries += 1;
     s->admitted += 1;
     s->pending.pop_front();
   }
   return VP_OK;
 }
 
-vp_status complete(vp_server* s, uint32_t* n_done) {
-  cudaStream_t st = s->ctx->stream;
+void* pinned_acquire(vp_server* s, size_t bytes, size_t* got) {
+  size_t best = (size_t)-1;
+  for (size_t i = 0; i < s->pinned_free.size(); ++i)
+    if (s->pinned_free[i].first >= bytes && (best == (size_t)-1 || s->pinned_free[i].first < s->pinned_free[best].first))
+      best = i;
+  if (best != (size_t)-1) {
+    auto pr = s->pinned_free[best];
+    s->pinned_free.erase(s->pinned_free.begin() + best);
+    *got = pr.first;
+    return pr.second;
+  }
+  const size_t sz = std::max<size_t>((bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1), 1u << 20);
+  void* p = nullptr;
+  if (cudaMallocHost(&p, sz) != cudaSuccess) return nullptr;
+  s->pinned_all.push_back(p);
+  *got = sz;
+  return p;
+}
+
+// Completed requests of one harvested step: the mean is formed on the compute stream (behind the
+// step now running), host outputs are copied on the copy stream into pinned staging, and one event
+// on the copy stream marks the batch ready for delivery.
+vp_status harvest(vp_server* s, int slot) {
+  cudaStream_t st = s->ctx->stream, cs = s->copy_stream;
+  if (s->h_status[slot])
+    return fail(VP_ERROR_DEVICE_STATUS, "a serving kernel raised device status " + std::to_string(s->h_status[slot]));
+  float ms = 0.f;
+  VP_CUDA(cudaEventElapsedTime(&ms, s->ev_beg[slot], s->ev_end[slot]));
+  s->device_ms += ms;
   const uint32_t R = s->cfg.max_requests;
-  uint32_t nd = 0;
+  const unsigned long long* done = s->h_done_slot[slot];
+  vp_server::OutBatch batch{};
+  struct Copy {
+    float4* tmp;
+    void* pinned;
+    size_t bytes;
+  };
+  std::vector<Copy> copies;
   for (uint32_t e = 0; e < R; ++e) {
     vp_server::Active& a = s->active[e];
-    if (!a.used || s->h_done[e] < a.n_paths) continue;
+    if (!a.used || a.admit_step > s->slot_step[slot] || done[e] < a.n_paths) continue;
     const float inv = 1.0f / (float)a.spp;
     const unsigned nb = (a.n_pix + 255u) / 256u;
+    vp_server::Delivery d{a.id, a.n_paths, nullptr, nullptr, 16ull * a.n_pix, 0, a.bytes};
     if (a.memory == VP_MEMORY_DEVICE) {
       k_srv_finish<<<nb, 256, 0, st>>>(a.sum, a.n_pix, inv, reinterpret_cast<float4*>(a.out));
       VP_CUDA(cudaGetLastError());
@@ -643,20 +728,61 @@ vp_status complete(vp_server* s, uint32_t* n_done) {
       VP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp), 16ull * a.n_pix, st));
       k_srv_finish<<<nb, 256, 0, st>>>(a.sum, a.n_pix, inv, tmp);
       VP_CUDA(cudaGetLastError());
-      VP_CUDA(cudaMemcpyAsync(a.out, tmp, 16ull * a.n_pix, cudaMemcpyDeviceToHost, st));
-      VP_CUDA(cudaFreeAsync(tmp, st));
+      d.pinned = pinned_acquire(s, d.bytes, &d.pinned_bytes);
+      if (!d.pinned) return fail(VP_ERROR_OUT_OF_MEMORY, "pinned staging for a request's output");
+      d.host_out = a.out;
+      copies.push_back({tmp, d.pinned, d.bytes});
     }
     VP_CUDA(cudaFreeAsync(a.sum, st));
-    s->bytes_active -= a.bytes;
-    s->paths_completed += a.n_paths;
-    s->done_ids.push_back(a.id);
+    batch.items.push_back(d);
     a = vp_server::Active{};
-    s->n_active -= 1;
-    s->completed += 1;
-    ++nd;
+    s->n_entries -= 1;
   }
-  if (nd) VP_CUDA(cudaStreamSynchronize(st));
-  *n_done = nd;
+  if (batch.items.empty()) return VP_OK;
+  if (s->spare_events.empty()) {
+    cudaEvent_t ev;
+    VP_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    s->spare_events.push_back(ev);
+  }
+  batch.ev = s->spare_events.back();
+  s->spare_events.pop_back();
+  VP_CUDA(cudaEventRecord(batch.ev, st));  // the finish kernels
+  VP_CUDA(cudaStreamWaitEvent(cs, batch.ev, 0));
+  for (const Copy& c : copies) {
+    VP_CUDA(cudaMemcpyAsync(c.pinned, c.tmp, c.bytes, cudaMemcpyDeviceToHost, cs));
+    VP_CUDA(cudaFreeAsync(c.tmp, cs));
+  }
+  VP_CUDA(cudaEventRecord(batch.ev, cs));  // finish kernels and copies
+  s->outs.push_back(std::move(batch));
+  return VP_OK;
+}
+
+// Hands over the output batches whose copies have landed (all of them, waiting, when `wait`).
+vp_status deliver(vp_server* s, bool wait, uint32_t* n_done) {
+  while (!s->outs.empty()) {
+    vp_server::OutBatch& b = s->outs.front();
+    if (wait) {
+      VP_CUDA(cudaEventSynchronize(b.ev));
+    } else {
+      const cudaError_t q = cudaEventQuery(b.ev);
+      if (q == cudaErrorNotReady) break;
+      if (q != cudaSuccess) return cuda_fail(q, "vp_server output copy");
+    }
+    for (const vp_server::Delivery& d : b.items) {
+      if (d.host_out) {
+        std::memcpy(d.host_out, d.pinned, d.bytes);
+        s->pinned_free.push_back({d.pinned_bytes, d.pinned});
+      }
+      s->done_ids.push_back(d.id);
+      s->bytes_active -= d.held;  // its accumulator and output staging are released by now
+      s->paths_completed += d.paths;
+      s->completed += 1;
+      s->n_active -= 1;
+      *n_done += 1;
+    }
+    s->spare_events.push_back(b.ev);
+    s->outs.pop_front();
+  }
   return VP_OK;
 }
 
@@ -681,6 +807,11 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
     return fail(VP_ERROR_LIMIT, "max_requests above 1024");
   }
   if (c.iterations_per_step == 0) c.iterations_per_step = 4;
+  if (!(c.srpt_reserve > 0.0f)) c.srpt_reserve = 0.5f;
+  if (c.srpt_reserve > 1.0f) {
+    srv_free(s);
+    return fail(VP_ERROR_INVALID_ARGUMENT, "srpt_reserve above 1");
+  }
   c.iterations_per_step = (c.iterations_per_step + 1u) & ~1u;
   if (c.path_slots > (1u << 28)) {
     srv_free(s);
@@ -709,12 +840,21 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   chk(cudaMallocHost(&s->h_done, R * sizeof(unsigned long long)));
   chk(cudaEventCreate(&s->ev0));
   chk(cudaEventCreate(&s->ev1));
+  chk(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) {
+    chk(cudaEventCreate(&s->ev_beg[k]));
+    chk(cudaEventCreate(&s->ev_end[k]));
+    chk(cudaEventCreateWithFlags(&s->ev_step[k], cudaEventDisableTiming));
+  }
+  chk(cudaMallocHost(&s->h_done_slot[0], 2ull * R * sizeof(unsigned long long)));
+  chk(cudaMallocHost(&s->h_status, 2 * sizeof(unsigned int)));
   const size_t slot_bytes = (size_t)P * kSlotBytes + 32 * 256;
   chk(cudaMalloc(&s->path_mem, slot_bytes));
   if (e != cudaSuccess) {
     srv_free(s);
     return cuda_fail(e, "vp_server_create");
   }
+  s->h_done_slot[1] = s->h_done_slot[0] + R;
   char* cur = static_cast<char*>(s->path_mem);
   SrvPaths& b = s->paths;
   srv_carve(cur, b.o4, P);
@@ -742,6 +882,7 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, R * sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_started, 0, R * sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_table, 0, R * sizeof(SrvRequest), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, sizeof(Counters), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     srv_free(s);
@@ -798,33 +939,42 @@ vp_status vp_server_step(vp_server* s, uint32_t* completed) {
   if (s->scenes.empty()) return fail(VP_ERROR_INVALID_ARGUMENT, "no resident scene");
   VP_CUDA(cudaSetDevice(s->ctx->device));
   vp_status r;
-  if ((r = prepare_launch(s))) return r;
-  if ((r = admit(s))) return r;
-  if (s->n_active == 0) return VP_OK;
-  cudaStream_t st = s->ctx->stream;
-  VP_CUDA(cudaMemsetAsync(s->ctx->counters, 0, sizeof(Counters), st));
-  VP_CUDA(cudaEventRecord(s->ev0, st));
-  for (uint32_t k = 0; k < s->cfg.iterations_per_step; k += 2) {
-    if (s->graph_exec) {
-      VP_CUDA(cudaGraphLaunch(s->graph_exec, st));
-    } else {
-      if ((r = enqueue_iteration(s, true))) return r;
-      if ((r = enqueue_iteration(s, false))) return r;
-    }
-  }
-  VP_CUDA(cudaEventRecord(s->ev1, st));
-  VP_CUDA(cudaMemcpyAsync(s->h_done, s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
-                          cudaMemcpyDeviceToHost, st));
-  VP_CUDA(cudaStreamSynchronize(st));
-  float ms = 0.f;
-  VP_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
-  s->device_ms += ms;
-  s->iterations += s->cfg.iterations_per_step;
-  Counters c{};
-  VP_CUDA(cudaMemcpy(&c, s->ctx->counters, sizeof(c), cudaMemcpyDeviceToHost));
-  if (c.status) return fail(VP_ERROR_DEVICE_STATUS, "a serving kernel raised device status " + std::to_string(c.status));
   uint32_t nd = 0;
-  if ((r = complete(s, &nd))) return r;
+  if ((r = prepare_launch(s))) return r;
+  if ((r = deliver(s, false, &nd))) return r;
+  if ((r = admit(s))) return r;
+  cudaStream_t st = s->ctx->stream;
+  const bool launch = s->n_entries > 0;
+  if (launch) {  // queue step k: its iterations, then the done counters and status to pinned memory
+    const int slot = s->inflight.empty() ? 0 : (s->inflight.back() ^ 1);
+    VP_CUDA(cudaEventRecord(s->ev_beg[slot], st));
+    for (uint32_t k = 0; k < s->cfg.iterations_per_step; k += 2) {
+      if (s->graph_exec) {
+        VP_CUDA(cudaGraphLaunch(s->graph_exec, st));
+      } else {
+        if ((r = enqueue_iteration(s, true))) return r;
+        if ((r = enqueue_iteration(s, false))) return r;
+      }
+    }
+    VP_CUDA(cudaEventRecord(s->ev_end[slot], st));
+    VP_CUDA(cudaMemcpyAsync(s->h_done_slot[slot], s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    VP_CUDA(cudaMemcpyAsync(s->h_status + slot, &s->ctx->counters->status, sizeof(unsigned int),
+                            cudaMemcpyDeviceToHost, st));
+    VP_CUDA(cudaEventRecord(s->ev_step[slot], st));
+    s->slot_step[slot] = s->step_no++;
+    s->iterations += s->cfg.iterations_per_step;
+    s->inflight.push_back(slot);
+  }
+  // harvest step k-1 while step k runs (every queued step when nothing new was queued)
+  while (s->inflight.size() > (launch ? 1u : 0u)) {
+    const int slot = s->inflight.front();
+    s->inflight.pop_front();
+    VP_CUDA(cudaEventSynchronize(s->ev_step[slot]));
+    if ((r = harvest(s, slot))) return r;
+  }
+  // with no step left on the GPU, wait for the outputs still being copied
+  if ((r = deliver(s, s->inflight.empty() && s->n_entries == 0, &nd))) return r;
   if (completed) *completed = nd;
   return VP_OK;
 }

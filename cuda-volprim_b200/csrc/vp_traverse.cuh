@@ -21,6 +21,17 @@ constexpr int kHitCap = VP_HIT_CAP;  // hit-buffer entries per warp (retained ch
 #define VP_LEAF_PACK 1
 #endif
 
+// Stack discipline of the argmin traversal (the free-flight minimum, and so every result, is the
+// same either way): 0 = the hit children are ranked by entry distance and stacked farther-deeper;
+// 1 (default) = they are stacked in lane order (the nearest continues, as in transmittance) and
+// each pop takes the nearest entry within the bound among the top 32 of the stack.  On the 500k
+// showcase 1 visits 13.0 instead of 14.3 inner nodes and 98 instead of 110 boxes per bounce, and
+// the extend stage takes 124 instead of 137 ms per 16-spp step (ranking costs a pass over the hit
+// children at every inner node; the windowed minimum costs one redux.sync per pop).
+#ifndef VP_ARGMIN_BEST_FIRST
+#define VP_ARGMIN_BEST_FIRST 1
+#endif
+
 // Resident 256-thread blocks per SM the warp engine's register budget is sized for.
 #ifndef VP_WARP_MIN_BLOCKS
 #define VP_WARP_MIN_BLOCKS 4
@@ -31,13 +42,49 @@ __device__ __forceinline__ float3 safe_inv(float3 d) {
   return f3(inv1(d.x), inv1(d.y), inv1(d.z));
 }
 
-__device__ __forceinline__ bool slab(float3 o, float3 inv, float4 lo, float4 hi, float t_lo,
-                                     float t_hi, float& tnear) {
-  const float tx0 = (lo.x - o.x) * inv.x, tx1 = (hi.x - o.x) * inv.x;
-  const float ty0 = (lo.y - o.y) * inv.y, ty1 = (hi.y - o.y) * inv.y;
-  const float tz0 = (lo.z - o.z) * inv.z, tz1 = (hi.z - o.z) * inv.z;
-  const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), t_lo));
-  const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), t_hi));
+// Per-ray constants of the slab test.  With kFma each plane distance is one FMA,
+// t = b (1/d) - o (1/d); against (b - o)(1/d) this moves a plane by a few ulps of o (as the
+// subtraction's own rounding does), and the 3-sigma boxes are padded far beyond that.  It holds
+// three more registers through the traversal: the argmin kernels (64 registers) take it, the
+// transmittance kernel (48 registers, five blocks per SM) keeps the subtraction form, which
+// measured faster there (the extra registers raised its spills from 52 to 84 B).
+struct RayBox {
+  float3 o, inv, oinv;
+};
+__device__ __forceinline__ RayBox ray_box(float3 o, float3 d) {
+  RayBox r;
+  r.o = o;
+  r.inv = safe_inv(d);
+  r.oinv = f3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+  return r;
+}
+
+// Three-operand minimum / maximum (PTX ISA 8.8, sm_100a).
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
+template <bool kFma = true>
+__device__ __forceinline__ bool slab(const RayBox& r, float4 lo, float4 hi, float t_lo, float t_hi, float& tnear) {
+  float tx0, tx1, ty0, ty1, tz0, tz1;
+  if constexpr (kFma) {
+    tx0 = fmaf(lo.x, r.inv.x, -r.oinv.x), tx1 = fmaf(hi.x, r.inv.x, -r.oinv.x);
+    ty0 = fmaf(lo.y, r.inv.y, -r.oinv.y), ty1 = fmaf(hi.y, r.inv.y, -r.oinv.y);
+    tz0 = fmaf(lo.z, r.inv.z, -r.oinv.z), tz1 = fmaf(hi.z, r.inv.z, -r.oinv.z);
+  } else {
+    tx0 = (lo.x - r.o.x) * r.inv.x, tx1 = (hi.x - r.o.x) * r.inv.x;
+    ty0 = (lo.y - r.o.y) * r.inv.y, ty1 = (hi.y - r.o.y) * r.inv.y;
+    tz0 = (lo.z - r.o.z) * r.inv.z, tz1 = (hi.z - r.o.z) * r.inv.z;
+  }
+  const float tn = fmax3f(fminf(tx0, tx1), fminf(ty0, ty1), fmaxf(fminf(tz0, tz1), t_lo));
+  const float tf = fmin3f(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fminf(fmaxf(tz0, tz1), t_hi));
   tnear = tn;
   return tn <= tf;
 }
@@ -147,7 +194,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
                                 ScatterAlbedo* sa = nullptr, uint32_t seed = kNoGauss) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
-  const float3 inv = safe_inv(d);
+  const RayBox rb = ray_box(o, d);
   float t_hi = kInf;
   float acc = 0.0f;
   FF lane_tau = {0.0f, 0.0f};  // kAcc: this lane's chords as a compensated float pair
@@ -215,23 +262,47 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   while (true) {
     if (!have) {
       if (sp == 0) break;
-      if constexpr (kKind == kArgmin) {
-        // the argmin's bound shrinks: pop the topmost entry within it, skipping culled ones in
-        // one step (lane j looks at the j-th entry from the top)
+      if constexpr (kKind == kArgmin && VP_ARGMIN_BEST_FIRST) {
+        // the argmin's bound shrinks: pop the nearest entry within it among the top 32 of the
+        // stack (lane j looks at the j-th entry from the top); the top entry fills its place
         const int e = sp - 1 - lane;
-        const unsigned bm = __ballot_sync(kFull, e >= 0 && W.st_t[max(e, 0)] <= t_hi);
-        if (bm == 0u) {
+        const float te = e >= 0 ? W.st_t[e] + 0.0f : kInf;  // + 0: -0 -> +0, so bits order as values
+        const unsigned key = (e >= 0 && te <= t_hi) ? __float_as_uint(te) : 0xFFFFFFFFu;
+        const unsigned mn = __reduce_min_sync(kFull, key);
+        if (mn == 0xFFFFFFFFu) {  // the whole window lies beyond the bound
           sp = max(sp - 32, 0);
           __syncwarp();
           continue;
         }
-        sp -= __ffs(bm);
-      } else {
+        const int es = sp - 1 - (__ffs(__ballot_sync(kFull, key == mn)) - 1);
+        ref = W.st_ref[es];
+        tn = __uint_as_float(mn);
+        __syncwarp();
+        if (lane == 0 && es != sp - 1) {
+          W.st_ref[es] = W.st_ref[sp - 1];
+          W.st_t[es] = W.st_t[sp - 1];
+        }
         --sp;
+        __syncwarp();
+      } else {
+        if constexpr (kKind == kArgmin) {
+          // the argmin's bound shrinks: pop the topmost entry within it, skipping culled ones in
+          // one step (lane j looks at the j-th entry from the top)
+          const int e = sp - 1 - lane;
+          const unsigned bm = __ballot_sync(kFull, e >= 0 && W.st_t[max(e, 0)] <= t_hi);
+          if (bm == 0u) {
+            sp = max(sp - 32, 0);
+            __syncwarp();
+            continue;
+          }
+          sp -= __ffs(bm);
+        } else {
+          --sp;
+        }
+        ref = W.st_ref[sp];
+        tn = W.st_t[sp];
+        __syncwarp();
       }
-      ref = W.st_ref[sp];
-      tn = W.st_t[sp];
-      __syncwarp();
     }
     have = false;
     if (tn > t_hi) continue;
@@ -265,7 +336,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       bool boxed = false;
       if (lane < total && pi != seed) {  // the Gaussian's own 3-sigma box first (32 B), then its record
         float tb;
-        boxed = slab(o, inv, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, t_hi, tb);
+        boxed = slab<kKind == kArgmin>(rb, __ldg(S.pbox + 2u * pi), __ldg(S.pbox + 2u * pi + 1u), 0.0f, t_hi, tb);
       }
       if (boxed) {
         const PrimGeo g = load_geo(S.prims, pi);
@@ -353,7 +424,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       const float4 hi = __ldg(node + 32 + lane);
       const uint32_t cref = __float_as_uint(lo.w);
       float tnear = 0.f;
-      const bool hit = (cref != kEmptyRef) && slab(o, inv, lo, hi, 0.0f, t_hi, tnear);
+      const bool hit = (cref != kEmptyRef) && slab<kKind == kArgmin>(rb, lo, hi, 0.0f, t_hi, tnear);
       const unsigned m = __ballot_sync(kFull, hit);
       const int nh = __popc(m);
       if (nh > 0) {
@@ -368,8 +439,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
         // fixed few instructions instead of a pass over the hit children.
         int rank = 0;
         int src;
-        if constexpr (kKind == kTau) {
-          const unsigned key = hit ? __float_as_uint(tnear) : 0xFFFFFFFFu;  // tnear >= 0: bit order
+        if constexpr (kKind == kTau || VP_ARGMIN_BEST_FIRST) {
+          const unsigned key = hit ? __float_as_uint(tnear + 0.0f) : 0xFFFFFFFFu;  // tnear >= 0: bit order
           const unsigned mn = __reduce_min_sync(kFull, key);
           src = __ffs(__ballot_sync(kFull, hit && key == mn)) - 1;
           rank = __popc(m & lt_mask & ~(1u << src));
@@ -520,7 +591,7 @@ struct ThreadQueries {
 
   template <int kKind>
   __device__ float ray(float3 o, float3 d, uint64_t key) {
-    const float3 inv = safe_inv(d);
+    const RayBox rb = ray_box(o, d);
     uint32_t stack[kBinStack];
     int sp = 0;
     float t_hi = kInf;
@@ -534,8 +605,8 @@ struct ThreadQueries {
       const uint32_t refs[2] = {__float_as_uint(ll.w), __float_as_uint(rl.w)};
       float tn[2];
       bool hit[2];
-      hit[0] = refs[0] != kEmptyRef && slab(o, inv, ll, lh, 0.f, t_hi, tn[0]);
-      hit[1] = refs[1] != kEmptyRef && slab(o, inv, rl, rh, 0.f, t_hi, tn[1]);
+      hit[0] = refs[0] != kEmptyRef && slab(rb, ll, lh, 0.f, t_hi, tn[0]);
+      hit[1] = refs[1] != kEmptyRef && slab(rb, rl, rh, 0.f, t_hi, tn[1]);
       uint32_t next_inner[2];
       int n_inner = 0;
       for (int c = 0; c < 2; ++c) {

@@ -22,8 +22,6 @@
 // same order of radiance accumulation.
 #include <algorithm>
 
-#include <cub/device/device_radix_sort.cuh>
-
 #include "vp_internal.h"
 #include "vp_path.cuh"
 #include "vp_traverse.cuh"
@@ -374,7 +372,7 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   WfWorkspace& w = ctx->wf;
   if (w.cap >= paths && w.base) return VP_OK;
   free_wavefront(ctx);
-  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 4 + 3 * 48 + 16 + 4 * 5 + 3 * 4;
+  const size_t per_path = 4 * 16 + 16 + 8 + 4 + 16 + 4 + 3 * 48 + 16 + 4 * 3 + 3 * 4;
   const size_t bytes = paths * per_path + 64 * 256 + 4096;
   cudaError_t e = cudaMalloc(&w.base, bytes);
   if (e != cudaSuccess) {
@@ -404,14 +402,11 @@ vp_status ensure_workspace(vp_context* ctx, size_t paths) {
   carve_buf(cur, b.qa, paths);
   carve_buf(cur, b.qb, paths);
   carve_buf(cur, b.qs, 3 * paths);
-  carve_buf(cur, b.qt, paths);
   carve_buf(cur, b.sk_a, paths);
-  carve_buf(cur, b.sk_b, paths);
   carve_buf(cur, b.ctr, 64);
   w.cap = paths;
-  size_t tmp = 0;
-  e = cub::DeviceRadixSort::SortPairs(nullptr, tmp, b.sk_a, b.sk_b, b.qa, b.qt, (int)paths, 0, 30);
-  if (e == cudaSuccess) e = cudaMalloc(&w.sort_tmp, tmp);
+  const size_t tmp = radix_sort_tmp_bytes_u32(paths);
+  e = cudaMalloc(&w.sort_tmp, tmp);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     free_wavefront(ctx);
@@ -497,12 +492,9 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   for (uint32_t it = 0; it < P.max_bounces; ++it) {
     if (it != 0u && (it & 3u) == 0u && polled >= kSortMinPaths) {  // (camera rays share one origin)
       k_wf_sort_keys<<<(polled + 255) / 256, 256, 0, st>>>(polled, qcur, b.o4, blo, binv, b.sk_a);
-      size_t tmp = ctx->wf.sort_tmp_bytes;
-      VP_CUDA(cub::DeviceRadixSort::SortPairs(ctx->wf.sort_tmp, tmp, b.sk_a, b.sk_b, qcur, b.qt, (int)polled, 0, 30,
-                                              st));
-      VP_CUDA(cudaGetLastError());
-      ctx->launches += 1;
-      std::swap(qcur, b.qt);
+      vp_status r = radix_sort_pairs(b.sk_a, qcur, polled, 30, ctx->wf.sort_tmp, ctx->wf.sort_tmp_bytes, st,
+                                     &ctx->launches);
+      if (r) return r;
     }
     cudaEvent_t* e4 = ev + 4 * (it & 3u);
     if (timed) VP_CUDA(cudaEventRecord(e4[0], st));

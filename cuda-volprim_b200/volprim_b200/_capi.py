@@ -182,6 +182,7 @@ class vp_server_config(C.Structure):
         ("precision", C.c_int32),
         ("use_graph", C.c_int32),
         ("schedule", C.c_int32),
+        ("srpt_reserve", C.c_float),
     ]
 
 

@@ -4,7 +4,9 @@ include/volprim_b200.h states:
 
     L = (1 - T) C / S + T env(d),   S = sum tau_i,  C = sum tau_i e_i,  T = exp(-S)
 
-per jittered camera ray, averaged over spp (box filter).
+per jittered camera ray, averaged over spp (box filter).  The model has no occlusion between
+Gaussians: a Gaussian behind an opaque one still contributes its tau-weighted share of the colour;
+only the background is attenuated (by the exact transmittance T).
 """
 from __future__ import annotations
 

@@ -27,7 +27,7 @@ class Server:
 
     def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 18,
                  max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
-                 use_graph: bool = True, schedule: str = "fifo"):
+                 use_graph: bool = True, schedule: str = "fifo", srpt_reserve: float = 0.5):
         c = _capi.vp_server_config()
         c.memory_budget_bytes = int(memory_budget_bytes)
         c.path_slots = int(path_slots)
@@ -36,6 +36,7 @@ class Server:
         c.precision = {"auto": 0, "fast": 1, "accurate": 2}[precision]
         c.use_graph = 1 if use_graph else 0
         c.schedule = {"fifo": 0, "fair": 1, "srpt": 2}[schedule]
+        c.srpt_reserve = float(srpt_reserve)
         h = C.c_void_p()
         check(lib.vp_server_create(ctx.handle, C.byref(c), C.byref(h)))
         self.handle, self.ctx = h, ctx
@@ -220,62 +221,115 @@ def run_trace_plain(scenes: list, envs: list, trace: list) -> dict:
             "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "mpaths_per_s": paths / makespan / 1e6}
 
 
-def main(argv=None) -> None:
-    """The serving workload end to end: the 4 resident scenes (50k / 100k / 250k / 500k Gaussians),
-    the first --requests of the seeded request stream all at t = 0 (offline throughput), then
-    with Poisson arrivals at --load x that throughput under each schedule, then through one
-    vp_render per request.  One JSON line per run."""
-    import argparse
-    import json
+def capacity(trace: list) -> list:
+    """The trace with every arrival at t = 0 (saturation)."""
+    return [Request(0.0, r.scene_id, r.camera, r.config) for r in trace]
 
+
+def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, load: float = 0.8, seed: int = 2024,
+                  schedules=("fifo",), path_slots: int = 1 << 18, log=None, rate: float | None = None,
+                  srpt_reserve: float = 0.5, plain: bool = True, capacity_runs: bool = True) -> dict:
+    """The serving workload's measurements on the 4 resident scenes (50k / 100k / 250k / 500k
+    Gaussians, seeds 1-4):
+      offline capacity   the first `capacity_requests` requests of the seeded stream all at t = 0
+                         through one vp_render per request (the offline engine, back to back);
+      served capacity    the same requests at t = 0 through the server (each schedule);
+      latency            all `n_requests` with Poisson arrivals at `load` x the offline capacity,
+                         served (each schedule) and through the plain per-request loop, on the same
+                         arrivals: p50 / p90 / p99 / max of arrival-to-completion wall time.
+    `rate` (requests/s) fixes the arrival rate instead, so runs compare on identical arrivals;
+    `capacity_runs` / `plain` switch those runs off.  Returns the figures as a dict."""
     from . import scenes
-    from .api import Context, Environment, Scene
-
-    ap = argparse.ArgumentParser(prog="python -m volprim_b200.serving")
-    ap.add_argument("--requests", type=int, default=200)
-    ap.add_argument("--load", type=float, default=0.8)
-    ap.add_argument("--schedules", default="fifo,fair,srpt")
-    ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--device", type=int, default=0)
-    ap.add_argument("--slots", default=str(1 << 18), help="path-slot pool sizes to compare (comma separated)")
-    a = ap.parse_args(argv)
-    ctx = Context(a.device)
     gs, sigma, env_img = scenes.serving_scenes()
     scs = [Scene(ctx, g, sigma) for g in gs]
     env = Environment(ctx, rgb=env_img)
+    envs = [env] * len(scs)
 
-    def server(schedule, slots=1 << 18):
-        s = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule, path_slots=slots)
+    def server(schedule):
+        srv = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule, path_slots=path_slots,
+                     srpt_reserve=srpt_reserve)
         for sc in scs:
-            s.add_scene(sc, env)
-        return s
+            srv.add_scene(sc, env)
+        return srv
 
     def summary(r):
         lat = sorted(r["latency_s"])
         return {"p50_s": r["p50_s"], "p90_s": percentile(lat, 90), "p99_s": r["p99_s"], "max_s": lat[-1],
                 "mpaths_per_s": r["mpaths_per_s"], "makespan_s": r["makespan_s"]}
 
-    burst = make_trace(a.seed, a.requests, rate=0.0, n_scenes=len(scs))
-    srv = server("fifo")
-    off = run_trace(srv, burst)
-    srv.close()
-    rate = a.load * off["mpaths_per_s"] * 1e6 / (off["paths"] / a.requests)
-    print(json.dumps({"run": "offline", "requests": a.requests, "paths": off["paths"],
-                      "mpaths_per_s": off["mpaths_per_s"], "arrival_rate_per_s": rate, "load": a.load}), flush=True)
-    trace = make_trace(a.seed, a.requests, rate=rate, n_scenes=len(scs))
-    for slots in (int(x) for x in a.slots.split(",")):
-        for sched in a.schedules.split(","):
-            srv = server(sched, slots)
-            r = run_trace(srv, trace)
-            st = srv.stats()
-            srv.close()
-            print(json.dumps({"run": "served", "schedule": sched, "path_slots": slots, **summary(r),
-                              "device_ms": st["device_ms"], "iterations": st["iterations"]}), flush=True)
-    pl = run_trace_plain(scs, [env] * len(scs), trace)
-    print(json.dumps({"run": "plain per-request", **summary(pl), "busy_s": pl["busy_s"]}), flush=True)
-    for s in scs:
-        s.close()
+    def emit(d):
+        if log:
+            log(d)
+
+    base = make_trace(seed, n_requests, rate=1.0, n_scenes=len(scs))
+    mean_paths = sum(r.paths for r in base) / len(base)
+    burst = capacity(base[:capacity_requests])
+    # warm-up: a few requests through both loops (first-use allocations, graph capture)
+    w = server("fifo")
+    run_trace(w, burst[:8])
+    w.close()
+    run_trace_plain(scs, envs, burst[:8])
+    out = {"requests": n_requests, "capacity_requests": capacity_requests, "load": load,
+           "mean_paths_per_request": mean_paths, "path_slots": path_slots, "srpt_reserve": srpt_reserve}
+    out["served_capacity"] = {}
+    if capacity_runs:
+        pl = run_trace_plain(scs, envs, burst)
+        out["offline_mpaths_per_s"] = pl["mpaths_per_s"]
+        emit({"run": "offline capacity (plain per-request loop, all at t = 0)", **summary(pl)})
+    for sched in (schedules if capacity_runs else ()):
+        srv = server(sched)
+        r = run_trace(srv, burst)
+        st = srv.stats()
+        srv.close()
+        out["served_capacity"][sched] = {"mpaths_per_s": r["mpaths_per_s"],
+                                         "fraction_of_offline": r["mpaths_per_s"] / pl["mpaths_per_s"],
+                                         "device_busy": st["device_ms"] / 1e3 / r["makespan_s"]}
+        emit({"run": f"served capacity ({sched}, all at t = 0)", **summary(r), "device_s": st["device_ms"] / 1e3})
+    if rate is None:
+        rate = load * out["offline_mpaths_per_s"] * 1e6 / mean_paths
+    out["arrival_rate_per_s"] = rate
+    trace = make_trace(seed, n_requests, rate=rate, n_scenes=len(scs))
+    out["served"] = {}
+    for sched in schedules:
+        srv = server(sched)
+        r = run_trace(srv, trace)
+        st = srv.stats()
+        srv.close()
+        out["served"][sched] = {**summary(r), "device_s": st["device_ms"] / 1e3, "iterations": st["iterations"]}
+        emit({"run": f"served ({sched}) at {load:.0%} of offline capacity", **out["served"][sched]})
+    if plain:
+        pr = run_trace_plain(scs, envs, trace)
+        out["plain"] = {**summary(pr), "busy_s": pr["busy_s"]}
+        emit({"run": f"plain per-request loop at {load:.0%} of offline capacity", **out["plain"]})
+    for sc in scs:
+        sc.close()
     env.close()
+    return out
+
+
+def main(argv=None) -> None:
+    """The serving study end to end (serving_study), one JSON line per run and a summary line."""
+    import argparse
+    import json
+    from .api import Context
+    ap = argparse.ArgumentParser(prog="python -m volprim_b200.serving")
+    ap.add_argument("--requests", type=int, default=1000)
+    ap.add_argument("--capacity-requests", type=int, default=300)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--schedules", default="fifo")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--slots", type=int, default=1 << 18)
+    ap.add_argument("--rate", type=float, default=None, help="fixed arrival rate (requests/s)")
+    ap.add_argument("--srpt-reserve", type=float, default=0.5)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-capacity", action="store_true")
+    a = ap.parse_args(argv)
+    ctx = Context(a.device)
+    res = serving_study(ctx, a.requests, a.capacity_requests, a.load, a.seed, tuple(a.schedules.split(",")),
+                        a.slots, log=lambda d: print(json.dumps(d), flush=True), rate=a.rate,
+                        srpt_reserve=a.srpt_reserve, plain=not a.no_plain, capacity_runs=not a.no_capacity)
+    print(json.dumps({"run": "summary", **res}), flush=True)
     ctx.close()
 
 

@@ -397,7 +397,11 @@ vp_status vp_albedo_at(vp_scene* scene, const float* points, uint32_t n, int32_t
  *     L = (1 - T) C / S + T env(d)          (L = env(d) when S = 0),
  * the exact emission-absorption integral when the emission-to-extinction ratio along the ray
  * is its tau-weighted mean C / S (exact for one Gaussian and in the optically thin limit).  It
- * is independent of the order of the Gaussians along the ray.  A pixel is the mean of
+ * is independent of the order of the Gaussians along the ray.  Limitation: there is no
+ * occlusion between Gaussians -- with opaque Gaussians (the differentiation workload's central
+ * tau is in the thousands) a pixel shows the tau-weighted mean emission of every Gaussian its
+ * ray crosses, so a Gaussian behind an opaque one still colours it; only the background is
+ * attenuated, by the exact closed-form transmittance.  A pixel is the mean of
  * params->spp jittered camera rays seeded as vp_render's (box filter); only width, height, spp,
  * seed, pixel_filter_stddev, precision and measure of params are read. */
 
@@ -454,8 +458,9 @@ typedef enum vp_schedule {
   VP_SCHEDULE_FIFO = 0,  /* admission order: a request's paths all start before the next's; free
                             slots the oldest request cannot use go to the next (default) */
   VP_SCHEDULE_FAIR = 1,  /* equal shares (processor sharing); leftovers in table order */
-  VP_SCHEDULE_SRPT = 2   /* fewest unstarted paths first (shortest remaining work), with half of
-                            the free slots kept for the oldest request so large ones progress */
+  VP_SCHEDULE_SRPT = 2   /* fewest unstarted paths first (shortest remaining work), with a share
+                            of the free slots (srpt_reserve, default half) kept for the oldest
+                            request so large ones progress */
 } vp_schedule;
 
 typedef struct vp_server_config {
@@ -469,6 +474,8 @@ typedef struct vp_server_config {
   int32_t precision;             /* vp_precision of every request: FAST or ACCURATE (AUTO = FAST) */
   int32_t use_graph;             /* 1: replay the iterations as a captured CUDA graph */
   int32_t schedule;              /* vp_schedule: how free path slots are shared among requests */
+  float srpt_reserve;            /* VP_SCHEDULE_SRPT: fraction of each iteration's free slots kept
+                                    for the oldest request with unstarted paths (0 = 0.5; at most 1) */
 } vp_server_config;
 
 typedef struct vp_request {
@@ -485,7 +492,7 @@ typedef struct vp_server_stats {
   uint64_t submitted, admitted, completed;
   uint64_t paths_completed;
   uint64_t iterations;
-  uint32_t active;               /* admitted, not completed */
+  uint32_t active;               /* admitted, not yet delivered */
   uint32_t pending;              /* submitted, not admitted */
   uint64_t bytes_in_use;         /* scenes + slots + active accumulators (the budget's measure) */
   double device_ms;              /* device time of the iterations run so far (CUDA events) */
@@ -497,8 +504,14 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
 vp_status vp_server_add_scene(vp_server* server, vp_scene* scene, vp_env* env, uint32_t* scene_id);
 /* Queues a request (copied); returns its id (submission order, from 0). */
 vp_status vp_server_submit(vp_server* server, const vp_request* request, uint64_t* request_id);
-/* Admits what fits, runs iterations_per_step wavefront iterations (nothing if idle), then
- * completes finished requests.  *completed = requests completed by this call. */
+/* Admits what fits and queues iterations_per_step wavefront iterations (a step) on the GPU when
+ * any admitted request is unfinished; then waits for the previous step (every queued step when
+ * nothing new was queued) and harvests it: requests whose paths have all finished get their
+ * mean formed behind the running step, and host outputs are copied on a second stream.  The GPU
+ * never waits for the host between steps.  A request is delivered -- its output written, its
+ * memory released and its id visible to vp_server_poll -- by the first call after its copies
+ * land; a call with nothing left on the GPU waits for them.  *completed = requests delivered by
+ * this call. */
 vp_status vp_server_step(vp_server* server, uint32_t* completed);
 /* Ids of requests completed since the last call (up to cap; the rest stay queued). */
 vp_status vp_server_poll(vp_server* server, uint64_t* ids, uint32_t cap, uint32_t* n);

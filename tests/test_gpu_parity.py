@@ -222,6 +222,12 @@ def test_measurement_bits(vp_ctx):
     assert st["prim_tests"] == sum(st["query_prim_tests"]) > 0
     assert st["geo_loads"] == sum(st["query_geo_loads"]) > 0
     assert st["query_prim_tests"][1] > 0 and st["query_nodes"][1] > 0  # shadow rays traversed
+    # per-query chord histograms: one entry per query, and the top bin holds the maximum
+    hist = np.array(st["hits_hist"], dtype=np.int64)
+    assert hist[1].sum() == st["shadow_rays"] > 0
+    assert hist[0].sum() == st["bounces"] > 0  # albedo > 0: every bounce runs the argmin query
+    top = max(int(np.nonzero(hist[0])[0].max()), int(np.nonzero(hist[1])[0].max()))
+    assert top == int(st["max_hits_per_ray"]).bit_length()
     # two batches: generate + welford and 5 launches per iteration each
     it = st["stage_launches"][0]
     assert st["stage_launches"][1] == it and it >= 2
