@@ -75,7 +75,9 @@ struct SceneView {
   uint32_t count;
   uint32_t wide_root;    // ref of the BVH32 root (a node index; 0)
   uint32_t bin_root;     // ref of the binary root
-  uint32_t stack_cap;    // per-warp stack entries the BVH32 traversal can need
+  uint32_t stack_cap;    // per-warp stack entries a depth-first BVH32 traversal can need
+  uint32_t argmin_cap;   // per-warp stack entries of the argmin traversal (best-first pops need
+                         // room beyond the depth-first bound; see warp_ray_query)
   int32_t albedo_all_zero;
 };
 

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256, VP_WARP_MIN_BLOCKS) k_render_warp(SceneVi
                                                      Counters* __restrict__ ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, kHitCap), S.stack_cap, kHitCap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.argmin_cap, kHitCap), S.argmin_cap, kHitCap);
   const uint32_t n_pix = P.width * P.height;
   uint32_t status = 0;
   WarpStats ws;
@@ -312,7 +312,7 @@ vp_status launch_render(vp_scene* s, vp_env* e, const CameraView& cam, const Par
   cudaStream_t st = ctx->stream;
   if (engine == VP_ENGINE_WARP) {
     const int threads = 256;
-    const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kHitCap);
+    const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.argmin_cap, kHitCap);
     if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the warp engine's shared-memory stack");
     VP_CUDA(cudaMemsetAsync(ctx->work_counter, 0, sizeof(unsigned int), st));
     const bool adaptive = P.adaptive_threshold > 0.0f;

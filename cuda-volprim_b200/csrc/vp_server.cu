@@ -446,7 +446,8 @@ struct vp_server {
   bool accurate = false;
   std::vector<vp_scene*> scenes;
   std::vector<vp_env*> envs;
-  uint32_t max_cap = 0;
+  uint32_t max_cap = 0;         // largest depth-first stack over the scenes (transmittance)
+  uint32_t max_argmin_cap = 0;  // largest argmin stack over the scenes
   // device
   SceneView* d_scenes = nullptr;
   EnvView* d_envs = nullptr;
@@ -578,10 +579,10 @@ vp_status enqueue_iteration(vp_server* s, bool even) {
   k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_alloc_off, s->d_alloc_start, R, s->paths, qcur);
   if (s->accurate)
     k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
-                                                               s->max_cap, ctr);
+                                                               s->max_argmin_cap, ctr);
   else
     k_srv_extend<false><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
-                                                                s->max_cap, ctr);
+                                                                s->max_argmin_cap, ctr);
   k_srv_shade<<<s->thr_blocks, 256, 0, st>>>(s->d_envs, s->d_table, s->paths, qcur, s->d_ctl, qnext);
   if (s->accurate)
     k_srv_shadow<true><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, s->paths, s->d_ctl,
@@ -599,8 +600,12 @@ vp_status prepare_launch(vp_server* s) {
   if (s->thr_blocks) return VP_OK;
   vp_context* ctx = s->ctx;
   s->max_cap = 2;
-  for (vp_scene* sc : s->scenes) s->max_cap = std::max(s->max_cap, sc->view.stack_cap);
-  s->smem_ext = (size_t)8 * warp_smem_bytes(s->max_cap, kSrvHitCap);
+  s->max_argmin_cap = 2;
+  for (vp_scene* sc : s->scenes) {
+    s->max_cap = std::max(s->max_cap, sc->view.stack_cap);
+    s->max_argmin_cap = std::max(s->max_argmin_cap, sc->view.argmin_cap);
+  }
+  s->smem_ext = (size_t)8 * warp_smem_bytes(s->max_argmin_cap, kSrvHitCap);
   s->smem_shd = (size_t)8 * warp_smem_bytes(s->max_cap, 32);
   if (s->smem_ext > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the shared-memory stack");
   auto ext = s->accurate ? k_srv_extend<true> : k_srv_extend<false>;

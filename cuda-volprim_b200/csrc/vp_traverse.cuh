@@ -104,6 +104,7 @@ struct WarpSmem {
   uint32_t* hb_idx;
   float *hb_tc, *hb_rw, *hb_d2, *hb_tin, *hb_tout, *hb_icf;
   int hit_cap;
+  uint32_t st_cap;  // stack entries
 };
 
 __host__ __device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap, int hit_cap) {
@@ -123,6 +124,7 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_ca
   w.hb_tout = hb + 5 * hit_cap;
   w.hb_icf = hb + 6 * hit_cap;
   w.hit_cap = hit_cap;
+  w.st_cap = stack_cap;
   return w;
 }
 
@@ -224,6 +226,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     }
   }
   int sp = 0, hb = 0, kept = 0;  // retained chords [0, kept); hb == kept between leaves
+  // best-first pops while the stack holds at most bf_limit entries (negative: never)
+  const int bf_limit = (int)W.st_cap - (int)S.stack_cap - 64;
   bool keep = (kKind == kArgmin) && sa != nullptr;
   unsigned int hits_seen = 0;
   // The node to visit next is kept in registers (the nearest hit child of the last inner node);
@@ -262,9 +266,13 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   while (true) {
     if (!have) {
       if (sp == 0) break;
-      if constexpr (kKind == kArgmin && VP_ARGMIN_BEST_FIRST) {
+      if (kKind == kArgmin && VP_ARGMIN_BEST_FIRST && sp <= bf_limit) {
         // the argmin's bound shrinks: pop the nearest entry within it among the top 32 of the
-        // stack (lane j looks at the j-th entry from the top); the top entry fills its place
+        // stack (lane j looks at the j-th entry from the top); the top entry fills its place.
+        // Such pops can leave older entries below newer ones, so the stack is not bounded by the
+        // depth-first bound; above bf_limit the traversal pops depth-first (the branch below),
+        // which from any state adds at most one depth-first bound, and the warp's stack holds
+        // bf_limit + 32 + that bound.
         const int e = sp - 1 - lane;
         const float te = e >= 0 ? W.st_t[e] + 0.0f : kInf;  // + 0: -0 -> +0, so bits order as values
         const unsigned key = (e >= 0 && te <= t_hi) ? __float_as_uint(te) : 0xFFFFFFFFu;
@@ -428,7 +436,7 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
       const unsigned m = __ballot_sync(kFull, hit);
       const int nh = __popc(m);
       if (nh > 0) {
-        if ((uint32_t)(sp + nh) > S.stack_cap) {  // cannot happen for a BVH of the recorded depth
+        if ((uint32_t)(sp + nh) > W.st_cap) {  // cannot happen for a BVH of the recorded depth
           status |= kStatusStackOverflow;
           break;
         }

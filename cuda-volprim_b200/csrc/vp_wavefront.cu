@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
                                                    const uint32_t* count, unsigned int* work, Counters* ctr) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.stack_cap, kExtendHitCap), S.stack_cap, kExtendHitCap);
+  const WarpSmem W = carve(smem + warp * warp_smem_bytes(S.argmin_cap, kExtendHitCap), S.argmin_cap, kExtendHitCap);
   const uint32_t n = *count;
   uint32_t status = 0, max_overlap = 0;
   unsigned long long bounces = 0, scatters = 0;
@@ -441,7 +441,7 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
   if ((r = ensure_workspace(ctx, paths))) return r;
   WfBuffers b = ctx->wf.b;
   const int threads = 256;
-  const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, kExtendHitCap);
+  const size_t smem = (size_t)(threads / 32) * warp_smem_bytes(s->view.argmin_cap, kExtendHitCap);
   const size_t smem_sh = (size_t)(threads / 32) * warp_smem_bytes(s->view.stack_cap, 32);
   if (smem > 200 * 1024) return fail(VP_ERROR_LIMIT, "BVH too deep for the shared-memory stack");
   auto ext = P.accurate ? (P.measure ? k_wf_extend<true, true> : k_wf_extend<true, false>)
