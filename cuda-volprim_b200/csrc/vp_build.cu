@@ -838,7 +838,7 @@ vp_status build_empty_scene(vp_context* ctx, const vp_gaussians* g, float sigma_
   v.wide_root = 0u;
   v.bin_root = 0u;
   v.stack_cap = 31u + 2u;
-  v.argmin_cap = 2u * v.stack_cap + 64u;
+  v.argmin_cap = v.stack_cap + kArgminBestFirstStack + 64u;
   v.albedo_all_zero = 1;
   vp_scene_info& info = sc->info;
   info = vp_scene_info{};
@@ -1224,7 +1224,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   v.wide_root = 0u;
   v.bin_root = bin_root;
   v.stack_cap = 31u * depth + 2u;
-  v.argmin_cap = 2u * v.stack_cap + 64u;
+  v.argmin_cap = v.stack_cap + kArgminBestFirstStack + 64u;
   v.albedo_all_zero = eh.any_albedo ? 0 : 1;
   vp_scene_info& info = sc->info;
   info.count = n;

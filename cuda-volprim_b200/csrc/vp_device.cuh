@@ -57,6 +57,9 @@ __host__ __device__ inline uint32_t wide_leaf_ref(uint32_t first, uint32_t count
 __host__ __device__ inline uint32_t wide_leaf_first(uint32_t r) { return r & 0x03FFFFFFu; }
 __host__ __device__ inline uint32_t wide_leaf_count(uint32_t r) { return ((r >> 26) & 31u) + 1u; }
 
+// The argmin traversal pops best-first while its stack holds at most this many entries.
+constexpr uint32_t kArgminBestFirstStack = 64;
+
 // Device error words (raised instead of trapping; read back by the host).
 constexpr uint32_t kStatusStackOverflow = 1u;
 constexpr uint32_t kStatusBadInput = 2u;
@@ -76,8 +79,9 @@ struct SceneView {
   uint32_t wide_root;    // ref of the BVH32 root (a node index; 0)
   uint32_t bin_root;     // ref of the binary root
   uint32_t stack_cap;    // per-warp stack entries a depth-first BVH32 traversal can need
-  uint32_t argmin_cap;   // per-warp stack entries of the argmin traversal (best-first pops need
-                         // room beyond the depth-first bound; see warp_ray_query)
+  uint32_t argmin_cap;   // per-warp stack entries of the argmin traversal: stack_cap +
+                         // kArgminBestFirstStack + 64 (best-first pops need room beyond the
+                         // depth-first bound; see warp_ray_query)
   int32_t albedo_all_zero;
 };
 

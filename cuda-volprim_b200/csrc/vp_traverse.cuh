@@ -226,8 +226,9 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
     }
   }
   int sp = 0, hb = 0, kept = 0;  // retained chords [0, kept); hb == kept between leaves
-  // best-first pops while the stack holds at most bf_limit entries (negative: never)
-  const int bf_limit = (int)W.st_cap - (int)S.stack_cap - 64;
+  // best-first pops while the stack holds at most bf_limit entries (negative: never, for a warp
+  // stack without the argmin's extra room)
+  const int bf_limit = min((int)kArgminBestFirstStack, (int)W.st_cap - (int)S.stack_cap - 64);
   bool keep = (kKind == kArgmin) && sa != nullptr;
   unsigned int hits_seen = 0;
   // The node to visit next is kept in registers (the nearest hit child of the last inner node);
