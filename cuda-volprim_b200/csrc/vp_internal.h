@@ -52,7 +52,8 @@ struct WfBuffers {
   uint32_t* meta;                 // bounce | shadow count << 16 | alive << 18
   float4* alb4;                   // albedo at the scatter point, scatter distance
   uint32_t* sg;                   // the Gaussian of the scatter (scene order) or kNoGauss
-  float4 *so4, *sd4, *sw4;        // 3 transmittance queries per path: origin (+T in .w), dir (+ the
+  float4 *so4, *sd4, *sw4;        // 3 transmittance queries per path: origin (.w: the seed chord's
+                                  // optical depth, -1 without a seed; then T), dir (+ the
                                   // seed Gaussian's bits in .w), weight
   float4* L4;                     // finished sample radiance
   uint32_t *qa, *qb, *qs;         // path queues (current / next) and shadow-query queue

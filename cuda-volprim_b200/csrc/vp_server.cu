@@ -162,7 +162,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 // first pixel-major path index (alloc_start).
 __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, unsigned long long* __restrict__ started,
                               uint32_t* __restrict__ alloc_off, unsigned long long* __restrict__ alloc_start,
-                              int schedule, float srpt_reserve) {
+                              int schedule, float srpt_reserve, uint32_t lane, uint32_t lanes) {
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t s_free, s_surv;
   __shared__ unsigned long long s_key[kMaxRequests], s_seq[kMaxRequests];
@@ -176,8 +176,10 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
   }
   __syncthreads();
   const uint32_t F = s_free;
-  const unsigned long long st0 = started[e];
-  const unsigned long long rem64 = table[e].n_paths - st0;
+  // table entry e belongs to lane e % lanes: only that lane's kernels read or write it
+  const bool mine = (e % lanes) == lane;
+  const unsigned long long st0 = mine ? started[e] : 0ull;
+  const unsigned long long rem64 = mine ? table[e].n_paths - st0 : 0ull;
   const uint32_t rem = (uint32_t)min(rem64, (unsigned long long)F);
   uint32_t a = 0;
   if (schedule == VP_SCHEDULE_FAIR) {
@@ -195,7 +197,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
     a = a1 + (off2 >= F2 ? 0u : min(r2, F2 - off2));
   } else {
     // rank every entry by its key, then hand out the free slots in rank order
-    const unsigned long long seq = table[e].seq;
+    const unsigned long long seq = mine ? table[e].seq : ~0ull;
     const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? rem64 : seq);
     s_key[e] = key;
     s_seq[e] = seq;
@@ -238,7 +240,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
   const uint32_t off = block_exclusive_scan(a, warp_tot, m);
   alloc_off[e] = off;
   alloc_start[e] = st0;
-  started[e] = st0 + a;
+  if (mine) started[e] = st0 + a;
   if (e == R - 1) alloc_off[R] = m;
   if (e == 0) {
     c->survivors = s_surv;
@@ -320,7 +322,10 @@ __global__ void __launch_bounds__(256, 4) k_srv_extend(const SceneView* __restri
   if (lane == 0 && status) atomicOr(&ctr->status, status);
 }
 
-__global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ envs,
+// As the offline engine's shade stage, the shadow rays' seed chords are evaluated here, one
+// thread per ray; a ray whose seed chord alone is opaque gets T = 0 and skips the shadow queue.
+__global__ void __launch_bounds__(256) k_srv_shade(const SceneView* __restrict__ scenes,
+                                                   const EnvView* __restrict__ envs,
                                                    const SrvRequest* __restrict__ table, SrvPaths b,
                                                    const uint32_t* __restrict__ q, SrvCtl* c,
                                                    uint32_t* __restrict__ qnext) {
@@ -332,6 +337,7 @@ __global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ e
     const uint32_t i = base + lane;
     uint32_t p = 0;
     int ns = 0;
+    unsigned queued = 0u;
     bool alive = false;
     if (i < n) {
       p = q[i];
@@ -342,9 +348,15 @@ __global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ e
       alive = shade_bounce(envs[r.scene], r.P, s, a.w < kInf, a.w, f3(a.x, a.y, a.z), sh, b.sg[p]);
       ns = sh.n;
       for (int k = 0; k < sh.n; ++k) {
-        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, 1.f);
+        float seed_tau = -1.0f;  // no seed
+        if (sh.seed[k] != kNoGauss)
+          seed_tau = r.P.accurate ? seed_chord_tau<true>(scenes[r.scene], sh.seed[k], sh.o[k], sh.d[k])
+                                  : seed_chord_tau<false>(scenes[r.scene], sh.seed[k], sh.o[k], sh.d[k]);
+        const bool opaque_k = seed_tau >= kMaxOpticalDepth;
+        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, opaque_k ? 0.0f : seed_tau);
         b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k]));
         b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
+        if (!opaque_k) queued |= 1u << k;
       }
       if (alive) {
         const uint64_t key = draw_bounce_key(s.rng);
@@ -353,8 +365,9 @@ __global__ void __launch_bounds__(256) k_srv_shade(const EnvView* __restrict__ e
       srv_store(b, p, s);
       b.meta[p] = (s.bounce & 0xFFFFu) | ((uint32_t)sh.n << 16) | (alive ? kAlive : 0u);
     }
-    const uint32_t slot = srv_reserve(&c->ctr[2], (uint32_t)ns);
-    for (int k = 0; k < ns; ++k) b.qs[slot + k] = 3u * p + k;
+    uint32_t slot = srv_reserve(&c->ctr[2], (uint32_t)__popc(queued));
+    for (int k = 0; k < ns; ++k)
+      if (queued & (1u << k)) b.qs[slot++] = 3u * p + k;
     const uint32_t qslot = srv_reserve(&c->ctr[1], alive ? 1u : 0u);
     if (alive) qnext[qslot] = p;
   }
@@ -379,7 +392,7 @@ __global__ void __launch_bounds__(256, 4) k_srv_shadow(const SceneView* __restri
     const SceneView S = scenes[table[b.req[qslot / 3u]].scene];
     const float4 o = b.so4[qslot], d = b.sd4[qslot];
     const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws, false,
-                                                 nullptr, __float_as_uint(d.w));
+                                                 nullptr, __float_as_uint(d.w), o.w);
     if (lane == 0) b.so4[qslot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
     if (status) break;
   }
@@ -454,29 +467,37 @@ struct vp_server {
   SrvRequest* d_table = nullptr;
   unsigned long long* d_done = nullptr;
   unsigned long long* d_started = nullptr;      // paths started per table entry
-  uint32_t* d_alloc_off = nullptr;              // this iteration's new paths per entry (prefix, R + 1)
-  unsigned long long* d_alloc_start = nullptr;  // their first path index per entry
-  SrvCtl* d_ctl = nullptr;
-  void* path_mem = nullptr;
-  SrvPaths paths{};
-  // pinned staging (written only while the stream is idle)
+  // pinned staging of the table entries (each reaches the device by a stream-ordered copy)
   SrvRequest* h_table = nullptr;
-  unsigned long long* h_done = nullptr;
-  // graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
   int ext_blocks = 0, shd_blocks = 0, thr_blocks = 0;
   size_t smem_ext = 0, smem_shd = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // pipelining: two step slots, each with its own events and pinned copies of the done counters
-  // and status word
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ev_beg[2] = {}, ev_end[2] = {}, ev_step[2] = {};
-  unsigned long long* h_done_slot[2] = {};
-  unsigned int* h_status = nullptr;  // [2]
-  uint64_t slot_step[2] = {};
-  std::deque<int> inflight;  // step slots queued and not yet harvested (oldest first)
-  uint64_t step_no = 0;      // steps queued so far
+  cudaStream_t copy_stream = nullptr;  // output copies of completed requests
+  // A lane: one pool of path slots with its own control block, queues, stream and graph.  Table
+  // entry e belongs to lane e % lanes, so a lane's kernels read and write only entries that its
+  // own stream updates.  Pipelining: two step slots per lane, each with its own events and pinned
+  // copies of the done counters and the status word.
+  struct Lane {
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    uint32_t slots = 0;
+    SrvCtl* d_ctl = nullptr;
+    uint32_t* d_alloc_off = nullptr;              // this iteration's new paths per entry (prefix, R + 1)
+    unsigned long long* d_alloc_start = nullptr;  // their first path index per entry
+    void* path_mem = nullptr;
+    SrvPaths paths{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaEvent_t ev_beg[2] = {}, ev_end[2] = {}, ev_step[2] = {};
+    unsigned long long* h_done_slot[2] = {};
+    unsigned int* h_status = nullptr;  // [2]
+    uint64_t slot_step[2] = {};
+    std::deque<int> inflight;  // step slots queued and not yet harvested (oldest first)
+    uint64_t step_no = 0;      // steps queued so far
+    uint32_t entries = 0;      // table entries in use
+    unsigned long long load = 0;  // paths of its entries in use (the admission's balance)
+    double busy_ms = 0.0;      // device time of its steps
+  };
+  std::vector<Lane> lanes;
   // host bookkeeping
   struct Active {
     bool used = false;
@@ -487,7 +508,8 @@ struct vp_server {
     int32_t memory = 0;
     float4* sum = nullptr;
     size_t bytes = 0;
-    uint64_t admit_step = 0;  // the first step queued after the admission
+    uint64_t admit_step = 0;  // the first step of its lane queued after the admission
+    uint32_t lane = 0;
   };
   std::vector<Active> active;
   // completed requests whose outputs are still being formed / copied
@@ -517,7 +539,6 @@ struct vp_server {
   uint64_t next_id = 0, admitted = 0, completed = 0, paths_completed = 0, iterations = 0;
   uint32_t n_active = 0;
   size_t bytes_fixed = 0, bytes_active = 0;
-  double device_ms = 0.0;
 };
 
 namespace {
@@ -531,24 +552,32 @@ size_t request_bytes(const vp_request& r) {
 void srv_free(vp_server* s) {
   if (!s) return;
   cudaSetDevice(s->ctx->device);
-  cudaStream_t st = s->ctx->stream;
-  if (st) cudaStreamSynchronize(st);
+  for (auto& L : s->lanes)
+    if (L.st) cudaStreamSynchronize(L.st);
+  if (s->ctx->stream) cudaStreamSynchronize(s->ctx->stream);
   if (s->copy_stream) {
     cudaStreamSynchronize(s->copy_stream);
     cudaStreamDestroy(s->copy_stream);
   }
-  for (int k = 0; k < 2; ++k) {
-    if (s->ev_beg[k]) cudaEventDestroy(s->ev_beg[k]);
-    if (s->ev_end[k]) cudaEventDestroy(s->ev_end[k]);
-    if (s->ev_step[k]) cudaEventDestroy(s->ev_step[k]);
+  for (auto& L : s->lanes) {
+    for (int k = 0; k < 2; ++k) {
+      if (L.ev_beg[k]) cudaEventDestroy(L.ev_beg[k]);
+      if (L.ev_end[k]) cudaEventDestroy(L.ev_end[k]);
+      if (L.ev_step[k]) cudaEventDestroy(L.ev_step[k]);
+    }
+    if (L.h_done_slot[0]) cudaFreeHost(L.h_done_slot[0]);
+    if (L.h_status) cudaFreeHost(L.h_status);
+    if (L.graph_exec) cudaGraphExecDestroy(L.graph_exec);
+    if (L.graph) cudaGraphDestroy(L.graph);
+    cudaFree(L.d_ctl);
+    cudaFree(L.d_alloc_off);
+    cudaFree(L.d_alloc_start);
+    cudaFree(L.path_mem);
+    if (L.own_stream && L.st) cudaStreamDestroy(L.st);
   }
   for (auto& b : s->outs) cudaEventDestroy(b.ev);
   for (cudaEvent_t e : s->spare_events) cudaEventDestroy(e);
   for (void* p : s->pinned_all) cudaFreeHost(p);
-  if (s->h_done_slot[0]) cudaFreeHost(s->h_done_slot[0]);
-  if (s->h_status) cudaFreeHost(s->h_status);
-  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
-  if (s->graph) cudaGraphDestroy(s->graph);
   for (auto& a : s->active)
     if (a.sum) cudaFree(a.sum);
   cudaFree(s->d_scenes);
@@ -556,41 +585,35 @@ void srv_free(vp_server* s) {
   cudaFree(s->d_table);
   cudaFree(s->d_done);
   cudaFree(s->d_started);
-  cudaFree(s->d_alloc_off);
-  cudaFree(s->d_alloc_start);
-  cudaFree(s->d_ctl);
-  cudaFree(s->path_mem);
   cudaFreeHost(s->h_table);
-  cudaFreeHost(s->h_done);
-  if (s->ev0) cudaEventDestroy(s->ev0);
-  if (s->ev1) cudaEventDestroy(s->ev1);
   delete s;
 }
 
-// One wavefront iteration with the queues in the given roles.
-vp_status enqueue_iteration(vp_server* s, bool even) {
-  cudaStream_t st = s->ctx->stream;
-  const uint32_t R = s->cfg.max_requests;
-  uint32_t* qcur = even ? s->paths.qa : s->paths.qb;
-  uint32_t* qnext = even ? s->paths.qb : s->paths.qa;
+// One wavefront iteration of lane l with the queues in the given roles.
+vp_status enqueue_iteration(vp_server* s, uint32_t l, bool even) {
+  vp_server::Lane& L = s->lanes[l];
+  cudaStream_t st = L.st;
+  const uint32_t R = s->cfg.max_requests, nl = (uint32_t)s->lanes.size();
+  uint32_t* qcur = even ? L.paths.qa : L.paths.qb;
+  uint32_t* qnext = even ? L.paths.qb : L.paths.qa;
   Counters* ctr = s->ctx->counters;
-  k_srv_advance<<<1, R, 0, st>>>(s->d_ctl, s->d_table, s->d_started, s->d_alloc_off, s->d_alloc_start,
-                                 s->cfg.schedule, s->cfg.srpt_reserve);
-  k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(s->d_ctl, s->d_table, s->d_alloc_off, s->d_alloc_start, R, s->paths, qcur);
+  k_srv_advance<<<1, R, 0, st>>>(L.d_ctl, s->d_table, s->d_started, L.d_alloc_off, L.d_alloc_start,
+                                 s->cfg.schedule, s->cfg.srpt_reserve, l, nl);
+  k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(L.d_ctl, s->d_table, L.d_alloc_off, L.d_alloc_start, R, L.paths, qcur);
   if (s->accurate)
-    k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
+    k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, L.paths, qcur, L.d_ctl,
                                                                s->max_argmin_cap, ctr);
   else
-    k_srv_extend<false><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, s->paths, qcur, s->d_ctl,
+    k_srv_extend<false><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, L.paths, qcur, L.d_ctl,
                                                                 s->max_argmin_cap, ctr);
-  k_srv_shade<<<s->thr_blocks, 256, 0, st>>>(s->d_envs, s->d_table, s->paths, qcur, s->d_ctl, qnext);
+  k_srv_shade<<<s->thr_blocks, 256, 0, st>>>(s->d_scenes, s->d_envs, s->d_table, L.paths, qcur, L.d_ctl, qnext);
   if (s->accurate)
-    k_srv_shadow<true><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, s->paths, s->d_ctl,
+    k_srv_shadow<true><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, L.paths, L.d_ctl,
                                                                s->max_cap, ctr);
   else
-    k_srv_shadow<false><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, s->paths, s->d_ctl,
+    k_srv_shadow<false><<<s->shd_blocks, 256, s->smem_shd, st>>>(s->d_scenes, s->d_table, L.paths, L.d_ctl,
                                                                 s->max_cap, ctr);
-  k_srv_gather<<<s->thr_blocks, 256, 0, st>>>(s->d_table, s->paths, qcur, s->d_ctl, s->d_done);
+  k_srv_gather<<<s->thr_blocks, 256, 0, st>>>(s->d_table, L.paths, qcur, L.d_ctl, s->d_done);
   VP_CUDA(cudaGetLastError());
   return VP_OK;
 }
@@ -618,31 +641,41 @@ vp_status prepare_launch(vp_server* s) {
   s->shd_blocks = ctx->sm_count * srv_blocks(shd, 256, s->smem_shd);
   s->thr_blocks = ctx->sm_count * 8;
   if (s->cfg.use_graph) {
-    cudaStream_t st = ctx->stream;
-    VP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    vp_status r1 = enqueue_iteration(s, true);
-    vp_status r2 = r1 == VP_OK ? enqueue_iteration(s, false) : r1;
-    cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(st, &g);
-    if (r2 != VP_OK) {
-      if (g) cudaGraphDestroy(g);
-      return r2;
+    for (uint32_t l = 0; l < (uint32_t)s->lanes.size(); ++l) {
+      vp_server::Lane& L = s->lanes[l];
+      VP_CUDA(cudaStreamBeginCapture(L.st, cudaStreamCaptureModeThreadLocal));
+      vp_status r1 = enqueue_iteration(s, l, true);
+      vp_status r2 = r1 == VP_OK ? enqueue_iteration(s, l, false) : r1;
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(L.st, &g);
+      if (r2 != VP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r2;
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+      L.graph = g;
+      VP_CUDA(cudaGraphInstantiate(&L.graph_exec, g, 0));
     }
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    s->graph = g;
-    VP_CUDA(cudaGraphInstantiate(&s->graph_exec, g, 0));
   }
   return VP_OK;
 }
 
 vp_status admit(vp_server* s) {
-  cudaStream_t st = s->ctx->stream;
-  while (!s->pending.empty() && s->n_entries < s->cfg.max_requests) {
+  const uint32_t R = s->cfg.max_requests, nl = (uint32_t)s->lanes.size();
+  while (!s->pending.empty() && s->n_entries < R) {
     const vp_request& rq = s->pending.front().r;
     const size_t need = request_bytes(rq);
     if (s->cfg.memory_budget_bytes && s->bytes_fixed + s->bytes_active + need > s->cfg.memory_budget_bytes) break;
-    uint32_t e = 0;
-    while (s->active[e].used) ++e;
+    // the least-loaded lane with a free entry (entry e belongs to lane e % nl)
+    uint32_t lane = nl;
+    for (uint32_t l = 0; l < nl; ++l)
+      if (s->lanes[l].entries < (R - l + nl - 1) / nl && (lane == nl || s->lanes[l].load < s->lanes[lane].load))
+        lane = l;
+    if (lane == nl) break;
+    uint32_t e = lane;
+    while (s->active[e].used) e += nl;
+    vp_server::Lane& L = s->lanes[lane];
+    cudaStream_t st = L.st;
     vp_server::Active& a = s->active[e];
     const uint32_t n_pix = rq.params.width * rq.params.height;
     float4* sum = nullptr;
@@ -671,7 +704,10 @@ vp_status admit(vp_server* s) {
     a.memory = rq.memory;
     a.sum = sum;
     a.bytes = need;
-    a.admit_step = s->step_no;
+    a.admit_step = L.step_no;
+    a.lane = lane;
+    L.entries += 1;
+    L.load += t.n_paths;
     s->bytes_active += need;
     s->n_active += 1;
     s->n_entries += 1;
@@ -703,15 +739,16 @@ void* pinned_acquire(vp_server* s, size_t bytes, size_t* got) {
 // Completed requests of one harvested step: the mean is formed on the compute stream (behind the
 // step now running), host outputs are copied on the copy stream into pinned staging, and one event
 // on the copy stream marks the batch ready for delivery.
-vp_status harvest(vp_server* s, int slot) {
-  cudaStream_t st = s->ctx->stream, cs = s->copy_stream;
-  if (s->h_status[slot])
-    return fail(VP_ERROR_DEVICE_STATUS, "a serving kernel raised device status " + std::to_string(s->h_status[slot]));
+vp_status harvest(vp_server* s, uint32_t l, int slot) {
+  vp_server::Lane& L = s->lanes[l];
+  cudaStream_t st = L.st, cs = s->copy_stream;
+  if (L.h_status[slot])
+    return fail(VP_ERROR_DEVICE_STATUS, "a serving kernel raised device status " + std::to_string(L.h_status[slot]));
   float ms = 0.f;
-  VP_CUDA(cudaEventElapsedTime(&ms, s->ev_beg[slot], s->ev_end[slot]));
-  s->device_ms += ms;
-  const uint32_t R = s->cfg.max_requests;
-  const unsigned long long* done = s->h_done_slot[slot];
+  VP_CUDA(cudaEventElapsedTime(&ms, L.ev_beg[slot], L.ev_end[slot]));
+  L.busy_ms += ms;
+  const uint32_t R = s->cfg.max_requests, nl = (uint32_t)s->lanes.size();
+  const unsigned long long* done = L.h_done_slot[slot];
   vp_server::OutBatch batch{};
   struct Copy {
     float4* tmp;
@@ -719,9 +756,9 @@ vp_status harvest(vp_server* s, int slot) {
     size_t bytes;
   };
   std::vector<Copy> copies;
-  for (uint32_t e = 0; e < R; ++e) {
+  for (uint32_t e = l; e < R; e += nl) {  // the lane's entries
     vp_server::Active& a = s->active[e];
-    if (!a.used || a.admit_step > s->slot_step[slot] || done[e] < a.n_paths) continue;
+    if (!a.used || a.admit_step > L.slot_step[slot] || done[e] < a.n_paths) continue;
     const float inv = 1.0f / (float)a.spp;
     const unsigned nb = (a.n_pix + 255u) / 256u;
     vp_server::Delivery d{a.id, a.n_paths, nullptr, nullptr, 16ull * a.n_pix, 0, a.bytes};
@@ -740,6 +777,8 @@ vp_status harvest(vp_server* s, int slot) {
     }
     VP_CUDA(cudaFreeAsync(a.sum, st));
     batch.items.push_back(d);
+    L.entries -= 1;
+    L.load -= a.n_paths;
     a = vp_server::Active{};
     s->n_entries -= 1;
   }
@@ -827,8 +866,15 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
     srv_free(s);
     return fail(VP_ERROR_INVALID_ARGUMENT, "unknown schedule");
   }
-  const uint32_t R = c.max_requests, P = c.path_slots;
+  if (c.lanes == 0) c.lanes = 1;
+  if (c.lanes > 4) {
+    srv_free(s);
+    return fail(VP_ERROR_LIMIT, "lanes above 4");
+  }
+  const uint32_t R = c.max_requests, NL = c.lanes;
+  const uint32_t P = ((c.path_slots / NL) + 255u) & ~255u;  // slots per lane
   s->active.resize(R);
+  s->lanes.resize(NL);
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) {
     if (e == cudaSuccess) e = x;
@@ -838,30 +884,39 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   chk(cudaMalloc(&s->d_table, R * sizeof(SrvRequest)));
   chk(cudaMalloc(&s->d_done, R * sizeof(unsigned long long)));
   chk(cudaMalloc(&s->d_started, R * 8ull));
-  chk(cudaMalloc(&s->d_alloc_off, (R + 1ull) * 4ull));
-  chk(cudaMalloc(&s->d_alloc_start, R * 8ull));
-  chk(cudaMalloc(&s->d_ctl, sizeof(SrvCtl)));
   chk(cudaMallocHost(&s->h_table, R * sizeof(SrvRequest)));
-  chk(cudaMallocHost(&s->h_done, R * sizeof(unsigned long long)));
-  chk(cudaEventCreate(&s->ev0));
-  chk(cudaEventCreate(&s->ev1));
   chk(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
-  for (int k = 0; k < 2; ++k) {
-    chk(cudaEventCreate(&s->ev_beg[k]));
-    chk(cudaEventCreate(&s->ev_end[k]));
-    chk(cudaEventCreateWithFlags(&s->ev_step[k], cudaEventDisableTiming));
-  }
-  chk(cudaMallocHost(&s->h_done_slot[0], 2ull * R * sizeof(unsigned long long)));
-  chk(cudaMallocHost(&s->h_status, 2 * sizeof(unsigned int)));
   const size_t slot_bytes = (size_t)P * kSlotBytes + 32 * 256;
-  chk(cudaMalloc(&s->path_mem, slot_bytes));
+  for (uint32_t l = 0; l < NL; ++l) {
+    vp_server::Lane& L = s->lanes[l];
+    L.slots = P;
+    if (l == 0) {
+      L.st = ctx->stream;
+    } else {
+      chk(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
+      L.own_stream = e == cudaSuccess;
+    }
+    chk(cudaMalloc(&L.d_alloc_off, (R + 1ull) * 4ull));
+    chk(cudaMalloc(&L.d_alloc_start, R * 8ull));
+    chk(cudaMalloc(&L.d_ctl, sizeof(SrvCtl)));
+    for (int k = 0; k < 2; ++k) {
+      chk(cudaEventCreate(&L.ev_beg[k]));
+      chk(cudaEventCreate(&L.ev_end[k]));
+      chk(cudaEventCreateWithFlags(&L.ev_step[k], cudaEventDisableTiming));
+    }
+    chk(cudaMallocHost(&L.h_done_slot[0], 2ull * R * sizeof(unsigned long long)));
+    chk(cudaMallocHost(&L.h_status, 2 * sizeof(unsigned int)));
+    chk(cudaMalloc(&L.path_mem, slot_bytes));
+    if (e == cudaSuccess) L.h_done_slot[1] = L.h_done_slot[0] + R;
+  }
   if (e != cudaSuccess) {
     srv_free(s);
     return cuda_fail(e, "vp_server_create");
   }
-  s->h_done_slot[1] = s->h_done_slot[0] + R;
-  char* cur = static_cast<char*>(s->path_mem);
-  SrvPaths& b = s->paths;
+  for (uint32_t l = 0; l < NL; ++l) {
+  vp_server::Lane& L = s->lanes[l];
+  char* cur = static_cast<char*>(L.path_mem);
+  SrvPaths& b = L.paths;
   srv_carve(cur, b.o4, P);
   srv_carve(cur, b.d4, P);
   srv_carve(cur, b.thr4, P);
@@ -880,9 +935,10 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   srv_carve(cur, b.qb, P);
   srv_carve(cur, b.qs, 3ull * P);
   srv_carve(cur, b.free_stack, P);
-  s->bytes_fixed = slot_bytes + R * (sizeof(SrvRequest) + 28ull);
+  k_srv_init<<<(P + 255) / 256, 256, 0, ctx->stream>>>(L.d_ctl, b.free_stack, P);
+  }
+  s->bytes_fixed = NL * slot_bytes + R * (sizeof(SrvRequest) + 28ull);
   cudaStream_t st = ctx->stream;
-  k_srv_init<<<(P + 255) / 256, 256, 0, st>>>(s->d_ctl, b.free_stack, P);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, R * sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_started, 0, R * sizeof(unsigned long long), st);
@@ -948,38 +1004,48 @@ vp_status vp_server_step(vp_server* s, uint32_t* completed) {
   if ((r = prepare_launch(s))) return r;
   if ((r = deliver(s, false, &nd))) return r;
   if ((r = admit(s))) return r;
-  cudaStream_t st = s->ctx->stream;
-  const bool launch = s->n_entries > 0;
-  if (launch) {  // queue step k: its iterations, then the done counters and status to pinned memory
-    const int slot = s->inflight.empty() ? 0 : (s->inflight.back() ^ 1);
-    VP_CUDA(cudaEventRecord(s->ev_beg[slot], st));
+  const uint32_t nl = (uint32_t)s->lanes.size();
+  bool launched[4] = {false, false, false, false};
+  for (uint32_t l = 0; l < nl; ++l) {  // queue step k of every lane with work
+    vp_server::Lane& L = s->lanes[l];
+    if (L.entries == 0) continue;
+    cudaStream_t st = L.st;
+    const int slot = L.inflight.empty() ? 0 : (L.inflight.back() ^ 1);
+    VP_CUDA(cudaEventRecord(L.ev_beg[slot], st));
     for (uint32_t k = 0; k < s->cfg.iterations_per_step; k += 2) {
-      if (s->graph_exec) {
-        VP_CUDA(cudaGraphLaunch(s->graph_exec, st));
+      if (L.graph_exec) {
+        VP_CUDA(cudaGraphLaunch(L.graph_exec, st));
       } else {
-        if ((r = enqueue_iteration(s, true))) return r;
-        if ((r = enqueue_iteration(s, false))) return r;
+        if ((r = enqueue_iteration(s, l, true))) return r;
+        if ((r = enqueue_iteration(s, l, false))) return r;
       }
     }
-    VP_CUDA(cudaEventRecord(s->ev_end[slot], st));
-    VP_CUDA(cudaMemcpyAsync(s->h_done_slot[slot], s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
+    VP_CUDA(cudaEventRecord(L.ev_end[slot], st));
+    VP_CUDA(cudaMemcpyAsync(L.h_done_slot[slot], s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, st));
-    VP_CUDA(cudaMemcpyAsync(s->h_status + slot, &s->ctx->counters->status, sizeof(unsigned int),
+    VP_CUDA(cudaMemcpyAsync(L.h_status + slot, &s->ctx->counters->status, sizeof(unsigned int),
                             cudaMemcpyDeviceToHost, st));
-    VP_CUDA(cudaEventRecord(s->ev_step[slot], st));
-    s->slot_step[slot] = s->step_no++;
+    VP_CUDA(cudaEventRecord(L.ev_step[slot], st));
+    L.slot_step[slot] = L.step_no++;
     s->iterations += s->cfg.iterations_per_step;
-    s->inflight.push_back(slot);
+    L.inflight.push_back(slot);
+    launched[l] = true;
   }
-  // harvest step k-1 while step k runs (every queued step when nothing new was queued)
-  while (s->inflight.size() > (launch ? 1u : 0u)) {
-    const int slot = s->inflight.front();
-    s->inflight.pop_front();
-    VP_CUDA(cudaEventSynchronize(s->ev_step[slot]));
-    if ((r = harvest(s, slot))) return r;
+  // harvest each lane's step k-1 while its step k runs (every queued step of a lane that queued
+  // nothing new)
+  bool any_inflight = false;
+  for (uint32_t l = 0; l < nl; ++l) {
+    vp_server::Lane& L = s->lanes[l];
+    while (L.inflight.size() > (launched[l] ? 1u : 0u)) {
+      const int slot = L.inflight.front();
+      L.inflight.pop_front();
+      VP_CUDA(cudaEventSynchronize(L.ev_step[slot]));
+      if ((r = harvest(s, l, slot))) return r;
+    }
+    any_inflight = any_inflight || !L.inflight.empty();
   }
   // with no step left on the GPU, wait for the outputs still being copied
-  if ((r = deliver(s, s->inflight.empty() && s->n_entries == 0, &nd))) return r;
+  if ((r = deliver(s, !any_inflight && s->n_entries == 0, &nd))) return r;
   if (completed) *completed = nd;
   return VP_OK;
 }
@@ -1004,7 +1070,7 @@ vp_status vp_server_get_stats(vp_server* s, vp_server_stats* out) {
   out->active = s->n_active;
   out->pending = (uint32_t)s->pending.size();
   out->bytes_in_use = s->bytes_fixed + s->bytes_active;
-  out->device_ms = s->device_ms;
+  for (const auto& L : s->lanes) out->device_ms = std::max(out->device_ms, L.busy_ms);  // the busiest lane
   return VP_OK;
 }
 

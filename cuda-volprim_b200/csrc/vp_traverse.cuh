@@ -170,6 +170,19 @@ struct ScatterAlbedo {
   bool valid;
 };
 
+// Optical depth of the seed Gaussian's chord along a shadow ray from its origin: the first term of
+// a transmittance query, also evaluated ahead of the query, one thread per ray, by the shading
+// kernels (a ray whose seed chord alone reaches MAX_OPTICAL_DEPTH then never enters the query).
+template <bool kAcc>
+__device__ __forceinline__ float seed_chord_tau(const SceneView& S, uint32_t seed, float3 o, float3 d) {
+  const PrimGeo g = load_geo(S.prims, seed);
+  Chord ch;
+  if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f)
+    return chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, g.icf,
+                           ch.d2lo);
+  return 0.0f;
+}
+
 // One ray query of the warp: kArgmin returns the smallest accepted free-flight distance over
 // every Gaussian whose chord overlaps [0, t) (kInf = escape); kTau returns the optical depth
 // over [0, inf), stopping once it reaches MAX_OPTICAL_DEPTH.
@@ -188,12 +201,13 @@ struct ScatterAlbedo {
 // transmittance bound.
 //
 // A kTau query whose origin lies inside a known Gaussian (`seed`, the one whose free flight put
-// the path there) evaluates that chord first: in a dense medium it alone usually reaches
-// MAX_OPTICAL_DEPTH and the traversal is skipped; otherwise the traversal skips it at its leaf.
+// the path there) evaluates that chord first (or takes its value, seed_tau, when the caller
+// evaluated it already): in a dense medium it alone usually reaches MAX_OPTICAL_DEPTH and the
+// traversal is skipped; otherwise the traversal skips it at its leaf.
 template <bool kAcc, int kKind>
 __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o, float3 d,
                                 uint64_t key, uint32_t& status, WarpStats& ws, bool measure,
-                                ScatterAlbedo* sa = nullptr, uint32_t seed = kNoGauss) {
+                                ScatterAlbedo* sa = nullptr, uint32_t seed = kNoGauss, float seed_tau = -1.0f) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const RayBox rb = ray_box(o, d);
@@ -206,14 +220,8 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
   };
   uint32_t arg = kNoGauss;  // kArgmin: the Gaussian of the current minimum
   if (kKind == kTau && seed != kNoGauss) {
-    float v = 0.0f;
-    if (lane == 0) {
-      const PrimGeo g = load_geo(S.prims, seed);
-      Chord ch;
-      if (chord_setup<kAcc>(g, o, d, ch) && ch.t_out > 0.0f)
-        v = chord_tau<kAcc>(ch.tc, ch.rw, ch.d2, ch.h, chord_u0(ch, 0.0f), fmaxf(ch.t_in, 0.0f), ch.t_out, g.icf,
-                            ch.d2lo);
-    }
+    float v = 0.0f;  // seed_tau >= 0: evaluated ahead of the query (seed_chord_tau)
+    if (lane == 0) v = seed_tau >= 0.0f ? seed_tau : seed_chord_tau<kAcc>(S, seed, o, d);
     acc = __shfl_sync(kFull, v, 0);
     if (kAcc) lane_tau.hi = v;  // v is 0 on lanes other than 0
     if (measure) ws.crossings += 1;

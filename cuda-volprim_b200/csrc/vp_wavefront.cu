@@ -194,11 +194,14 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
   }
 }
 
-__global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuffers b, const uint32_t* q,
-                                                  const uint32_t* count, uint32_t* qnext, uint32_t* cnext,
-                                                  Counters* ctr) {
+// The shadow rays' seed chords are evaluated here, one thread per ray (seed_chord_tau): a ray
+// whose seed chord alone reaches MAX_OPTICAL_DEPTH gets T = 0 and never enters the shadow queue;
+// the others carry the seed's optical depth to the transmittance query in so4.w.
+__global__ void __launch_bounds__(256) k_wf_shade(SceneView S, EnvView E, ParamsView P, WfBuffers b,
+                                                  const uint32_t* q, const uint32_t* count, uint32_t* qnext,
+                                                  uint32_t* cnext, Counters* ctr) {
   const uint32_t n = *count;
-  unsigned long long shadows = 0;
+  unsigned long long shadows = 0, opaque = 0;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x / 32);
   const uint32_t wid = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
@@ -208,6 +211,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
     const bool valid = i < n;
     uint32_t p = 0;
     int ns = 0;
+    unsigned queued = 0u;  // bit k: shadow ray k enters the shadow queue
     bool alive = false;
     if (valid) {
       p = q[i];
@@ -218,9 +222,17 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
       alive = shade_bounce(E, P, s, scattered, a.w, f3(a.x, a.y, a.z), sh, b.sg[p]);
       ns = sh.n;
       for (int k = 0; k < sh.n; ++k) {
-        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, 1.f);
+        float seed_tau = -1.0f;  // no seed
+        if (sh.seed[k] != kNoGauss)
+          seed_tau = P.accurate ? seed_chord_tau<true>(S, sh.seed[k], sh.o[k], sh.d[k])
+                                : seed_chord_tau<false>(S, sh.seed[k], sh.o[k], sh.d[k]);
+        const bool opaque_k = seed_tau >= kMaxOpticalDepth;
+        // .w of the origin: the seed's optical depth for the query, or T = 0 already
+        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, opaque_k ? 0.0f : seed_tau);
         b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k]));
         b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
+        if (!opaque_k) queued |= 1u << k;
+        else opaque += 1;
       }
       if (alive) {
         const uint64_t key = draw_bounce_key(s.rng);
@@ -230,14 +242,23 @@ __global__ void __launch_bounds__(256) k_wf_shade(EnvView E, ParamsView P, WfBuf
       b.meta[p] = (s.bounce & 0xFFFFu) | ((uint32_t)sh.n << 16) | (alive ? kAliveBit : 0u);
     }
     shadows += (unsigned)ns;
-    const uint32_t slot = queue_reserve(b.ctr + 2, (uint32_t)ns);
-    for (int k = 0; k < ns; ++k) b.qs[slot + k] = 3u * p + k;
+    uint32_t slot = queue_reserve(b.ctr + 2, (uint32_t)__popc(queued));
+    for (int k = 0; k < ns; ++k)
+      if (queued & (1u << k)) b.qs[slot++] = 3u * p + k;
     const uint32_t qslot = queue_reserve(cnext, alive ? 1u : 0u);
     if (alive) qnext[qslot] = p;
   }
   if (P.measure) {
-    for (int o = 16; o > 0; o >>= 1) shadows += __shfl_xor_sync(0xFFFFFFFFu, shadows, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      shadows += __shfl_xor_sync(0xFFFFFFFFu, shadows, o);
+      opaque += __shfl_xor_sync(0xFFFFFFFFu, opaque, o);
+    }
     if ((threadIdx.x & 31) == 0 && shadows) atomicAdd(&ctr->shadow_rays, shadows);
+    if ((threadIdx.x & 31) == 0 && opaque) {  // transmittance queries answered by their seed chord
+      atomicAdd(&ctr->crossings, opaque);
+      atomicAdd(&ctr->hits_hist[1][1], opaque);
+      atomicMax(&ctr->max_hits, 1u);
+    }
   }
 }
 
@@ -260,7 +281,7 @@ __global__ void __launch_bounds__(256, kAcc ? VP_WF_MIN_BLOCKS : VP_WF_SHADOW_MI
     const uint32_t slot = __ldg(b.qs + item);
     const float4 o = b.so4[slot], d = b.sd4[slot];
     const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws,
-                                                 measure, nullptr, __float_as_uint(d.w));
+                                                 measure, nullptr, __float_as_uint(d.w), o.w);
     if (lane == 0) b.so4[slot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
     if (status) break;
   }
@@ -500,7 +521,8 @@ vp_status launch_wavefront(vp_scene* s, vp_env* e, const CameraView& cam, const 
     if (timed) VP_CUDA(cudaEventRecord(e4[0], st));
     ext<<<ext_blocks, threads, smem, st>>>(s->view, P, b, qcur, b.ctr + 0, b.ctr + 3, ctx->counters);
     if (timed) VP_CUDA(cudaEventRecord(e4[1], st));
-    k_wf_shade<<<thr_blocks, threads, 0, st>>>(e->view, P, b, qcur, b.ctr + 0, qnext, b.ctr + 1, ctx->counters);
+    k_wf_shade<<<thr_blocks, threads, 0, st>>>(s->view, e->view, P, b, qcur, b.ctr + 0, qnext, b.ctr + 1,
+                                               ctx->counters);
     if (timed) VP_CUDA(cudaEventRecord(e4[2], st));
     shd<<<shd_blocks, threads, smem_sh, st>>>(s->view, b, b.ctr + 2, b.ctr + 4, ctx->counters, P.measure);
     if (timed) VP_CUDA(cudaEventRecord(e4[3], st));

@@ -183,6 +183,7 @@ class vp_server_config(C.Structure):
         ("use_graph", C.c_int32),
         ("schedule", C.c_int32),
         ("srpt_reserve", C.c_float),
+        ("lanes", C.c_uint32),
     ]
 
 

@@ -27,7 +27,7 @@ class Server:
 
     def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 18,
                  max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
-                 use_graph: bool = True, schedule: str = "fifo", srpt_reserve: float = 0.5):
+                 use_graph: bool = True, schedule: str = "fifo", srpt_reserve: float = 0.5, lanes: int = 1):
         c = _capi.vp_server_config()
         c.memory_budget_bytes = int(memory_budget_bytes)
         c.path_slots = int(path_slots)
@@ -37,6 +37,7 @@ class Server:
         c.use_graph = 1 if use_graph else 0
         c.schedule = {"fifo": 0, "fair": 1, "srpt": 2}[schedule]
         c.srpt_reserve = float(srpt_reserve)
+        c.lanes = int(lanes)
         h = C.c_void_p()
         check(lib.vp_server_create(ctx.handle, C.byref(c), C.byref(h)))
         self.handle, self.ctx = h, ctx
@@ -228,7 +229,8 @@ def capacity(trace: list) -> list:
 
 def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, load: float = 0.8, seed: int = 2024,
                   schedules=("fifo",), path_slots: int = 1 << 18, log=None, rate: float | None = None,
-                  srpt_reserve: float = 0.5, plain: bool = True, capacity_runs: bool = True) -> dict:
+                  srpt_reserve: float = 0.5, plain: bool = True, capacity_runs: bool = True,
+                  lanes: int = 1) -> dict:
     """The serving workload's measurements on the 4 resident scenes (50k / 100k / 250k / 500k
     Gaussians, seeds 1-4):
       offline capacity   the first `capacity_requests` requests of the seeded stream all at t = 0
@@ -247,7 +249,7 @@ def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, loa
 
     def server(schedule):
         srv = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule, path_slots=path_slots,
-                     srpt_reserve=srpt_reserve)
+                     srpt_reserve=srpt_reserve, lanes=lanes)
         for sc in scs:
             srv.add_scene(sc, env)
         return srv
@@ -270,7 +272,8 @@ def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, loa
     w.close()
     run_trace_plain(scs, envs, burst[:8])
     out = {"requests": n_requests, "capacity_requests": capacity_requests, "load": load,
-           "mean_paths_per_request": mean_paths, "path_slots": path_slots, "srpt_reserve": srpt_reserve}
+           "mean_paths_per_request": mean_paths, "path_slots": path_slots, "srpt_reserve": srpt_reserve,
+           "lanes": lanes}
     out["served_capacity"] = {}
     if capacity_runs:
         pl = run_trace_plain(scs, envs, burst)
@@ -324,11 +327,13 @@ def main(argv=None) -> None:
     ap.add_argument("--srpt-reserve", type=float, default=0.5)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-capacity", action="store_true")
+    ap.add_argument("--lanes", type=int, default=1)
     a = ap.parse_args(argv)
     ctx = Context(a.device)
     res = serving_study(ctx, a.requests, a.capacity_requests, a.load, a.seed, tuple(a.schedules.split(",")),
                         a.slots, log=lambda d: print(json.dumps(d), flush=True), rate=a.rate,
-                        srpt_reserve=a.srpt_reserve, plain=not a.no_plain, capacity_runs=not a.no_capacity)
+                        srpt_reserve=a.srpt_reserve, plain=not a.no_plain, capacity_runs=not a.no_capacity,
+                        lanes=a.lanes)
     print(json.dumps({"run": "summary", **res}), flush=True)
     ctx.close()
 

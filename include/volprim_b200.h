@@ -476,6 +476,10 @@ typedef struct vp_server_config {
   int32_t schedule;              /* vp_schedule: how free path slots are shared among requests */
   float srpt_reserve;            /* VP_SCHEDULE_SRPT: fraction of each iteration's free slots kept
                                     for the oldest request with unstarted paths (0 = 0.5; at most 1) */
+  uint32_t lanes;                /* independent path pools (0 = 1, at most 4), each with
+                                    path_slots / lanes slots, its own stream and graph; a request
+                                    runs in the least-loaded lane, and one lane's kernels fill the
+                                    SMs that another lane's leave idle as they drain */
 } vp_server_config;
 
 typedef struct vp_request {
@@ -495,7 +499,8 @@ typedef struct vp_server_stats {
   uint32_t active;               /* admitted, not yet delivered */
   uint32_t pending;              /* submitted, not admitted */
   uint64_t bytes_in_use;         /* scenes + slots + active accumulators (the budget's measure) */
-  double device_ms;              /* device time of the iterations run so far (CUDA events) */
+  double device_ms;              /* device time of the iterations run so far (CUDA events; with
+                                    several lanes, the busiest lane's) */
 } vp_server_stats;
 
 vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_server** out);

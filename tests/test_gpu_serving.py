@@ -132,6 +132,21 @@ def test_graph_and_direct_launches_agree(vp_ctx, world):
         assert np.all(close(a, b))
 
 
+def test_lanes_agree(vp_ctx, world):
+    """Two lanes (independent path pools on their own streams, each request in one of them) give
+    every request the output one lane gives it."""
+    reqs = requests(13, 10)
+    out = {}
+    for lanes in (1, 2):
+        srv = new_server(vp_ctx, world, lanes=lanes)
+        ids = [srv.submit(r.scene_id, r.camera, r.config) for r in reqs]
+        assert sorted(drain(srv)) == sorted(ids)
+        out[lanes] = [srv.result(i) for i in ids]
+        srv.close()
+    for a, b in zip(out[1], out[2]):
+        assert np.all(close(a, b))
+
+
 def test_schedules(vp_ctx, world):
     """Every schedule gives the same images; under FAIR and SRPT a small request submitted after
     a large one (more paths than the slot pool) completes first."""
