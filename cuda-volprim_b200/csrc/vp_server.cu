@@ -53,6 +53,8 @@ struct SrvRequest {  // device request-table entry (all zero while unused)
   ParamsView P;
   uint32_t scene;    // resident (scene, env) pair
   uint32_t n_pix;
+  uint32_t cancelled;  // set by vp_server_cancel: start no further paths
+  uint32_t pad;
   unsigned long long n_paths;  // width * height * spp
   unsigned long long seq;      // admission order
   float4* sum;       // per-pixel radiance sums
@@ -179,7 +181,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
   // table entry e belongs to lane e % lanes: only that lane's kernels read or write it
   const bool mine = (e % lanes) == lane;
   const unsigned long long st0 = mine ? started[e] : 0ull;
-  const unsigned long long rem64 = mine ? table[e].n_paths - st0 : 0ull;
+  const unsigned long long rem64 = (mine && !table[e].cancelled) ? table[e].n_paths - st0 : 0ull;
   const uint32_t rem = (uint32_t)min(rem64, (unsigned long long)F);
   uint32_t a = 0;
   if (schedule == VP_SCHEDULE_FAIR) {
@@ -489,6 +491,7 @@ struct vp_server {
     cudaGraphExec_t graph_exec = nullptr;
     cudaEvent_t ev_beg[2] = {}, ev_end[2] = {}, ev_step[2] = {};
     unsigned long long* h_done_slot[2] = {};
+    unsigned long long* h_started_slot[2] = {};  // paths started per entry, read with the done counts
     unsigned int* h_status = nullptr;  // [2]
     uint64_t slot_step[2] = {};
     std::deque<int> inflight;  // step slots queued and not yet harvested (oldest first)
@@ -510,6 +513,8 @@ struct vp_server {
     size_t bytes = 0;
     uint64_t admit_step = 0;  // the first step of its lane queued after the admission
     uint32_t lane = 0;
+    bool cancelled = false;
+    uint64_t cancel_step = 0;  // the first step of its lane that sees the cancel flag
   };
   std::vector<Active> active;
   // completed requests whose outputs are still being formed / copied
@@ -537,6 +542,8 @@ struct vp_server {
   std::deque<Pending> pending;
   std::vector<uint64_t> done_ids;
   uint64_t next_id = 0, admitted = 0, completed = 0, paths_completed = 0, iterations = 0;
+  uint64_t cancelled = 0, alloc_failures = 0;
+  uint32_t inject_alloc_failures = 0;  // host fault injection: accumulator allocations left to fail
   uint32_t n_active = 0;
   size_t bytes_fixed = 0, bytes_active = 0;
 };
@@ -566,6 +573,7 @@ void srv_free(vp_server* s) {
       if (L.ev_step[k]) cudaEventDestroy(L.ev_step[k]);
     }
     if (L.h_done_slot[0]) cudaFreeHost(L.h_done_slot[0]);
+    if (L.h_started_slot[0]) cudaFreeHost(L.h_started_slot[0]);
     if (L.h_status) cudaFreeHost(L.h_status);
     if (L.graph_exec) cudaGraphExecDestroy(L.graph_exec);
     if (L.graph) cudaGraphDestroy(L.graph);
@@ -679,7 +687,19 @@ vp_status admit(vp_server* s) {
     vp_server::Active& a = s->active[e];
     const uint32_t n_pix = rq.params.width * rq.params.height;
     float4* sum = nullptr;
-    VP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sum), 16ull * n_pix, st));
+    cudaError_t ae = cudaErrorMemoryAllocation;
+    if (s->inject_alloc_failures)
+      s->inject_alloc_failures -= 1;
+    else
+      ae = cudaMallocAsync(reinterpret_cast<void**>(&sum), 16ull * n_pix, st);
+    if (ae != cudaSuccess) {
+      if (ae != cudaErrorMemoryAllocation) return cuda_fail(ae, "cudaMallocAsync");
+      (void)cudaGetLastError();  // not sticky: the request stays queued
+      s->alloc_failures += 1;
+      if (s->n_active == 0)  // nothing admitted would release memory
+        return fail(VP_ERROR_OUT_OF_MEMORY, "request accumulator: device out of memory with no request admitted");
+      break;  // wait for the admitted requests to release theirs
+    }
     VP_CUDA(cudaMemsetAsync(sum, 0, 16ull * n_pix, st));
     VP_CUDA(cudaMemsetAsync(s->d_done + e, 0, sizeof(unsigned long long), st));
     VP_CUDA(cudaMemsetAsync(s->d_started + e, 0, sizeof(unsigned long long), st));
@@ -749,6 +769,7 @@ vp_status harvest(vp_server* s, uint32_t l, int slot) {
   L.busy_ms += ms;
   const uint32_t R = s->cfg.max_requests, nl = (uint32_t)s->lanes.size();
   const unsigned long long* done = L.h_done_slot[slot];
+  const unsigned long long* started = L.h_started_slot[slot];
   vp_server::OutBatch batch{};
   struct Copy {
     float4* tmp;
@@ -758,7 +779,20 @@ vp_status harvest(vp_server* s, uint32_t l, int slot) {
   std::vector<Copy> copies;
   for (uint32_t e = l; e < R; e += nl) {  // the lane's entries
     vp_server::Active& a = s->active[e];
-    if (!a.used || a.admit_step > L.slot_step[slot] || done[e] < a.n_paths) continue;
+    if (!a.used || a.admit_step > L.slot_step[slot]) continue;
+    if (a.cancelled) {
+      // released once a step that saw the flag ends with every started path finished
+      if (L.slot_step[slot] < a.cancel_step || done[e] < started[e]) continue;
+      VP_CUDA(cudaFreeAsync(a.sum, st));
+      s->bytes_active -= a.bytes;
+      s->n_active -= 1;
+      L.entries -= 1;
+      L.load -= a.n_paths;
+      a = vp_server::Active{};
+      s->n_entries -= 1;
+      continue;
+    }
+    if (done[e] < a.n_paths) continue;
     const float inv = 1.0f / (float)a.spp;
     const unsigned nb = (a.n_pix + 255u) / 256u;
     vp_server::Delivery d{a.id, a.n_paths, nullptr, nullptr, 16ull * a.n_pix, 0, a.bytes};
@@ -905,9 +939,13 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
       chk(cudaEventCreateWithFlags(&L.ev_step[k], cudaEventDisableTiming));
     }
     chk(cudaMallocHost(&L.h_done_slot[0], 2ull * R * sizeof(unsigned long long)));
+    chk(cudaMallocHost(&L.h_started_slot[0], 2ull * R * sizeof(unsigned long long)));
     chk(cudaMallocHost(&L.h_status, 2 * sizeof(unsigned int)));
     chk(cudaMalloc(&L.path_mem, slot_bytes));
-    if (e == cudaSuccess) L.h_done_slot[1] = L.h_done_slot[0] + R;
+    if (e == cudaSuccess) {
+      L.h_done_slot[1] = L.h_done_slot[0] + R;
+      L.h_started_slot[1] = L.h_started_slot[0] + R;
+    }
   }
   if (e != cudaSuccess) {
     srv_free(s);
@@ -1023,6 +1061,8 @@ vp_status vp_server_step(vp_server* s, uint32_t* completed) {
     VP_CUDA(cudaEventRecord(L.ev_end[slot], st));
     VP_CUDA(cudaMemcpyAsync(L.h_done_slot[slot], s->d_done, s->cfg.max_requests * sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, st));
+    VP_CUDA(cudaMemcpyAsync(L.h_started_slot[slot], s->d_started, s->cfg.max_requests * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
     VP_CUDA(cudaMemcpyAsync(L.h_status + slot, &s->ctx->counters->status, sizeof(unsigned int),
                             cudaMemcpyDeviceToHost, st));
     VP_CUDA(cudaEventRecord(L.ev_step[slot], st));
@@ -1050,6 +1090,38 @@ vp_status vp_server_step(vp_server* s, uint32_t* completed) {
   return VP_OK;
 }
 
+vp_status vp_server_cancel(vp_server* s, uint64_t request_id) {
+  if (!s) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+    if (it->id == request_id) {
+      s->pending.erase(it);
+      s->cancelled += 1;
+      return VP_OK;
+    }
+  for (uint32_t e = 0; e < s->cfg.max_requests; ++e) {
+    vp_server::Active& a = s->active[e];
+    if (!a.used || a.id != request_id) continue;
+    if (a.cancelled) return fail(VP_ERROR_INVALID_ARGUMENT, "request already cancelled");
+    VP_CUDA(cudaSetDevice(s->ctx->device));
+    vp_server::Lane& L = s->lanes[a.lane];
+    // stream-ordered: the lane's next queued step is the first whose advance sees the flag
+    s->h_table[e].cancelled = 1u;
+    VP_CUDA(cudaMemcpyAsync(&s->d_table[e].cancelled, &s->h_table[e].cancelled, sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, L.st));
+    a.cancelled = true;
+    a.cancel_step = L.step_no;
+    s->cancelled += 1;
+    return VP_OK;
+  }
+  return fail(VP_ERROR_INVALID_ARGUMENT, "unknown request id, or the request has already finished");
+}
+
+vp_status vp_server_inject_alloc_failures(vp_server* s, uint32_t n) {
+  if (!s) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
+  s->inject_alloc_failures = n;
+  return VP_OK;
+}
+
 vp_status vp_server_poll(vp_server* s, uint64_t* ids, uint32_t cap, uint32_t* n) {
   if (!s || !n || (cap && !ids)) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
   const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done_ids.size());
@@ -1070,6 +1142,8 @@ vp_status vp_server_get_stats(vp_server* s, vp_server_stats* out) {
   out->active = s->n_active;
   out->pending = (uint32_t)s->pending.size();
   out->bytes_in_use = s->bytes_fixed + s->bytes_active;
+  out->cancelled = s->cancelled;
+  out->alloc_failures = s->alloc_failures;
   for (const auto& L : s->lanes) out->device_ms = std::max(out->device_ms, L.busy_ms);  // the busiest lane
   return VP_OK;
 }

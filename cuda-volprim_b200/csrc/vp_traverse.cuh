@@ -104,8 +104,24 @@ struct WarpSmem {
   uint32_t* hb_idx;
   float *hb_tc, *hb_rw, *hb_d2, *hb_tin, *hb_tout, *hb_icf;
   int hit_cap;
-  uint32_t st_cap;  // stack entries
+  uint32_t st_cap;     // stack entries
+  bool root_staged;    // the BVH32 root's child boxes sit at the start of dynamic shared memory
 };
+
+// VP_STAGE_ROOT: the wavefront traversal kernels copy the BVH32 root (which every query visits
+// first) into shared memory once per block and read it from there instead of through L1.
+#ifndef VP_STAGE_ROOT
+#define VP_STAGE_ROOT 0
+#endif
+constexpr size_t kRootStageBytes = VP_STAGE_ROOT ? 64u * sizeof(float4) : 0u;
+extern __shared__ __align__(16) unsigned char vp_dyn_smem[];  // every kernel's dynamic shared memory
+
+// All threads of the block call it, before any warp traverses.
+__device__ __forceinline__ void stage_root(const float4* wide, uint32_t root) {
+  float4* r = reinterpret_cast<float4*>(vp_dyn_smem);
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) r[i] = __ldg(wide + (size_t)root * 64u + i);
+  __syncthreads();
+}
 
 __host__ __device__ __forceinline__ size_t warp_smem_bytes(uint32_t stack_cap, int hit_cap) {
   return (size_t)stack_cap * 8u + (size_t)hit_cap * 7u * 4u;
@@ -125,6 +141,7 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, uint32_t stack_ca
   w.hb_icf = hb + 6 * hit_cap;
   w.hit_cap = hit_cap;
   w.st_cap = stack_cap;
+  w.root_staged = false;
   return w;
 }
 
@@ -436,9 +453,16 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
         ws.nodes++;
         ws.kind_nodes[kKind]++;
       }
-      const float4* node = S.wide + (size_t)ref * 64u;
-      const float4 lo = __ldg(node + lane);
-      const float4 hi = __ldg(node + 32 + lane);
+      float4 lo, hi;
+      if (VP_STAGE_ROOT && W.root_staged && ref == S.wide_root) {
+        const float4* r = reinterpret_cast<const float4*>(vp_dyn_smem);
+        lo = r[lane];
+        hi = r[32 + lane];
+      } else {
+        const float4* node = S.wide + (size_t)ref * 64u;
+        lo = __ldg(node + lane);
+        hi = __ldg(node + 32 + lane);
+      }
       const uint32_t cref = __float_as_uint(lo.w);
       float tnear = 0.f;
       const bool hit = (cref != kEmptyRef) && slab<kKind == kArgmin>(rb, lo, hi, 0.0f, t_hi, tnear);

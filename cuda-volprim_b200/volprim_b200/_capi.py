@@ -209,6 +209,8 @@ class vp_server_stats(C.Structure):
         ("pending", C.c_uint32),
         ("bytes_in_use", C.c_uint64),
         ("device_ms", C.c_double),
+        ("cancelled", C.c_uint64),
+        ("alloc_failures", C.c_uint64),
     ]
 
 
@@ -259,6 +261,8 @@ SIGNATURES = {
     "vp_server_add_scene": [P, P, P, C.POINTER(C.c_uint32)],
     "vp_server_submit": [P, C.POINTER(vp_request), C.POINTER(C.c_uint64)],
     "vp_server_step": [P, C.POINTER(C.c_uint32)],
+    "vp_server_cancel": [P, C.c_uint64],
+    "vp_server_inject_alloc_failures": [P, C.c_uint32],
     "vp_server_poll": [P, C.POINTER(C.c_uint64), C.c_uint32, C.POINTER(C.c_uint32)],
     "vp_server_get_stats": [P, C.POINTER(vp_server_stats)],
     "vp_server_destroy": [P],

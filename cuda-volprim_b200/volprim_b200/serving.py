@@ -77,6 +77,16 @@ class Server:
         check(lib.vp_server_step(self.handle, C.byref(n)))
         return n.value
 
+    def cancel(self, request_id: int) -> None:
+        """vp_server_cancel: the request is never delivered and its output is never written."""
+        check(lib.vp_server_cancel(self.handle, C.c_uint64(request_id)))
+        self._outs.pop(request_id, None)
+
+    def inject_alloc_failures(self, n: int) -> None:
+        """vp_server_inject_alloc_failures: the next n accumulator allocations fail (host-side
+        fault injection for tests)."""
+        check(lib.vp_server_inject_alloc_failures(self.handle, C.c_uint32(n)))
+
     def poll(self) -> list:
         ids = (C.c_uint64 * 1024)()
         out = []

@@ -501,6 +501,9 @@ typedef struct vp_server_stats {
   uint64_t bytes_in_use;         /* scenes + slots + active accumulators (the budget's measure) */
   double device_ms;              /* device time of the iterations run so far (CUDA events; with
                                     several lanes, the busiest lane's) */
+  uint64_t cancelled;            /* requests ended by vp_server_cancel (never delivered) */
+  uint64_t alloc_failures;       /* accumulator allocations that failed (device out of memory,
+                                    or injected by vp_server_inject_alloc_failures) */
 } vp_server_stats;
 
 vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_server** out);
@@ -518,9 +521,24 @@ vp_status vp_server_submit(vp_server* server, const vp_request* request, uint64_
  * land; a call with nothing left on the GPU waits for them.  *completed = requests delivered by
  * this call. */
 vp_status vp_server_step(vp_server* server, uint32_t* completed);
+/* Ends a request that has not been delivered.  A queued request leaves the queue.  An admitted
+ * request starts no further paths from the next queued step on; its paths already in flight run
+ * to their end, and then its table entry, accumulator and share of the memory budget are released
+ * by a later vp_server_step.  A cancelled request never appears in vp_server_poll and its output
+ * buffer is never written.  VP_ERROR_INVALID_ARGUMENT for an id that was never submitted, is
+ * already cancelled, or that a vp_server_step has already found finished (its output is being
+ * or has been delivered). */
+vp_status vp_server_cancel(vp_server* server, uint64_t request_id);
 /* Ids of requests completed since the last call (up to cap; the rest stay queued). */
 vp_status vp_server_poll(vp_server* server, uint64_t* ids, uint32_t cap, uint32_t* n);
 vp_status vp_server_get_stats(vp_server* server, vp_server_stats* out);
+/* Fault injection on the host, for tests: the next n accumulator allocations of admissions fail
+ * as a device out-of-memory would, without calling the allocator.  A failed allocation (injected
+ * or real) leaves the request at the head of the queue and ends this step's admissions; while
+ * other requests are admitted it waits for the memory they release.  When none is admitted,
+ * vp_server_step returns VP_ERROR_OUT_OF_MEMORY, with the request still queued and the server
+ * usable: a later vp_server_step retries it, or vp_server_cancel removes it. */
+vp_status vp_server_inject_alloc_failures(vp_server* server, uint32_t n);
 vp_status vp_server_destroy(vp_server* server);
 
 /* ---------------------------------------------------------------------------------------- */

@@ -223,3 +223,103 @@ def test_invalid_requests_raise(vp_ctx, world):
     with pytest.raises(vp.VpError, match="memory budget"):
         small.submit(0, r.camera, r.config)
     small.close()
+
+
+# -- host-side faults: cancellation and failed accumulator allocations ---------------------------
+
+VP_ERROR_OUT_OF_MEMORY = -3
+
+
+def solo_image(vp_ctx, world, r):
+    solo = new_server(vp_ctx, world)
+    sid = solo.submit(r.scene_id, r.camera, r.config)
+    drain(solo)
+    img = solo.result(sid)
+    solo.close()
+    return img
+
+
+def test_cancel_queued_and_running_requests(vp_ctx, world):
+    """A request cancelled while queued and one cancelled while its paths run: neither is ever
+    delivered nor writes its output, the others finish with their solo results, and the table
+    entries and memory come back."""
+    reqs = make_trace(17, 3, rate=0.0, n_scenes=2, resolutions=(96,), spps=(16,))
+    srv = new_server(vp_ctx, world, iterations_per_step=2)
+    fixed = srv.stats()["bytes_in_use"]
+    shape = (96, 96, 4)
+    outs = [np.full(shape, -7.0, np.float32) for _ in reqs]
+    ids = [srv.submit(r.scene_id, r.camera, r.config, out=o) for r, o in zip(reqs, outs)]
+    srv.cancel(ids[2])  # still queued
+    assert srv.stats()["pending"] == 2
+    srv.step()
+    srv.step()
+    assert srv.stats()["active"] == 2
+    srv.cancel(ids[0])  # admitted, paths in flight
+    with pytest.raises(vp.VpError, match="already cancelled"):
+        srv.cancel(ids[0])
+    done = drain(srv)
+    assert done == [ids[1]]
+    st = srv.stats()
+    assert st["cancelled"] == 2 and st["completed"] == 1 and st["active"] == 0
+    assert st["bytes_in_use"] == fixed
+    assert np.all(outs[0] == -7.0) and np.all(outs[2] == -7.0)
+    assert np.all(close(srv.result(ids[1]), solo_image(vp_ctx, world, reqs[1])))
+    for rid in (ids[1], ids[0], 12345):  # delivered, released after cancel, never submitted
+        with pytest.raises(vp.VpError):
+            srv.cancel(rid)
+    # the freed entries and memory serve new requests
+    rid = srv.submit(reqs[0].scene_id, reqs[0].camera, reqs[0].config)
+    assert drain(srv) == [rid]
+    assert np.all(close(srv.result(rid), solo_image(vp_ctx, world, reqs[0])))
+    srv.close()
+
+
+def test_cancel_releases_the_memory_budget(vp_ctx, world):
+    probe = new_server(vp_ctx, world)
+    fixed = probe.stats()["bytes_in_use"]
+    probe.close()
+    reqs = make_trace(19, 2, rate=0.0, n_scenes=2, resolutions=(64,), spps=(64,))
+    per = 64 * 64 * 16 * 2
+    srv = new_server(vp_ctx, world, memory_budget_bytes=fixed + per, iterations_per_step=2)
+    ids = [srv.submit(r.scene_id, r.camera, r.config) for r in reqs]
+    srv.step()
+    assert srv.stats()["active"] == 1 and srv.stats()["pending"] == 1
+    srv.cancel(ids[0])
+    assert drain(srv) == [ids[1]]
+    assert np.all(close(srv.result(ids[1]), solo_image(vp_ctx, world, reqs[1])))
+    srv.close()
+
+
+def test_failed_accumulator_allocation(vp_ctx, world):
+    """Injected on the host: with nothing admitted the step reports out of memory and keeps the
+    request queued; with a request admitted the new one waits; either way the server stays usable
+    and the results are the solo ones."""
+    reqs = requests(23, 3)
+    srv = new_server(vp_ctx, world)
+    srv.inject_alloc_failures(1)
+    a = srv.submit(reqs[0].scene_id, reqs[0].camera, reqs[0].config)
+    with pytest.raises(vp.VpError) as ei:
+        srv.step()
+    assert ei.value.status == VP_ERROR_OUT_OF_MEMORY
+    st = srv.stats()
+    assert st["alloc_failures"] == 1 and st["pending"] == 1 and st["active"] == 0
+    srv.step()  # the retry succeeds
+    assert srv.stats()["active"] == 1
+    srv.inject_alloc_failures(1)
+    b = srv.submit(reqs[1].scene_id, reqs[1].camera, reqs[1].config)
+    srv.step()  # a is admitted: b waits instead of failing the step
+    st = srv.stats()
+    assert st["alloc_failures"] == 2 and st["pending"] == 1
+    assert sorted(drain(srv)) == sorted([a, b])
+    for rid, r in ((a, reqs[0]), (b, reqs[1])):
+        assert np.all(close(srv.result(rid), solo_image(vp_ctx, world, r)))
+    # a request stuck behind failing allocations can be cancelled
+    srv.inject_alloc_failures(3)
+    c = srv.submit(reqs[2].scene_id, reqs[2].camera, reqs[2].config)
+    with pytest.raises(vp.VpError):
+        srv.step()
+    srv.cancel(c)
+    srv.inject_alloc_failures(0)
+    st = srv.stats()
+    assert st["pending"] == 0 and st["cancelled"] == 1 and st["completed"] == 2
+    srv.close()
