@@ -60,29 +60,6 @@ __host__ __device__ inline uint32_t wide_leaf_count(uint32_t r) { return ((r >> 
 // The argmin traversal pops best-first while its stack holds at most this many entries.
 constexpr uint32_t kArgminBestFirstStack = 64;
 
-// Per-path and per-ray state (gigabytes for a full batch) is read or written once per stage, so
-// those accesses are marked evict-first (cache-streaming) and leave L2 to the scene, which every
-// query of every stage re-reads.
-#ifndef VP_STREAM_HINTS
-#define VP_STREAM_HINTS 1
-#endif
-template <class T>
-__device__ __forceinline__ T ld_stream(const T* p) {
-#if VP_STREAM_HINTS
-  return __ldcs(p);
-#else
-  return *p;
-#endif
-}
-template <class T>
-__device__ __forceinline__ void st_stream(T* p, T v) {
-#if VP_STREAM_HINTS
-  __stcs(p, v);
-#else
-  *p = v;
-#endif
-}
-
 // Device error words (raised instead of trapping; read back by the host).
 constexpr uint32_t kStatusStackOverflow = 1u;
 constexpr uint32_t kStatusBadInput = 2u;

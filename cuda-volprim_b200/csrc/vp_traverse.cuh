@@ -109,9 +109,10 @@ struct WarpSmem {
 };
 
 // VP_STAGE_ROOT: the wavefront traversal kernels copy the BVH32 root (which every query visits
-// first) into shared memory once per block and read it from there instead of through L1.
+// first) into shared memory once per block and read it from there instead of through L1
+// (measured on the 500k showcase: extend -1.7%, shadow -0.5% per step).
 #ifndef VP_STAGE_ROOT
-#define VP_STAGE_ROOT 0
+#define VP_STAGE_ROOT 1
 #endif
 constexpr size_t kRootStageBytes = VP_STAGE_ROOT ? 64u * sizeof(float4) : 0u;
 extern __shared__ __align__(16) unsigned char vp_dyn_smem[];  // every kernel's dynamic shared memory

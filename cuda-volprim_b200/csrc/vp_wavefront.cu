@@ -58,19 +58,18 @@ __device__ __forceinline__ uint32_t meta_bounce(uint32_t m) { return m & 0xFFFFu
 __device__ __forceinline__ uint32_t meta_nshadow(uint32_t m) { return (m >> 16) & 3u; }
 
 __device__ __forceinline__ void store_path(const WfBuffers& b, uint32_t p, const PathState& s) {
-  st_stream(b.o4 + p, make_float4(s.o.x, s.o.y, s.o.z, 0.f));
-  st_stream(b.d4 + p, make_float4(s.d.x, s.d.y, s.d.z, 0.f));
-  st_stream(b.thr4 + p, make_float4(s.thr.x, s.thr.y, s.thr.z, 0.f));
-  st_stream(b.rad4 + p, make_float4(s.rad.x, s.rad.y, s.rad.z, 0.f));
-  st_stream(b.rng4 + p, make_uint4((uint32_t)s.rng.state, (uint32_t)(s.rng.state >> 32), (uint32_t)s.rng.inc,
-                                   (uint32_t)(s.rng.inc >> 32)));
+  b.o4[p] = make_float4(s.o.x, s.o.y, s.o.z, 0.f);
+  b.d4[p] = make_float4(s.d.x, s.d.y, s.d.z, 0.f);
+  b.thr4[p] = make_float4(s.thr.x, s.thr.y, s.thr.z, 0.f);
+  b.rad4[p] = make_float4(s.rad.x, s.rad.y, s.rad.z, 0.f);
+  b.rng4[p] = make_uint4((uint32_t)s.rng.state, (uint32_t)(s.rng.state >> 32), (uint32_t)s.rng.inc,
+                         (uint32_t)(s.rng.inc >> 32));
 }
 
 __device__ __forceinline__ PathState load_path(const WfBuffers& b, uint32_t p, uint32_t bounce) {
   PathState s;
-  const float4 o = ld_stream(b.o4 + p), d = ld_stream(b.d4 + p), t = ld_stream(b.thr4 + p),
-               r = ld_stream(b.rad4 + p);
-  const uint4 g = ld_stream(b.rng4 + p);
+  const float4 o = b.o4[p], d = b.d4[p], t = b.thr4[p], r = b.rad4[p];
+  const uint4 g = b.rng4[p];
   s.o = f3(o.x, o.y, o.z);
   s.d = f3(d.x, d.y, d.z);
   s.thr = f3(t.x, t.y, t.z);
@@ -157,9 +156,9 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
     item = __shfl_sync(kFull, item, 0);
     if (item >= n) break;
     const uint32_t p = __ldg(q + item);
-    const float4 o = ld_stream(b.o4 + p), d = ld_stream(b.d4 + p);
-    const uint2 k2 = ld_stream(b.key2 + p);
-    const uint32_t bounce = meta_bounce(ld_stream(b.meta + p));
+    const float4 o = b.o4[p], d = b.d4[p];
+    const uint2 k2 = b.key2[p];
+    const uint32_t bounce = meta_bounce(b.meta[p]);
     const float3 of = f3(o.x, o.y, o.z), df = f3(d.x, d.y, d.z);
     float tstar = kInf;
     ScatterAlbedo sa;
@@ -175,8 +174,8 @@ __global__ void __launch_bounds__(256, VP_WF_MIN_BLOCKS) k_wf_extend(SceneView S
     }
     ++bounces;
     if (lane == 0) {
-      st_stream(b.alb4 + p, make_float4(albedo.x, albedo.y, albedo.z, tstar));
-      st_stream(b.sg + p, tstar < kInf ? sa.gauss : kNoGauss);
+      b.alb4[p] = make_float4(albedo.x, albedo.y, albedo.z, tstar);
+      b.sg[p] = tstar < kInf ? sa.gauss : kNoGauss;
     }
     if (status) break;
   }
@@ -221,11 +220,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(SceneView S, EnvView E, Params
     bool alive = false;
     if (valid) {
       p = q[i];
-      PathState s = load_path(b, p, meta_bounce(ld_stream(b.meta + p)));
-      const float4 a = ld_stream(b.alb4 + p);
+      PathState s = load_path(b, p, meta_bounce(b.meta[p]));
+      const float4 a = b.alb4[p];
       const bool scattered = a.w < kInf;
       ShadowSet sh;
-      alive = shade_bounce(E, P, s, scattered, a.w, f3(a.x, a.y, a.z), sh, ld_stream(b.sg + p));
+      alive = shade_bounce(E, P, s, scattered, a.w, f3(a.x, a.y, a.z), sh, b.sg[p]);
       ns = sh.n;
       for (int k = 0; k < sh.n; ++k) {
         float seed_tau = -1.0f;  // no seed
@@ -234,18 +233,18 @@ __global__ void __launch_bounds__(256) k_wf_shade(SceneView S, EnvView E, Params
                                 : seed_chord_tau<false>(S, sh.seed[k], sh.o[k], sh.d[k]);
         const bool opaque_k = seed_tau >= kMaxOpticalDepth;
         // .w of the origin: the seed's optical depth for the query, or T = 0 already
-        st_stream(b.so4 + 3u * p + k, make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, opaque_k ? 0.0f : seed_tau));
-        st_stream(b.sd4 + 3u * p + k, make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k])));
-        st_stream(b.sw4 + 3u * p + k, make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f));
+        b.so4[3u * p + k] = make_float4(sh.o[k].x, sh.o[k].y, sh.o[k].z, opaque_k ? 0.0f : seed_tau);
+        b.sd4[3u * p + k] = make_float4(sh.d[k].x, sh.d[k].y, sh.d[k].z, __uint_as_float(sh.seed[k]));
+        b.sw4[3u * p + k] = make_float4(sh.w[k].x, sh.w[k].y, sh.w[k].z, 0.f);
         if (!opaque_k) queued |= 1u << k;
         else opaque += 1;
       }
       if (alive) {
         const uint64_t key = draw_bounce_key(s.rng);
-        st_stream(b.key2 + p, make_uint2((uint32_t)key, (uint32_t)(key >> 32)));
+        b.key2[p] = make_uint2((uint32_t)key, (uint32_t)(key >> 32));
       }
       store_path(b, p, s);
-      st_stream(b.meta + p, (s.bounce & 0xFFFFu) | ((uint32_t)sh.n << 16) | (alive ? kAliveBit : 0u));
+      b.meta[p] = (s.bounce & 0xFFFFu) | ((uint32_t)sh.n << 16) | (alive ? kAliveBit : 0u);
     }
     shadows += (unsigned)ns;
     uint32_t slot = queue_reserve(b.ctr + 2, (uint32_t)__popc(queued));
@@ -288,11 +287,11 @@ __global__ void __launch_bounds__(256, kAcc ? VP_WF_MIN_BLOCKS : VP_WF_SHADOW_MI
     if (lane == 0) item = atomicAdd(work, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= n) break;
-    const uint32_t slot = ld_stream(b.qs + item);
-    const float4 o = ld_stream(b.so4 + slot), d = ld_stream(b.sd4 + slot);
+    const uint32_t slot = __ldg(b.qs + item);
+    const float4 o = b.so4[slot], d = b.sd4[slot];
     const float tau = warp_ray_query<kAcc, kTau>(S, W, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), 0ull, status, ws,
                                                  measure, nullptr, __float_as_uint(d.w), o.w);
-    if (lane == 0) st_stream(&b.so4[slot].w, tau >= kMaxOpticalDepth ? 0.0f : expf(-tau));
+    if (lane == 0) b.so4[slot].w = tau >= kMaxOpticalDepth ? 0.0f : expf(-tau);
     if (status) break;
   }
   if (lane == 0) {
@@ -317,16 +316,16 @@ __global__ void __launch_bounds__(256) k_wf_gather(ParamsView P, WfBuffers b, co
   const uint32_t n = *count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t p = q[i];
-    const uint32_t m = ld_stream(b.meta + p);
+    const uint32_t m = b.meta[p];
     const int ns = (int)meta_nshadow(m);
-    const float4 r = ld_stream(b.rad4 + p);
+    const float4 r = b.rad4[p];
     float3 rad = f3(r.x, r.y, r.z);
     for (int k = 0; k < ns; ++k) {
-      const float4 w = ld_stream(b.sw4 + 3u * p + k);
-      rad = add(rad, mul(f3(w.x, w.y, w.z), ld_stream(&b.so4[3u * p + k].w)));
+      const float4 w = b.sw4[3u * p + k];
+      rad = add(rad, mul(f3(w.x, w.y, w.z), b.so4[3u * p + k].w));
     }
     if (m & kAliveBit) {
-      st_stream(b.rad4 + p, make_float4(rad.x, rad.y, rad.z, 0.f));
+      b.rad4[p] = make_float4(rad.x, rad.y, rad.z, 0.f);
     } else {
       const float3 L = finalize_sample(P, rad);
       b.L4[p] = make_float4(L.x, L.y, L.z, 0.f);
