@@ -66,6 +66,7 @@ struct SrvCtl {  // device control block of the iteration
   uint32_t regen_from;  // free-stack index of the first slot they take
   uint32_t survivors;   // paths carried over from the previous iteration
   uint32_t ctr[8];      // [0] paths this iteration, [1] next, [2] shadow queries, [3..4] work heads
+  unsigned long long total_started;  // paths the lane has started (the clock of SRPT aging)
 };
 
 struct SrvPaths {  // per path slot
@@ -159,12 +160,15 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 //                     still has), then what is left over in table order;
 //   VP_SCHEDULE_SRPT  fewest unstarted paths first (ties in admission order), with a fraction
 //                     (srpt_reserve, default half) of the free slots kept for the oldest request
-//                     that still has unstarted paths.
+//                     that still has unstarted paths; with srpt_aging > 0 the key is the unstarted
+//                     paths minus srpt_aging x the paths the lane started since the request's first
+//                     iteration here (age_base, set on that iteration).
 // Writes the per-entry offsets of this iteration's new paths (alloc_off, size R + 1) and their
 // first pixel-major path index (alloc_start).
 __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, unsigned long long* __restrict__ started,
-                              uint32_t* __restrict__ alloc_off, unsigned long long* __restrict__ alloc_start,
-                              int schedule, float srpt_reserve, uint32_t lane, uint32_t lanes) {
+                              unsigned long long* __restrict__ age_base, uint32_t* __restrict__ alloc_off,
+                              unsigned long long* __restrict__ alloc_start, int schedule, float srpt_reserve,
+                              float srpt_aging, uint32_t lane, uint32_t lanes) {
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t s_free, s_surv;
   __shared__ unsigned long long s_key[kMaxRequests], s_seq[kMaxRequests];
@@ -200,7 +204,18 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
   } else {
     // rank every entry by its key, then hand out the free slots in rank order
     const unsigned long long seq = mine ? table[e].seq : ~0ull;
-    const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? rem64 : seq);
+    unsigned long long srpt_key = rem64;
+    if (schedule == VP_SCHEDULE_SRPT && mine && srpt_aging > 0.0f) {
+      const unsigned long long now = c->total_started;
+      unsigned long long base = age_base[e];
+      if (base == ~0ull) {  // the request's first iteration in this lane
+        base = now;
+        age_base[e] = now;
+      }
+      const unsigned long long credit = (unsigned long long)((double)srpt_aging * (double)(now - base));
+      srpt_key = rem64 > credit ? rem64 - credit : 0ull;
+    }
+    const unsigned long long key = rem == 0 ? ~0ull : (schedule == VP_SCHEDULE_SRPT ? srpt_key : seq);
     s_key[e] = key;
     s_seq[e] = seq;
     // SRPT: a fraction of the free slots stays with the oldest request that has unstarted paths,
@@ -251,6 +266,7 @@ __global__ void k_srv_advance(SrvCtl* c, const SrvRequest* __restrict__ table, u
     c->free_count = F - m;
     c->ctr[0] = s_surv + m;
     c->ctr[1] = c->ctr[2] = c->ctr[3] = c->ctr[4] = 0u;
+    c->total_started += m;
   }
 }
 
@@ -469,6 +485,8 @@ struct vp_server {
   SrvRequest* d_table = nullptr;
   unsigned long long* d_done = nullptr;
   unsigned long long* d_started = nullptr;      // paths started per table entry
+  unsigned long long* d_age_base = nullptr;     // SRPT aging: the lane's started-path clock at the
+                                                // entry's first iteration (~0 until then)
   // pinned staging of the table entries (each reaches the device by a stream-ordered copy)
   SrvRequest* h_table = nullptr;
   int ext_blocks = 0, shd_blocks = 0, thr_blocks = 0;
@@ -593,6 +611,7 @@ void srv_free(vp_server* s) {
   cudaFree(s->d_table);
   cudaFree(s->d_done);
   cudaFree(s->d_started);
+  cudaFree(s->d_age_base);
   cudaFreeHost(s->h_table);
   delete s;
 }
@@ -605,8 +624,8 @@ vp_status enqueue_iteration(vp_server* s, uint32_t l, bool even) {
   uint32_t* qcur = even ? L.paths.qa : L.paths.qb;
   uint32_t* qnext = even ? L.paths.qb : L.paths.qa;
   Counters* ctr = s->ctx->counters;
-  k_srv_advance<<<1, R, 0, st>>>(L.d_ctl, s->d_table, s->d_started, L.d_alloc_off, L.d_alloc_start,
-                                 s->cfg.schedule, s->cfg.srpt_reserve, l, nl);
+  k_srv_advance<<<1, R, 0, st>>>(L.d_ctl, s->d_table, s->d_started, s->d_age_base, L.d_alloc_off,
+                                 L.d_alloc_start, s->cfg.schedule, s->cfg.srpt_reserve, s->cfg.srpt_aging, l, nl);
   k_srv_regen<<<s->thr_blocks, 256, 0, st>>>(L.d_ctl, s->d_table, L.d_alloc_off, L.d_alloc_start, R, L.paths, qcur);
   if (s->accurate)
     k_srv_extend<true><<<s->ext_blocks, 256, s->smem_ext, st>>>(s->d_scenes, s->d_table, L.paths, qcur, L.d_ctl,
@@ -703,6 +722,7 @@ vp_status admit(vp_server* s) {
     VP_CUDA(cudaMemsetAsync(sum, 0, 16ull * n_pix, st));
     VP_CUDA(cudaMemsetAsync(s->d_done + e, 0, sizeof(unsigned long long), st));
     VP_CUDA(cudaMemsetAsync(s->d_started + e, 0, sizeof(unsigned long long), st));
+    VP_CUDA(cudaMemsetAsync(s->d_age_base + e, 0xFF, sizeof(unsigned long long), st));
     SrvRequest& t = s->h_table[e];
     std::memset(&t, 0, sizeof(t));
     build_camera(rq.camera, rq.params.width, rq.params.height, t.cam);
@@ -891,6 +911,10 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
     return fail(VP_ERROR_INVALID_ARGUMENT, "srpt_reserve above 1");
   }
   c.iterations_per_step = (c.iterations_per_step + 1u) & ~1u;
+  if (!(c.srpt_aging >= 0.0f) || c.srpt_aging > 1e6f) {
+    srv_free(s);
+    return fail(VP_ERROR_INVALID_ARGUMENT, "srpt_aging must be in [0, 1e6]");
+  }
   if (c.path_slots > (1u << 28)) {
     srv_free(s);
     return fail(VP_ERROR_LIMIT, "path_slots above 2^28");
@@ -918,6 +942,7 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   chk(cudaMalloc(&s->d_table, R * sizeof(SrvRequest)));
   chk(cudaMalloc(&s->d_done, R * sizeof(unsigned long long)));
   chk(cudaMalloc(&s->d_started, R * 8ull));
+  chk(cudaMalloc(&s->d_age_base, R * 8ull));
   chk(cudaMallocHost(&s->h_table, R * sizeof(SrvRequest)));
   chk(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
   const size_t slot_bytes = (size_t)P * kSlotBytes + 32 * 256;
@@ -975,11 +1000,12 @@ vp_status vp_server_create(vp_context* ctx, const vp_server_config* config, vp_s
   srv_carve(cur, b.free_stack, P);
   k_srv_init<<<(P + 255) / 256, 256, 0, ctx->stream>>>(L.d_ctl, b.free_stack, P);
   }
-  s->bytes_fixed = NL * slot_bytes + R * (sizeof(SrvRequest) + 28ull);
+  s->bytes_fixed = NL * slot_bytes + R * (sizeof(SrvRequest) + 36ull);
   cudaStream_t st = ctx->stream;
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, R * sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_started, 0, R * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_age_base, 0xFF, R * sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_table, 0, R * sizeof(SrvRequest), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, sizeof(Counters), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

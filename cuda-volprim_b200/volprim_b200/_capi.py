@@ -184,6 +184,7 @@ class vp_server_config(C.Structure):
         ("schedule", C.c_int32),
         ("srpt_reserve", C.c_float),
         ("lanes", C.c_uint32),
+        ("srpt_aging", C.c_float),
     ]
 
 

@@ -27,7 +27,8 @@ class Server:
 
     def __init__(self, ctx: Context, memory_budget_bytes: int = 150 * 10 ** 9, path_slots: int = 1 << 18,
                  max_requests: int = 256, iterations_per_step: int = 4, precision: str = "fast",
-                 use_graph: bool = True, schedule: str = "fifo", srpt_reserve: float = 0.5, lanes: int = 1):
+                 use_graph: bool = True, schedule: str = "fifo", srpt_reserve: float = 0.5, lanes: int = 1,
+                 srpt_aging: float = 0.0):
         c = _capi.vp_server_config()
         c.memory_budget_bytes = int(memory_budget_bytes)
         c.path_slots = int(path_slots)
@@ -38,6 +39,7 @@ class Server:
         c.schedule = {"fifo": 0, "fair": 1, "srpt": 2}[schedule]
         c.srpt_reserve = float(srpt_reserve)
         c.lanes = int(lanes)
+        c.srpt_aging = float(srpt_aging)
         h = C.c_void_p()
         check(lib.vp_server_create(ctx.handle, C.byref(c), C.byref(h)))
         self.handle, self.ctx = h, ctx
@@ -249,6 +251,7 @@ def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, loa
       latency            all `n_requests` with Poisson arrivals at `load` x the offline capacity,
                          served (each schedule) and through the plain per-request loop, on the same
                          arrivals: p50 / p90 / p99 / max of arrival-to-completion wall time.
+    A schedule "srpt/A" is SRPT with srpt_aging A.
     `rate` (requests/s) fixes the arrival rate instead, so runs compare on identical arrivals;
     `capacity_runs` / `plain` switch those runs off.  Returns the figures as a dict."""
     from . import scenes
@@ -258,8 +261,10 @@ def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, loa
     envs = [env] * len(scs)
 
     def server(schedule):
-        srv = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=schedule, path_slots=path_slots,
-                     srpt_reserve=srpt_reserve, lanes=lanes)
+        # "srpt/A": SRPT with srpt_aging A
+        name, _, aging = schedule.partition("/")
+        srv = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=name, path_slots=path_slots,
+                     srpt_reserve=srpt_reserve, lanes=lanes, srpt_aging=float(aging or 0.0))
         for sc in scs:
             srv.add_scene(sc, env)
         return srv
@@ -329,7 +334,7 @@ def main(argv=None) -> None:
     ap.add_argument("--requests", type=int, default=1000)
     ap.add_argument("--capacity-requests", type=int, default=300)
     ap.add_argument("--load", type=float, default=0.8)
-    ap.add_argument("--schedules", default="fifo")
+    ap.add_argument("--schedules", default="fifo", help="comma-separated: fifo, fair, srpt, srpt/AGING")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--slots", type=int, default=1 << 18)

@@ -480,6 +480,10 @@ typedef struct vp_server_config {
                                     path_slots / lanes slots, its own stream and graph; a request
                                     runs in the least-loaded lane, and one lane's kernels fill the
                                     SMs that another lane's leave idle as they drain */
+  float srpt_aging;              /* VP_SCHEDULE_SRPT: a request's key is its unstarted paths minus
+                                    srpt_aging x the paths its lane has started since the request's
+                                    first iteration (at least 0), so a large request that waits
+                                    behind small ones rises in rank (0 = plain SRPT) */
 } vp_server_config;
 
 typedef struct vp_request {

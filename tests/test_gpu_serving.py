@@ -167,6 +167,22 @@ def test_schedules(vp_ctx, world):
             assert np.all(close(a, b)), sched
 
 
+def test_srpt_aging(vp_ctx, world):
+    """SRPT with aging gives the same images as plain SRPT; a negative aging is refused."""
+    reqs = requests(21, 6)
+    out = {}
+    for aging in (0.0, 1.0):
+        srv = new_server(vp_ctx, world, schedule="srpt", srpt_aging=aging, iterations_per_step=2)
+        ids = [srv.submit(r.scene_id, r.camera, r.config) for r in reqs]
+        assert sorted(drain(srv)) == sorted(ids)
+        out[aging] = [srv.result(i) for i in ids]
+        srv.close()
+    for a, b in zip(out[0.0], out[1.0]):
+        assert np.all(close(a, b))
+    with pytest.raises(vp.VpError, match="srpt_aging"):
+        new_server(vp_ctx, world, schedule="srpt", srpt_aging=-1.0)
+
+
 def test_admission_respects_the_memory_budget(vp_ctx, world):
     probe = new_server(vp_ctx, world)
     fixed = probe.stats()["bytes_in_use"]
