@@ -12,12 +12,12 @@
 //
 // Use rules (repeated in include/volprim_b200.h):
 //  * The first call on a device resolves the array's device address (cudaGetSymbolAddress, with
-//    that device current) and caches it for the life of the process; make that first call
-//    before any stream capture.  The cached address belongs to the device's primary context:
+//    that device current) and caches it for the life of the process.  The cached address
+//    belongs to the device's primary context:
 //    like every handle of this library, it does not survive cudaDeviceReset (or a destroyed and
 //    re-created primary context), so reset no device while the library is in use.
 //  * Each call waits for its own work on the context's stream (cudaStreamSynchronize) before it
-//    returns, and reads the status word back to the host.
+//    returns, and reads the status word back to the host, so no call can be stream-captured.
 //  * All calls share the one array, and each call leaves its contents behind: the queue head
 //    and status word are cleared at the start of every call.  Calls whose work overlaps on the
 //    GPU (other streams, other host threads) race on the array and must be serialised by the

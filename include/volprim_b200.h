@@ -361,9 +361,9 @@ vp_status vp_transmittance(vp_scene* scene, const float* origins, const float* d
  * static __device__ array sized for at most 65536 rays (about 1.8 MB), which every GPU that loads
  * the library holds until the process exits.  n > 65536 returns VP_ERROR_LIMIT.  The first call
  * on a device looks up the array's address on that device and keeps it for the life of the
- * process; make that first call before any stream capture, and reset no device
- * (cudaDeviceReset) while the library is in use.  Each call synchronises the context's stream
- * before it returns.  All calls share the array and leave their data in it (the queue head and status word are
+ * process, so reset no device (cudaDeviceReset) while the library is in use.  Each call
+ * synchronises the context's stream before it returns, so no call can be captured into a CUDA
+ * graph.  All calls share the array and leave their data in it (the queue head and status word are
  * cleared at the start of each call): calls whose work overlaps on the GPU race and must be
  * serialised by the caller.  No counterpart in the reference. */
 vp_status vp_transmittance_static(vp_scene* scene, const float* origins, const float* dirs,
