@@ -24,7 +24,12 @@ namespace {
 struct ErrorWords {
   int bad_scale, bad_density, bad_center;  // lowest failing index (INT_MAX = none)
   unsigned int any_albedo;                 // 1 if some albedo component > 0
+  unsigned int opaque_cores;               // Gaussians opaque at their core (vp_tau_order AUTO)
 };
+
+// A Gaussian is "opaque at its core" when the optical depth through its centre along its thinnest
+// direction, M / (2 pi s_mid s_max), is at least this (4 x MAX_OPTICAL_DEPTH).
+constexpr float kOpaqueCoreTau = 4.0f * kMaxOpticalDepth;
 
 __device__ __forceinline__ float clamp_albedo(float v) {
   if (!isfinite(v)) return 0.0f;
@@ -69,6 +74,14 @@ __global__ void k_precompute(uint32_t n, const float* __restrict__ mean,
   if (!isfinite(cx) || !isfinite(cy) || !isfinite(cz) || !isfinite(w) || !isfinite(x) ||
       !isfinite(y) || !isfinite(z))
     atomicMin(&err->bad_center, (int)i);
+  {
+    const float smax = fmaxf(sx, fmaxf(sy, sz)), smin = fminf(sx, fminf(sy, sz));
+    const float smid = sx + sy + sz - smax - smin;
+    const bool core = scale_ok && M >= kOpaqueCoreTau * 6.28318531f * smid * smax;
+    const unsigned am = __activemask();
+    const unsigned cm = __ballot_sync(am, core);
+    if (cm && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(&err->opaque_cores, (unsigned)__popc(cm));
+  }
   // Primitive ctor (primitive.h:80-87): rcp_scale, density_norm_factor, inv_cdf_factor.
   const float rx = __fdiv_rn(1.0f, sx), ry = __fdiv_rn(1.0f, sy), rz = __fdiv_rn(1.0f, sz);
   const float dnf = __fmul_rn(0.0634936359f, __fmul_rn(__fmul_rn(rx, ry), rz));
@@ -840,8 +853,10 @@ vp_status build_empty_scene(vp_context* ctx, const vp_gaussians* g, float sigma_
   v.stack_cap = 31u + 2u;
   v.argmin_cap = v.stack_cap + kArgminBestFirstStack + 64u;
   v.albedo_all_zero = 1;
+  v.tau_nearest = 0;
   vp_scene_info& info = sc->info;
   info = vp_scene_info{};
+  info.tau_order = VP_TAU_ORDER_LANE;
   info.wide_nodes = 1;
   info.wide_depth = 1;
   info.binary_nodes = 1;
@@ -903,7 +918,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   if ((s = dev_alloc(&errw.p, 1, st))) return s;
   if ((s = dev_alloc(&bounds.p, 12, st))) return s;
   {
-    ErrorWords e0{0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, 0u};
+    ErrorWords e0{0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, 0u, 0u};
     VP_CUDA(cudaMemcpyAsync(errw.p, &e0, sizeof(e0), cudaMemcpyHostToDevice, st));
     unsigned int b0[12];
     for (int k = 0; k < 3; ++k) {
@@ -1226,6 +1241,13 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   v.stack_cap = 31u * depth + 2u;
   v.argmin_cap = v.stack_cap + kArgminBestFirstStack + 64u;
   v.albedo_all_zero = eh.any_albedo ? 0 : 1;
+  // AUTO: nearest first where rays need many translucent Gaussians to become opaque and the tree
+  // has levels below the root's children to order (on a two-level tree the ranking pass costs
+  // more than it saves)
+  const int32_t tau_order = opt.tau_order != VP_TAU_ORDER_AUTO ? opt.tau_order
+                            : (2ull * eh.opaque_cores < n && depth >= 3u) ? VP_TAU_ORDER_NEAREST
+                                                                         : VP_TAU_ORDER_LANE;
+  v.tau_nearest = tau_order == VP_TAU_ORDER_NEAREST ? 1 : 0;
   vp_scene_info& info = sc->info;
   info.count = n;
   info.wide_nodes = wide_nodes;
@@ -1238,6 +1260,7 @@ vp_status build_scene(vp_context* ctx, const vp_gaussians* g, float sigma_multip
   info.leaf_max = kLeafMax;
   info.wide_collapse = dp_used ? VP_COLLAPSE_SAH : VP_COLLAPSE_GREEDY;
   info.albedo_all_zero = v.albedo_all_zero;
+  info.tau_order = tau_order;
   info.build_ms = ms;
   for (int k = 0; k < 3; ++k) {
     auto o2f = [](unsigned int u) {

@@ -252,7 +252,7 @@ vp_status vp_context_sm_count(vp_context* c, int32_t* out) {
 
 vp_status vp_scene_options_default(vp_scene_options* out) {
   if (!out) return fail(VP_ERROR_INVALID_ARGUMENT, "NULL argument");
-  *out = vp_scene_options{VP_TREE_PLOC, VP_TREE_PLOC, 24u, VP_DEFAULT_COLLAPSE};
+  *out = vp_scene_options{VP_TREE_PLOC, VP_TREE_PLOC, 24u, VP_DEFAULT_COLLAPSE, VP_TAU_ORDER_AUTO};
   return VP_OK;
 }
 
@@ -270,6 +270,8 @@ vp_status vp_scene_create_ex(vp_context* ctx, const vp_gaussians* g, float sigma
     return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.wide_collapse must be VP_COLLAPSE_GREEDY or VP_COLLAPSE_SAH");
   if (opt.leaf_max < 1u || opt.leaf_max > 32u)
     return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.leaf_max must be in [1, 32]");
+  if (opt.tau_order < VP_TAU_ORDER_AUTO || opt.tau_order > VP_TAU_ORDER_NEAREST)
+    return fail(VP_ERROR_INVALID_ARGUMENT, "vp_scene_options.tau_order must be a vp_tau_order");
   VP_CUDA(cudaSetDevice(ctx->device));
   auto* s = new (std::nothrow) vp_scene();
   if (!s) return fail(VP_ERROR_OUT_OF_MEMORY, "host allocation failed");

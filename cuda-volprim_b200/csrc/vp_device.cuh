@@ -83,6 +83,7 @@ struct SceneView {
                          // kArgminBestFirstStack + 64 (best-first pops need room beyond the
                          // depth-first bound; see warp_ray_query)
   int32_t albedo_all_zero;
+  uint32_t tau_nearest;  // transmittance stacks hit children nearest first (VP_TAU_ORDER_NEAREST)
 };
 
 struct CameraView {

@@ -474,14 +474,16 @@ __device__ float warp_ray_query(const SceneView& S, const WarpSmem& W, float3 o,
           status |= kStatusStackOverflow;
           break;
         }
-        // The traversal continues into the nearest child.  The argmin stacks the others by
-        // distance (farther deeper; rank nh-1 is the nearest), so its culling at the best t*
-        // pops the near ones first.  Transmittance sums every chord whatever the order: it picks
-        // the nearest child by a warp min and stacks the others in lane order, which costs a
-        // fixed few instructions instead of a pass over the hit children.
+        // The traversal continues into the nearest child.  The argmin (without best-first pops)
+        // stacks the others by distance (farther deeper; rank nh-1 is the nearest), so its
+        // culling at the best t* pops the near ones first.  Transmittance sums every chord
+        // whatever the order: in lane order (the nearest child picked by a warp min, a fixed few
+        // instructions) or, for scenes whose rays need many overlapping Gaussians to reach
+        // MAX_OPTICAL_DEPTH (S.tau_nearest), ranked like the argmin so the stop comes sooner.
         int rank = 0;
         int src;
-        if constexpr (kKind == kTau || VP_ARGMIN_BEST_FIRST) {
+        const bool ranked = kKind == kArgmin ? !VP_ARGMIN_BEST_FIRST : (kKind == kTau && S.tau_nearest != 0u);
+        if (!ranked) {
           const unsigned key = hit ? __float_as_uint(tnear + 0.0f) : 0xFFFFFFFFu;  // tnear >= 0: bit order
           const unsigned mn = __reduce_min_sync(kFull, key);
           src = __ffs(__ballot_sync(kFull, hit && key == mn)) - 1;

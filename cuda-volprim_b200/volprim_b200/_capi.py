@@ -19,6 +19,7 @@ VP_MEASURE_COUNTERS, VP_MEASURE_STAGES = 1, 2
 VP_SCHEDULE_FIFO, VP_SCHEDULE_FAIR, VP_SCHEDULE_SRPT = 0, 1, 2
 VP_TREE_PLOC, VP_TREE_LBVH = 0, 1
 VP_COLLAPSE_GREEDY, VP_COLLAPSE_SAH = 0, 1
+VP_TAU_ORDER_AUTO, VP_TAU_ORDER_LANE, VP_TAU_ORDER_NEAREST = 0, 1, 2
 
 ERROR_NAMES = {
     -1: "VP_ERROR_INVALID_ARGUMENT", -2: "VP_ERROR_CUDA", -3: "VP_ERROR_OUT_OF_MEMORY",
@@ -65,7 +66,7 @@ class vp_scene_info(C.Structure):
         ("binary_height", C.c_uint32),
         ("leaf_max", C.c_uint32),
         ("wide_collapse", C.c_int32),
-        ("reserved", C.c_uint32),
+        ("tau_order", C.c_int32),
     ]
 
 
@@ -75,6 +76,7 @@ class vp_scene_options(C.Structure):
         ("binary_builder", C.c_int32),
         ("leaf_max", C.c_uint32),
         ("wide_collapse", C.c_int32),
+        ("tau_order", C.c_int32),
     ]
 
 

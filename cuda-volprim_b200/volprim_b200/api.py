@@ -116,6 +116,8 @@ class Gaussians:
 
 _BUILDERS = {"ploc": _capi.VP_TREE_PLOC, "lbvh": _capi.VP_TREE_LBVH}
 _COLLAPSES = {"greedy": _capi.VP_COLLAPSE_GREEDY, "sah": _capi.VP_COLLAPSE_SAH}
+_TAU_ORDERS = {"auto": _capi.VP_TAU_ORDER_AUTO, "lane": _capi.VP_TAU_ORDER_LANE,
+               "nearest": _capi.VP_TAU_ORDER_NEAREST}
 
 
 class Scene:
@@ -124,20 +126,27 @@ class Scene:
     wide_builder / binary_builder pick the binary tree of the BVH32 (warp and wavefront engines)
     and of the megakernel: "ploc" (clustering, the default) or "lbvh" (Karras radix tree);
     leaf_max is the largest BVH32 leaf (1..32); collapse cuts the BVH32 from its binary tree:
-    "sah" (SAH-optimal slot assignment, the default) or "greedy" (largest area first)."""
+    "sah" (SAH-optimal slot assignment, the default) or "greedy" (largest area first);
+    tau_order is the order transmittance queries visit a node's hit children after the nearest:
+    "lane", "nearest" or "auto" (nearest when fewer than half of the Gaussians are opaque at
+    their core and the BVH32 is at least 3 levels deep)."""
 
     def __init__(self, ctx: Context, g: Gaussians, sigma_multiplier: float = 1.0, wide_builder: str = "ploc",
-                 binary_builder: str = "ploc", leaf_max: int = 24, collapse: str = "sah"):
+                 binary_builder: str = "ploc", leaf_max: int = 24, collapse: str = "sah",
+                 tau_order: str = "auto"):
         n = g.count
         if wide_builder not in _BUILDERS or binary_builder not in _BUILDERS:
             raise ValueError("builders are 'ploc' or 'lbvh'")
         if collapse not in _COLLAPSES:
             raise ValueError("collapse is 'sah' or 'greedy'")
+        if tau_order not in _TAU_ORDERS:
+            raise ValueError("tau_order is 'auto', 'lane' or 'nearest'")
         opt = _capi.vp_scene_options()
         check(lib.vp_scene_options_default(C.byref(opt)))
         opt.wide_builder, opt.binary_builder = _BUILDERS[wide_builder], _BUILDERS[binary_builder]
         opt.leaf_max = int(leaf_max)
         opt.wide_collapse = _COLLAPSES[collapse]
+        opt.tau_order = _TAU_ORDERS[tau_order]
         self.ctx = ctx
         self._keep = []
         s = _capi.vp_gaussians()
@@ -183,6 +192,7 @@ class Scene:
             "binary_builder": "ploc" if i.binary_builder == _capi.VP_TREE_PLOC else "lbvh",
             "binary_height": i.binary_height, "leaf_max": i.leaf_max,
             "wide_collapse": "sah" if i.wide_collapse == _capi.VP_COLLAPSE_SAH else "greedy",
+            "tau_order": "nearest" if i.tau_order == _capi.VP_TAU_ORDER_NEAREST else "lane",
         }
 
     def transmittance(self, origins, dirs, precision: int = _capi.VP_PRECISION_AUTO,

@@ -149,7 +149,7 @@ typedef struct vp_scene_info {
   uint32_t binary_height;   /* height of the PLOC tree (0 when no PLOC tree was built) */
   uint32_t leaf_max;        /* largest BVH32 leaf the build allowed */
   int32_t wide_collapse;    /* vp_collapse the BVH32 was cut with */
-  uint32_t reserved;
+  int32_t tau_order;        /* vp_tau_order in use: VP_TAU_ORDER_LANE or VP_TAU_ORDER_NEAREST */
 } vp_scene_info;
 
 /* Validates the primitives (positive finite scales, positive finite density, finite centres;
@@ -179,6 +179,20 @@ typedef enum vp_collapse {
                              greedy bound, use the greedy collapse */
 } vp_collapse;
 
+/* The order in which a transmittance query visits the hit children of a BVH32 node after the
+ * nearest one.  The optical depth is the same sum either way; the order decides how soon a ray
+ * reaches MAX_OPTICAL_DEPTH and stops. */
+typedef enum vp_tau_order {
+  VP_TAU_ORDER_AUTO = 0,    /* NEAREST when fewer than half of the Gaussians are opaque at their
+                               core (central optical depth along their thinnest direction below
+                               4 x MAX_OPTICAL_DEPTH) and the BVH32 is at least 3 levels deep,
+                               else LANE */
+  VP_TAU_ORDER_LANE = 1,    /* in child-slot order (no ranking pass): best when single Gaussians
+                               stop most rays */
+  VP_TAU_ORDER_NEAREST = 2  /* nearest first (a ranking pass per node): best when a ray needs many
+                               overlapping Gaussians to become opaque */
+} vp_tau_order;
+
 /* Build choices of vp_scene_create_ex; vp_scene_create uses vp_scene_options_default. */
 typedef struct vp_scene_options {
   int32_t wide_builder;   /* vp_tree_builder collapsed into the BVH32 of the warp and wavefront
@@ -189,6 +203,7 @@ typedef struct vp_scene_options {
   uint32_t leaf_max;      /* largest BVH32 leaf in Gaussians, 1..32 (default 24) */
   int32_t wide_collapse;  /* vp_collapse: how the binary tree becomes 32-wide nodes (default
                              VP_COLLAPSE_SAH) */
+  int32_t tau_order;      /* vp_tau_order of the scene's transmittance queries (default AUTO) */
 } vp_scene_options;
 
 vp_status vp_scene_options_default(vp_scene_options* out);
