@@ -659,7 +659,7 @@ def other_configs(device):
     out["stress_2m"] = {"mpaths_per_s": statistics.median(rates), "mpaths_per_s_spread": spread(rates),
                         "ms_per_render": statistics.median(totals), "spp": spp, "paths": paths,
                         "gaussians": info["count"], "bvh_build_ms": statistics.median(builds),
-                        "bvh_build_ms_spread": spread(builds), "bvh32_nodes": info["wide_nodes"],
+                        "bvh_build_ms_spread": spread(builds), "bvh32_nodes": info["wide_nodes"], "tau_order": info["tau_order"],
                         "precision": cfg.precision,
                         "max_point_overlap": m["max_point_overlap"], "max_hits_per_ray": m["max_hits_per_ray"],
                         "crossings_per_16spp": m["crossings"],
