@@ -196,7 +196,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
             "config": {"workload": f"showcase_{args.n // 1000}k", "gaussians": args.n, "width": args.res,
-                       "height": args.res, "spp": args.spp, "nee": "mis", "max_depth": 64, "rr_depth": 12,
+                       "height": args.res, "spp_per_rank": args.spp, "nee": "mis", "max_depth": 64, "rr_depth": 12,
                        "env": "procedural 2048x1024", "l2": "n/a (host)"},
             "cpu_baseline": {**res[-1], "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
