@@ -529,8 +529,6 @@ def differentiation_form(device):
     256x256 x 8 spp, L2 loss against a render of perturbed parameters): one gradient = the
     autograd Function's scene build + 4 forward renders + 4 adjoint renders, timed on the host
     around torch.cuda.synchronize (the library calls are synchronous)."""
-    import ctypes as C
-
     import numpy as np
     import torch
     import volprim_b200 as vp

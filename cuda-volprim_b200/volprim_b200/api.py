@@ -16,7 +16,7 @@ to an EXR file, errors raise VpError instead of exiting the process, and the sce
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Optional
 
 import numpy as np

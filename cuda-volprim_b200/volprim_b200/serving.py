@@ -13,7 +13,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 

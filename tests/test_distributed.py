@@ -3,7 +3,6 @@ multi-GPU path.  Each rank renders its sample range with the oracle (the CPU che
 ranks combine with volprim_b200.distributed.combine; the result must equal the single-process
 render over all samples."""
 import math
-import os
 import socket
 
 import numpy as np

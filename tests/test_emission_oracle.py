@@ -5,7 +5,6 @@ finite differences of itself."""
 import math
 
 import numpy as np
-import pytest
 import torch
 
 import oracle as O

@@ -15,7 +15,6 @@ seeded render of perturbed parameters -- against the FP64 oracle (oracle/emissio
             grazes the ellipsoid; each step is kept below 2% of the parameter distance at which
             any ray first reaches it (a parameter whose step would fall below 1e-9 is skipped).
 """
-import math
 
 import numpy as np
 import pytest
