@@ -672,7 +672,7 @@ def other_configs(device):
     return out
 
 
-SERVING_P99_TARGET_S = 3.0  # stated p99 latency target at 80% of offline throughput
+SERVING_P99_TARGET_S = 3.0  # the stated p99 latency target of the serving form, at 80% of offline throughput
 
 
 def serving_form(device, n_requests):
