@@ -239,6 +239,18 @@ def capacity(trace: list) -> list:
     return [Request(0.0, r.scene_id, r.camera, r.config) for r in trace]
 
 
+def schedule_spec(spec: str) -> tuple:
+    """A schedule name of the serving study: "fifo", "fair", "srpt", or "srpt/A" for SRPT with
+    srpt_aging A (>= 0).  Returns (schedule, srpt_aging)."""
+    name, sep, aging = spec.partition("/")
+    if name not in ("fifo", "fair", "srpt") or (sep and name != "srpt"):
+        raise ValueError(f"unknown schedule {spec!r}: fifo, fair, srpt or srpt/AGING")
+    a = float(aging) if sep else 0.0
+    if not a >= 0.0:
+        raise ValueError(f"negative srpt aging in {spec!r}")
+    return name, a
+
+
 def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, load: float = 0.8, seed: int = 2024,
                   schedules=("fifo",), path_slots: int = 1 << 18, log=None, rate: float | None = None,
                   srpt_reserve: float = 0.5, plain: bool = True, capacity_runs: bool = True,
@@ -261,10 +273,9 @@ def serving_study(ctx, n_requests: int = 1000, capacity_requests: int = 300, loa
     envs = [env] * len(scs)
 
     def server(schedule):
-        # "srpt/A": SRPT with srpt_aging A
-        name, _, aging = schedule.partition("/")
+        name, aging = schedule_spec(schedule)
         srv = Server(ctx, memory_budget_bytes=150 * 10 ** 9, schedule=name, path_slots=path_slots,
-                     srpt_reserve=srpt_reserve, lanes=lanes, srpt_aging=float(aging or 0.0))
+                     srpt_reserve=srpt_reserve, lanes=lanes, srpt_aging=aging)
         for sc in scs:
             srv.add_scene(sc, env)
         return srv

@@ -1,7 +1,8 @@
 """CPU: the serving workload's request stream and the latency statistics (no device work)."""
 import numpy as np
+import pytest
 
-from volprim_b200.serving import make_trace, percentile
+from volprim_b200.serving import make_trace, percentile, schedule_spec
 
 
 def test_trace_distribution():
@@ -41,3 +42,12 @@ def test_percentile_nearest_rank():
     assert percentile(v, 99) == 99
     assert percentile(v, 100) == 100
     assert percentile([3.0], 99) == 3.0
+
+
+def test_schedule_spec():
+    assert schedule_spec("fifo") == ("fifo", 0.0)
+    assert schedule_spec("srpt") == ("srpt", 0.0)
+    assert schedule_spec("srpt/0.25") == ("srpt", 0.25)
+    for bad in ("lifo", "fair/1", "srpt/-1", "srpt/x"):
+        with pytest.raises(ValueError):
+            schedule_spec(bad)
